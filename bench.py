@@ -1,0 +1,481 @@
+"""Benchmark: COTs/sec of the silent-OT hot path on B200.
+
+A step produces one full COT correlation on the GPU: both roles (sender and
+receiver) of one OT-extension instance, seeded synthetic inputs of the named
+shape.
+
+Workloads (--workload):
+  sot_n20     plain SOT, n = 2^20: 256 GGM trees of depth 12 (both roles),
+              exact quasi-cyclic encode of the 128 bit planes of the 2n-bit
+              (zero-padded) noise vector, transposes both ways, plus the
+              receiver's choice-bit encode.            [default]
+  ferret_b13  plain Ferret at full size (ferret_b13): n = 10,485,760,
+              t = 1280 trees of depth 13, k = 452,000, d = 10 (both roles:
+              MPCOT + primal LPN).
+  ferret_c1   plain Ferret small: t = 64, h = 10, k = 8192.
+
+Multi-GPU: one process per GPU (torchrun), each rank runs its own instance
+(the path shards by independent instances; no data-path collective):
+"scaling": "weak", value = COTs of all ranks / max-over-ranks time.
+
+--impl reference: the reference's CPU implementation of the path (emp-ot /
+cryptoTools semantics restated in oracle/, since emp-tool is not buildable
+here) timed on all host threads on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np
+
+WORKLOADS = {
+    "sot_n20": dict(kind="sot", t=256, h=12),
+    "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
+    "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
+}
+CONFIG_TEXT = {
+    "sot_n20": "plain SOT n=2^20: 256 GGM trees depth 12, exact QC encode of 128 planes, transposes (both roles)",
+    "ferret_b13": "plain Ferret ferret_b13: n=10485760, t=1280, h=13, k=452000, d=10 (both roles)",
+    "ferret_c1": "plain Ferret small: n=65536, t=64, h=10, k=8192, d=10 (both roles)",
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# --------------------------------------------------------------------------
+class Instance:
+    """Seeded synthetic inputs + device buffers for one workload instance."""
+
+    def __init__(self, name: str, seed: int, torch, cuot_b200):
+        self.name, self.spec = name, WORKLOADS[name]
+        self.torch, self.cb = torch, cuot_b200
+        s = self.spec
+        self.t, self.h = s["t"], s["h"]
+        self.n = self.t << self.h
+        rng = np.random.default_rng(seed)
+        blk = lambda m: rng.integers(0, 256, (m, 16), dtype=np.uint8)
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device="cuda")
+        t, h, n = self.t, self.h, self.n
+        self.roots = blk(t)
+        self.delta = blk(1)[0]
+        self.delta[0] |= 1
+        self.choice = rng.integers(0, 2, t * h).astype(np.uint8)
+        # device buffers
+        self.sctx = cuot_b200.Context(torch.cuda.current_device())
+        self.rctx = cuot_b200.Context(torch.cuda.current_device())
+        self.d_roots = dev(self.roots)
+        self.d_choice = dev(self.choice)
+        self.leaves_s, self.leaves_r = emp(n), emp(n)
+        if s["kind"] == "ferret":
+            k = s["k"]
+            self.k, self.d = k, s["d"]
+            self.kk_s = blk(k)
+            self.kk_r = blk(k)
+            self.d_kk_s, self.d_kk_r = dev(self.kk_s), dev(self.kk_r)
+            self.lsum, self.rsum, self.ss = emp(t * h), emp(t * h), emp(t)
+            self.mc = emp(t * h)
+            self.seed = blk(1)[0]
+        else:
+            self.base0, self.base1 = blk(h * t), blk(h * t)
+            self.d_b0, self.d_b1 = dev(self.base0), dev(self.base1)
+            self.mc_np = np.where(self.choice[:, None] == 0, self.base0, self.base1)
+            self.d_mc = dev(self.mc_np)
+            self.m0, self.m1 = emp((h + 1) * t), emp((h + 1) * t)
+            self.a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+            self.sctx.qc_gen_a(blk(1)[0], n, self.a)
+            self.plan_s = self.sctx.qc_plan(self.a, n)
+            self.plan_r = self.rctx.qc_plan(self.a, n)
+            chm = self.choice.reshape(h, t)
+            pos = np.zeros(t, np.int64)
+            for dd in range(h):
+                pos = pos * 2 + 1 - chm[dd].astype(np.int64)
+            self.d_pos = dev(pos + np.arange(t) * (1 << h))
+            self.cbits = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+
+    # one step on the device (inputs resident); stage events optional
+    def step(self, ev=None):
+        torch = self.torch
+        mark = (lambda k: ev[k].record()) if ev is not None else (lambda k: None)
+        if self.spec["kind"] == "ferret":
+            t, h = self.t, self.h
+            mark("pprf0")
+            self.sctx.ferret_pprf_sender(self.d_roots, h, self.delta, self.leaves_s, self.lsum, self.rsum, self.ss)
+            # ideal OT of the per-level sums (OTIdeal, emp-ot/ideal.h): mc = choice ? rsum : lsum
+            torch.where(self.d_choice.view(-1, 1).bool(), self.rsum, self.lsum, out=self.mc)
+            self.rctx.ferret_pprf_recver(self.mc, self.d_choice, self.ss, h, self.leaves_r)
+            mark("pprf1")
+            self.sctx.lpn_primal(self.seed, self.d_kk_s, self.leaves_s, d=self.d)
+            self.rctx.lpn_primal(self.seed, self.d_kk_r, self.leaves_r, d=self.d)
+            mark("lpn1")
+        else:
+            t, h, n = self.t, self.h, self.n
+            mark("pprf0")
+            self.sctx.sot_pprf_sender(self.d_roots, h, self.delta, self.d_b0, self.d_b1, self.leaves_s,
+                                      self.m0, self.m1)
+            self.rctx.sot_pprf_recver(self.m0, self.m1, self.d_mc, self.d_choice, t, h, self.leaves_r)
+            mark("pprf1")
+            self.plan_s.dual_lpn(self.leaves_s)
+            self.plan_r.dual_lpn(self.leaves_r)
+            self.rctx.qc_encode_sparse(self.a, self.d_pos, n, self.cbits)
+            mark("lpn1")
+
+    def launches_per_step(self) -> int:
+        before = self.cb.launch_count()
+        self.step()
+        self.torch.cuda.synchronize()
+        return self.cb.launch_count() - before
+
+
+def e2e_step(inst: Instance, host, stream):
+    """Same step through the public API with HOST buffers: H2D of the step's
+    inputs from pinned memory, D2H of the results, inside the timed region.
+    Returns (h2d_bytes, d2h_bytes)."""
+    torch = inst.torch
+    h2d = d2h = 0
+    with torch.cuda.stream(stream):
+        inst.d_roots.copy_(host["roots"], non_blocking=True)
+        inst.d_choice.copy_(host["choice"], non_blocking=True)
+        h2d += host["roots"].numel() + host["choice"].numel()
+        if inst.spec["kind"] == "ferret":
+            inst.d_kk_s.copy_(host["kk_s"], non_blocking=True)
+            inst.d_kk_r.copy_(host["kk_r"], non_blocking=True)
+            h2d += host["kk_s"].numel() + host["kk_r"].numel()
+            inst.sctx.ferret_pprf_sender(inst.d_roots, inst.h, inst.delta, inst.leaves_s, inst.lsum, inst.rsum,
+                                         inst.ss, stream=stream)
+            # sums and secret sums go to the host (sent to the receiver by the OT), as in
+            # dev_layer.cu:40-41,50; the chosen messages come back to the receiver's GPU
+            host["lsum"].copy_(inst.lsum, non_blocking=True)
+            host["rsum"].copy_(inst.rsum, non_blocking=True)
+            host["ss"].copy_(inst.ss, non_blocking=True)
+            d2h += 3 * 0 + host["lsum"].numel() + host["rsum"].numel() + host["ss"].numel()
+            torch.where(inst.d_choice.view(-1, 1).bool(), inst.rsum, inst.lsum, out=inst.mc)
+            inst.rctx.ferret_pprf_recver(inst.mc, inst.d_choice, inst.ss, inst.h, inst.leaves_r, stream=stream)
+            inst.sctx.lpn_primal(inst.seed, inst.d_kk_s, inst.leaves_s, d=inst.d, stream=stream)
+            inst.rctx.lpn_primal(inst.seed, inst.d_kk_r, inst.leaves_r, d=inst.d, stream=stream)
+        else:
+            inst.d_b0.copy_(host["b0"], non_blocking=True)
+            inst.d_b1.copy_(host["b1"], non_blocking=True)
+            inst.d_mc.copy_(host["mc"], non_blocking=True)
+            h2d += host["b0"].numel() + host["b1"].numel() + host["mc"].numel()
+            inst.sctx.sot_pprf_sender(inst.d_roots, inst.h, inst.delta, inst.d_b0, inst.d_b1, inst.leaves_s,
+                                      inst.m0, inst.m1, stream=stream)
+            inst.rctx.sot_pprf_recver(inst.m0, inst.m1, inst.d_mc, inst.d_choice, inst.t, inst.h, inst.leaves_r,
+                                      stream=stream)
+            inst.plan_s.dual_lpn(inst.leaves_s, stream=stream)
+            inst.plan_r.dual_lpn(inst.leaves_r, stream=stream)
+            inst.rctx.qc_encode_sparse(inst.a, inst.d_pos, inst.n, inst.cbits, stream=stream)
+            host["c"].copy_(inst.cbits, non_blocking=True)
+            d2h += host["c"].numel() * 8
+        host["v"].copy_(inst.leaves_s, non_blocking=True)
+        host["w"].copy_(inst.leaves_r, non_blocking=True)
+        d2h += host["v"].numel() + host["w"].numel()
+    return h2d, d2h
+
+
+def make_host(inst: Instance):
+    torch = inst.torch
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    host = {"roots": pin(inst.roots), "choice": pin(inst.choice),
+            "v": torch.empty((inst.n, 16), dtype=torch.uint8).pin_memory(),
+            "w": torch.empty((inst.n, 16), dtype=torch.uint8).pin_memory()}
+    if inst.spec["kind"] == "ferret":
+        host.update(kk_s=pin(inst.kk_s), kk_r=pin(inst.kk_r),
+                    lsum=torch.empty((inst.t * inst.h, 16), dtype=torch.uint8).pin_memory(),
+                    rsum=torch.empty((inst.t * inst.h, 16), dtype=torch.uint8).pin_memory(),
+                    ss=torch.empty((inst.t, 16), dtype=torch.uint8).pin_memory())
+    else:
+        host.update(b0=pin(inst.base0), b1=pin(inst.base1), mc=pin(inst.mc_np),
+                    c=torch.empty(inst.n // 64, dtype=torch.int64).pin_memory())
+    return host
+
+
+# --------------------------------------------------------------------------
+def cpu_sample(name: str, threads: int, budget_s: float = 10.0):
+    """Times the oracle port (restated emp-ot / cryptoTools CPU path) on a
+    bounded sample of the workload; returns (COTs/s, sample description)."""
+    import oracle
+    spec = WORKLOADS[name]
+    rng = np.random.default_rng(99)
+    blk = lambda m: rng.integers(0, 256, (m, 16), dtype=np.uint8)
+    t_full, h = spec["t"], spec["h"]
+    if spec["kind"] == "ferret":
+        t = min(t_full, max(threads, 64))
+        n = t << h
+        roots, delta = blk(t), blk(1)[0]
+        delta[0] |= 1
+        kk = blk(spec["k"])
+        ch = rng.integers(0, 2, t * h).astype(np.uint8)
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            lv, ls, rs, ss = oracle.ferret_pprf_sender(roots, h, delta, threads=threads)
+            mc = np.where(ch[:, None] == 0, ls, rs)
+            rl = oracle.ferret_pprf_recver(mc, ch, ss, h, threads=threads)
+            oracle.lpn_primal(blk(1)[0], kk, lv, d=spec["d"], threads=threads)
+            oracle.lpn_primal(blk(1)[0], kk, rl, d=spec["d"], threads=threads)
+            reps += 1
+            el = time.perf_counter() - t0
+            if el > budget_s or reps >= 3:
+                break
+        return reps * n / el, f"{t} of {t_full} trees (n={n}), both roles, MPCOT + LPN (k={spec['k']}), {reps} reps"
+    # SOT: PPRF both roles on all trees; QC encode on a subset of planes, scaled
+    n = t_full << h
+    roots, delta = blk(t_full), blk(1)[0]
+    b0, b1 = blk(h * t_full), blk(h * t_full)
+    ch = rng.integers(0, 2, h * t_full).astype(np.uint8)
+    mc = np.where(ch[:, None] == 0, b0, b1)
+    a = oracle.qc_gen_a(blk(1)[0], n)
+    nplanes = max(4, min(128, threads * 2))
+    t0 = time.perf_counter()
+    lv, m0, m1 = oracle.sot_pprf_sender(roots, h, delta, b0, b1, threads=threads)
+    rl = oracle.sot_pprf_recver(m0, m1, mc, ch, t_full, h, threads=threads)
+    t_pprf = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    pl = oracle.bit_transpose(lv, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    oracle.qc_encode(a, pl[:nplanes].copy(), n, threads=threads)
+    t_qc = (time.perf_counter() - t0) * (128 / nplanes) * 2  # both roles
+    el = t_pprf + t_qc
+    return n / el, f"both roles PPRF on all {t_full} trees; QC encode timed on {nplanes} of 128 planes (one role) and scaled x{128 / nplanes * 2:g}"
+
+
+# --------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    name = args.workload
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    sample = ""
+    for i in range(args.warmup + args.steps):
+        v, sample = cpu_sample(name, threads, budget_s=5.0)
+        if i >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    unit = "COTs/s"
+    print(json.dumps({
+        "impl": "reference", "metric": "COTs/sec on 1 B200 (plain path, bit-exact)", "value": v, "unit": unit,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": name, "what": CONFIG_TEXT[name]},
+        "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path: emp-ot/cryptoTools semantics restated in oracle/ (emp-tool is not "
+                "vendored, so emp-ot cannot be built); all host threads",
+    }), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import cuot_b200
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    inst = Instance(args.workload, 1234 + rank, torch, cuot_b200)
+    n = inst.n
+    # warm-up
+    for _ in range(args.warmup):
+        inst.step()
+    torch.cuda.synchronize()
+    launches = inst.launches_per_step()
+
+    # L2 flush buffer (larger than the 126 MB L2), written between steps
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    names = ["pprf0", "pprf1", "lpn1"]
+    step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stage_ev = [{k: torch.cuda.Event(enable_timing=True) for k in names} for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        flush.zero_()
+        step_ev[i][0].record()
+        inst.step(stage_ev[i])
+        step_ev[i][1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = clk.stop()
+    ms_steps = [a.elapsed_time(b) for a, b in step_ev]
+    ms = sum(ms_steps) / len(ms_steps)
+    pprf_ms = statistics.mean(e["pprf0"].elapsed_time(e["pprf1"]) for e in stage_ev)
+    lpn_ms = statistics.mean(e["pprf1"].elapsed_time(e["lpn1"]) for e in stage_ev)
+    if dist:
+        tt = torch.tensor([ms, pprf_ms, lpn_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, pprf_ms, lpn_ms = tt.tolist()
+    value = world * n / (ms / 1e3)
+
+    # e2e through the public API with host buffers
+    host = make_host(inst)
+    stream = torch.cuda.Stream()
+    for _ in range(max(1, args.warmup)):
+        e2e_step(inst, host, stream)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        h2d, d2h = e2e_step(inst, host, stream)
+    e1.record(stream)
+    stream.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = tt.item()
+
+    # roofline of the dominant stage
+    peaks, peak_kind = measured_peaks()
+    if inst.spec["kind"] == "ferret":
+        k = inst.k
+        # LPN: algorithmic bytes per launch = 32n (e read + y write) + 16k (kk once); 2 launches / step
+        lpn_bytes = 2 * (32 * n + 16 * k)
+        pprf_bytes = 2 * (16 * n + 32 * inst.t * inst.h)
+        stages = {"pprf": (pprf_ms, pprf_bytes), "lpn": (lpn_ms, lpn_bytes)}
+    else:
+        # dual LPN: two transposes (32n each) + encode in/out (32n) per role
+        stages = {"pprf": (pprf_ms, 2 * (16 * n + 32 * inst.t * (inst.h + 1))),
+                  "dual_lpn": (lpn_ms, 2 * (3 * 32 * n))}
+    dom = max(stages, key=lambda s: stages[s][0])
+    dms, dbytes = stages[dom]
+    achieved = dbytes / (dms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(f"{args.workload}:{dom}")
+    out = {
+        "metric": "COTs/sec on 1 B200 (plain path, bit-exact)",
+        "value": value, "unit": "COTs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "cots_per_step_per_gpu": n,
+                   "parallelism": f"replicas x{world} (independent instances per GPU)",
+                   "l2": "256 MiB buffer written between timed steps (L2 flush)"},
+        "stages_ms": {k: v[0] for k, v in stages.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                     "algorithmic_bytes_per_step": dbytes},
+        "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sample = cpu_sample(args.workload, threads)
+        out["cpu_baseline"] = {"value": v, "unit": "COTs/s", "cores": threads, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del inst
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sot_n20", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,242 @@
+// lpn.cu -- Ferret primal LPN and plain AES-128 ECB.
+//
+// LPN: e[i] ^= XOR_{j<d} kk[idx(i, j)] with emp-ot's index matrix
+// (lpn_f2.h:46-79, one task over [0, n)):
+//   rows i..i+3 (i % 4 == 0, i < tail): the d blocks makeBlock(i, m), m < d,
+//     are AES-encrypted under the seed key; their 4d little-endian u32 words
+//     give row i + q/d, term q%d: idx = w & mask, minus k if >= k.
+//   rows j >= tail (tail = first multiple of 4 >= n-4): ceil(d/4) blocks
+//     makeBlock(j, m), idx = w % k.
+// The index AES runs in the same kernel as the gather, so the n*d index
+// matrix never touches HBM (cuOT materialises it, dev_layer.cu:171-173).
+// kk (k blocks) is read through the read-only path and stays L2-resident.
+#include "ctx.cuh"
+
+namespace cuot {
+
+struct LpnArgs {
+  AesKey key;
+  const uint32_t *t0;
+  const Blk *kk;
+  Blk *e;
+  int64_t n, k, tail, ngroups, ntail;
+  uint32_t mask;
+  int d;
+};
+
+constexpr int kLpnThreads = 256;
+
+__device__ __forceinline__ uint32_t lpn_idx(uint32_t w, uint32_t mask, uint32_t k) {
+  uint32_t x = w & mask;
+  return x >= k ? x - k : x;
+}
+
+// Rows 4g..4g+3 for d = D known at compile time.
+template <int D>
+__device__ __forceinline__ void lpn_group4(const LpnArgs &a, const TabRef &T, int64_t g) {
+  const int64_t i = 4 * g;
+  const uint32_t k = uint32_t(a.k), mask = a.mask;
+  Blk acc[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) acc[m] = Blk{{0, 0, 0, 0}};
+  // makeBlock(i, m): low qword m, high qword i.
+  const uint32_t ilo = uint32_t(uint64_t(i)), ihi = uint32_t(uint64_t(i) >> 32);
+#pragma unroll
+  for (int m = 0; m < D; m += 2) {
+    uint32_t x[4] = {uint32_t(m), 0u, ilo, ihi};
+    uint32_t y[4] = {uint32_t(m + 1), 0u, ilo, ihi};
+    if (m + 1 < D) {
+      aes_enc2(T, x, a.key.rk, y, a.key.rk);
+    } else {
+      aes_enc(T, x, a.key.rk);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int word = 4 * m + q;  // compile-time after unrolling
+      const Blk v = ldg_blk(a.kk + lpn_idx(x[q], mask, k));
+      acc[word / D] = blk_xor(acc[word / D], v);
+    }
+    if (m + 1 < D) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int word = 4 * (m + 1) + q;
+        const Blk v = ldg_blk(a.kk + lpn_idx(y[q], mask, k));
+        acc[word / D] = blk_xor(acc[word / D], v);
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    Blk *p = a.e + i + m;
+    st_blk_cs(p, blk_xor(ld_blk(p), acc[m]));
+  }
+}
+
+// Rows 4g..4g+3 for any d (1..32).
+__device__ void lpn_group4_dyn(const LpnArgs &a, const TabRef &T, int64_t g) {
+  const int64_t i = 4 * g;
+  const uint32_t k = uint32_t(a.k), mask = a.mask;
+  Blk acc[4] = {{{0, 0, 0, 0}}, {{0, 0, 0, 0}}, {{0, 0, 0, 0}}, {{0, 0, 0, 0}}};
+  const uint32_t ilo = uint32_t(uint64_t(i)), ihi = uint32_t(uint64_t(i) >> 32);
+  for (int m = 0; m < a.d; m++) {
+    uint32_t x[4] = {uint32_t(m), 0u, ilo, ihi};
+    aes_enc(T, x, a.key.rk);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int word = 4 * m + q;
+      const Blk v = ldg_blk(a.kk + lpn_idx(x[q], mask, k));
+      const int row = word / a.d;
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+        if (r == row) acc[r] = blk_xor(acc[r], v);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    Blk *p = a.e + i + m;
+    st_blk_cs(p, blk_xor(ld_blk(p), acc[m]));
+  }
+}
+
+// One tail row (emp-ot __compute1, lpn_f2.h:61-70).
+__device__ void lpn_row1(const LpnArgs &a, const TabRef &T, int64_t j) {
+  const int nb = (a.d + 3) / 4;
+  const uint32_t k = uint32_t(a.k);
+  const uint32_t jlo = uint32_t(uint64_t(j)), jhi = uint32_t(uint64_t(j) >> 32);
+  Blk acc{{0, 0, 0, 0}};
+  int done = 0;
+  for (int m = 0; m < nb; m++) {
+    uint32_t x[4] = {uint32_t(m), 0u, jlo, jhi};
+    aes_enc(T, x, a.key.rk);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (done < a.d) acc = blk_xor(acc, ldg_blk(a.kk + (x[q] % k)));
+      done++;
+    }
+  }
+  Blk *p = a.e + j;
+  st_blk(p, blk_xor(ld_blk(p), acc));
+}
+
+template <int D>
+__global__ void __launch_bounds__(kLpnThreads) lpn_kernel(LpnArgs a) {
+  extern __shared__ __align__(16) uint32_t smem_tab[];
+  stage_table(smem_tab, a.t0);
+  __syncthreads();
+  const TabRef T{reinterpret_cast<const char *>(smem_tab), uint32_t(threadIdx.x & 31) * 4u};
+  const int64_t total = a.ngroups + a.ntail;
+  for (int64_t w = int64_t(blockIdx.x) * kLpnThreads + threadIdx.x; w < total;
+       w += int64_t(gridDim.x) * kLpnThreads) {
+    if (w < a.ngroups) {
+      if (D > 0) lpn_group4<(D > 0 ? D : 1)>(a, T, w);
+      else lpn_group4_dyn(a, T, w);
+    } else {
+      lpn_row1(a, T, a.tail + (w - a.ngroups));
+    }
+  }
+}
+
+// Plain in-place AES-128 ECB, two blocks per thread.
+__global__ void __launch_bounds__(kLpnThreads) ecb_kernel(AesKey key, const uint32_t *t0,
+                                                          Blk *io, uint64_t n) {
+  extern __shared__ __align__(16) uint32_t smem_tab[];
+  stage_table(smem_tab, t0);
+  __syncthreads();
+  const TabRef T{reinterpret_cast<const char *>(smem_tab), uint32_t(threadIdx.x & 31) * 4u};
+  const uint64_t half = (n + 1) / 2;
+  for (uint64_t i = uint64_t(blockIdx.x) * kLpnThreads + threadIdx.x; i < half;
+       i += uint64_t(gridDim.x) * kLpnThreads) {
+    const uint64_t j = i + half;  // second block, keeps both accesses coalesced
+    Blk p = ld_blk(io + i);
+    uint32_t x[4] = {p.w[0], p.w[1], p.w[2], p.w[3]};
+    if (j < n) {
+      Blk q = ld_blk(io + j);
+      uint32_t y[4] = {q.w[0], q.w[1], q.w[2], q.w[3]};
+      aes_enc2(T, x, key.rk, y, key.rk);
+      st_blk(io + j, Blk{{y[0], y[1], y[2], y[3]}});
+    } else {
+      aes_enc(T, x, key.rk);
+    }
+    st_blk(io + i, Blk{{x[0], x[1], x[2], x[3]}});
+  }
+}
+
+static int grid_for(cuot_ctx *ctx, const void *fn, int64_t work, int *grid) {
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kLpnThreads, kTableBytes);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  if (per_sm < 1) per_sm = 1;
+  int64_t need = (work + kLpnThreads - 1) / kLpnThreads;
+  int64_t cap = int64_t(per_sm) * sms * 8;
+  *grid = int(need < cap ? (need > 0 ? need : 1) : cap);
+  return CUOT_OK;
+}
+
+template <typename F>
+static int set_smem(F fn) {
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kTableBytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "cudaFuncSetAttribute failed: %s", cudaGetErrorString(e));
+  }
+  return CUOT_OK;
+}
+
+}  // namespace cuot
+
+using namespace cuot;
+
+extern "C" {
+
+int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
+                    int64_t k, int d, cuot_block *e_io_d, int64_t n, void *stream) {
+  if (!ctx || !seed || !kk_d || !e_io_d) return fail(CUOT_EINVAL, "null argument");
+  if (k < 1 || k > 0x7fffffffll) return fail(CUOT_EINVAL, "k=%lld out of range", (long long)k);
+  if (d < 1 || d > 32) return fail(CUOT_EINVAL, "d=%d out of range [1,32]", d);
+  if (n < 0) return fail(CUOT_EINVAL, "n < 0");
+  if (n == 0) return CUOT_OK;
+  DeviceGuard g(ctx);
+  LpnArgs a{};
+  host_aes_key_expand(seed, &a.key);
+  a.t0 = ctx->t0_d;
+  a.kk = reinterpret_cast<const Blk *>(kk_d);
+  a.e = reinterpret_cast<Blk *>(e_io_d);
+  a.n = n; a.k = k; a.d = d;
+  uint32_t mask = 1;
+  while (int64_t(mask) < k) mask = (mask << 1) | 1u;  // lpn_f2.h:27-31
+  a.mask = mask;
+  int64_t tail = 0;
+  if (n > 4) tail = ((n - 4) + 3) / 4 * 4;  // first j = 0 mod 4 with j >= n-4
+  a.tail = tail;
+  a.ngroups = tail / 4;
+  a.ntail = n - tail;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int grid = 1;
+  if (d == 10) {
+    CUOT_TRY(set_smem(lpn_kernel<10>));
+    grid_for(ctx, (const void *)lpn_kernel<10>, a.ngroups + a.ntail, &grid);
+    lpn_kernel<10><<<grid, kLpnThreads, kTableBytes, st>>>(a);
+  } else {
+    CUOT_TRY(set_smem(lpn_kernel<0>));
+    grid_for(ctx, (const void *)lpn_kernel<0>, a.ngroups + a.ntail, &grid);
+    lpn_kernel<0><<<grid, kLpnThreads, kTableBytes, st>>>(a);
+  }
+  return launch_status();
+}
+
+int cuot_aes128_ecb(cuot_ctx *ctx, const uint8_t key[16], cuot_block *io_d,
+                    uint64_t nblocks, void *stream) {
+  if (!ctx || !key || (!io_d && nblocks)) return fail(CUOT_EINVAL, "null argument");
+  if (nblocks == 0) return CUOT_OK;
+  DeviceGuard g(ctx);
+  AesKey k;
+  host_aes_key_expand(key, &k);
+  CUOT_TRY(set_smem(ecb_kernel));
+  int grid = 1;
+  grid_for(ctx, (const void *)ecb_kernel, int64_t((nblocks + 1) / 2), &grid);
+  ecb_kernel<<<grid, kLpnThreads, kTableBytes, static_cast<cudaStream_t>(stream)>>>(
+      k, ctx->t0_d, reinterpret_cast<Blk *>(io_d), nblocks);
+  return launch_status();
+}
+
+}  // extern "C"

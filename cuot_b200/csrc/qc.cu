@@ -1,0 +1,528 @@
+// qc.cu -- exact quasi-cyclic encode over GF(2)[x]/(x^n - 1) (SOT dual LPN).
+//
+// The reference multiplies with float32 cuFFT and recovers bits by truncating
+// the unnormalised result (silent/quasi_cyclic.cu:34-49, 118-128), which is
+// not exact.  Here out_r = a * b_r mod (x^n - 1) is the parity of the
+// integer cyclic convolution, whose coefficients lie in [0, n]; it is
+// computed exactly with a number-theoretic transform over
+//   p = 7 * 2^26 + 1 = 469762049 (prime, 3 a primitive root),
+// so every coefficient < n <= 2^26 < p is recovered exactly and its parity
+// is the GF(2) coefficient.  n = 2^e, 10 <= e <= 26.
+//
+// Four-step NTT, n = N1 * N2, input index j = N2*j1 + j2, output k = k1 + N1*k2:
+//   A  (columns): per plane and 8 columns j2: load bits, N1-point DIF NTT
+//      over j1 (natural -> bit-reversed row label r), multiply by
+//      w_n^(j2 * rev(r)), store Y[r][j2].
+//   B  (rows):   per row r: N2-point DIF NTT, multiply by A_hat / n (Shoup),
+//      N2-point DIT inverse NTT (bit-reversed -> natural), store.
+//   C  (columns): per plane and 8 columns: multiply by w_n^-(j2 * rev(r)),
+//      N1-point DIT inverse over r (-> natural j1), reduce mod p, take the
+//      parity, pack 8 bits per byte.
+// Butterflies use Harvey's lazy reduction (values kept in [0, 2p)) and
+// Shoup multiplication by precomputed twiddles (w, floor(w * 2^32 / p)).
+// A_hat is the NTT of `a` in the same (r, q) label order, computed on the
+// device with passes A and B-forward; planes are processed in batches so
+// the 4-byte-per-coefficient intermediate stays within a bounded footprint.
+#include <cstdlib>
+#include <vector>
+#include "ctx.cuh"
+
+namespace cuot {
+
+constexpr uint32_t kP = 469762049u;
+constexpr uint32_t kG = 3u;
+constexpr int kQcThreads = 256;
+constexpr int kCW = 8;  // columns per CTA in the column passes
+
+__host__ __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) {
+  return uint32_t((uint64_t)a * b % kP);
+}
+__host__ __device__ inline uint32_t powmod(uint32_t b, uint64_t e) {
+  uint64_t r = 1, x = b;
+  while (e) {
+    if (e & 1) r = r * x % kP;
+    x = x * x % kP;
+    e >>= 1;
+  }
+  return uint32_t(r);
+}
+__host__ __device__ __forceinline__ uint2 shoup_pair(uint32_t w) {
+  return make_uint2(w, uint32_t((uint64_t(w) << 32) / kP));
+}
+// x * w mod p, result in [0, 2p), for any x < 2^32.
+__device__ __forceinline__ uint32_t shoup_mul(uint32_t x, uint2 w) {
+  const uint32_t q = __umulhi(x, w.y);
+  return x * w.x - q * kP;
+}
+__device__ __forceinline__ uint32_t red2p(uint32_t x) { return x >= 2 * kP ? x - 2 * kP : x; }
+__device__ __forceinline__ unsigned brev(unsigned x, int bits) { return __brev(x) >> (32 - bits); }
+
+// ---------------------------------------------------------------------------
+// In-shared-memory transforms over `rows` rows of length N = 2^lg at stride
+// `ld` words.  DIF forward: natural in, bit-reversed out.  DIT inverse:
+// bit-reversed in, natural out (unscaled).  Values in [0, 2p).
+__device__ void smem_dif(uint32_t *x, int rows, int lg, int ld, const uint2 *tw) {
+  const int N = 1 << lg, half = N >> 1;
+  for (int s = lg - 1; s >= 0; s--) {
+    const int len = 1 << s;
+    const int tstride = half >> s;  // N / (2 len)
+    for (int idx = threadIdx.x; idx < rows * half; idx += blockDim.x) {
+      const int row = idx >> (lg - 1), i = idx & (half - 1);
+      const int off = i & (len - 1), base = (i >> s) << (s + 1);
+      uint32_t *px = x + row * ld + base + off;
+      const uint32_t u = px[0], v = px[len];
+      px[0] = red2p(u + v);
+      px[len] = shoup_mul(u - v + 2 * kP, __ldg(&tw[off * tstride]));
+    }
+    __syncthreads();
+  }
+}
+
+__device__ void smem_dit(uint32_t *x, int rows, int lg, int ld, const uint2 *tw) {
+  const int N = 1 << lg, half = N >> 1;
+  for (int s = 0; s < lg; s++) {
+    const int len = 1 << s;
+    const int tstride = half >> s;
+    for (int idx = threadIdx.x; idx < rows * half; idx += blockDim.x) {
+      const int row = idx >> (lg - 1), i = idx & (half - 1);
+      const int off = i & (len - 1), base = (i >> s) << (s + 1);
+      uint32_t *px = x + row * ld + base + off;
+      const uint32_t u = px[0];
+      const uint32_t t = shoup_mul(px[len], __ldg(&tw[off * tstride]));
+      px[0] = red2p(u + t);
+      px[len] = red2p(u - t + 2 * kP);
+    }
+    __syncthreads();
+  }
+}
+
+// Pass A.  bits: plane-major, plane_words 32-bit words per plane.
+// grid (N2 / kCW, nplanes_batch).  Y: [plane][N1][N2].
+__global__ void __launch_bounds__(kQcThreads) qc_col_fwd(
+    const uint32_t *__restrict__ bits, uint64_t plane_words, int e1, int e2,
+    const uint2 *__restrict__ tw1f, const uint2 *__restrict__ fsf, uint32_t *__restrict__ Y) {
+  extern __shared__ uint32_t xs[];
+  const int N1 = 1 << e1, N2 = 1 << e2, ld = N1 + 1;
+  const int c0 = blockIdx.x * kCW;
+  const uint64_t plane = blockIdx.y;
+  const uint32_t *pb = bits + plane * plane_words;
+  for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
+    const uint64_t bit = uint64_t(j1) * N2 + c0;
+    const uint32_t w = __ldg(&pb[bit >> 5]) >> (bit & 31);
+#pragma unroll
+    for (int c = 0; c < kCW; c++) xs[c * ld + j1] = (w >> c) & 1u;
+  }
+  __syncthreads();
+  smem_dif(xs, kCW, e1, ld, tw1f);
+  uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
+  for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
+    const int r = idx / kCW, c = idx % kCW;
+    const uint64_t o = uint64_t(r) * N2 + c0 + c;
+    Yp[o] = shoup_mul(xs[c * ld + r], __ldg(&fsf[o]));
+  }
+}
+
+// Pass B.  grid (N1 / rows_per_cta, nplanes_batch).  mode 0: forward,
+// pointwise by ahat, inverse.  mode 1: forward only (used to build ahat).
+__global__ void __launch_bounds__(kQcThreads) qc_row(
+    uint32_t *__restrict__ Y, int e1, int e2, int rows_per_cta,
+    const uint2 *__restrict__ tw2f, const uint2 *__restrict__ tw2i,
+    const uint2 *__restrict__ ahat, int mode) {
+  extern __shared__ uint32_t xs[];
+  const int N1 = 1 << e1, N2 = 1 << e2;
+  const uint64_t plane = blockIdx.y;
+  const int r0 = blockIdx.x * rows_per_cta;
+  uint32_t *Yp = Y + (plane * N1 + r0) * uint64_t(N2);
+  const int cnt = rows_per_cta * N2;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[i] = Yp[i];
+  __syncthreads();
+  smem_dif(xs, rows_per_cta, e2, N2, tw2f);
+  if (mode == 0) {
+    const uint2 *ah = ahat + uint64_t(r0) * N2;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[i] = shoup_mul(xs[i], __ldg(&ah[i]));
+    __syncthreads();
+    smem_dit(xs, rows_per_cta, e2, N2, tw2i);
+  }
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) Yp[i] = xs[i];
+}
+
+// Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits.
+__global__ void __launch_bounds__(kQcThreads) qc_col_inv(
+    const uint32_t *__restrict__ Y, int e1, int e2, const uint2 *__restrict__ fsi,
+    const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes) {
+  extern __shared__ uint32_t xs[];
+  const int N1 = 1 << e1, N2 = 1 << e2, ld = N1 + 1;
+  const int c0 = blockIdx.x * kCW;
+  const uint64_t plane = blockIdx.y;
+  const uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
+  for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
+    const int r = idx / kCW, c = idx % kCW;
+    const uint64_t o = uint64_t(r) * N2 + c0 + c;
+    xs[c * ld + r] = shoup_mul(Yp[o], __ldg(&fsi[o]));
+  }
+  __syncthreads();
+  smem_dit(xs, kCW, e1, ld, tw1i);
+  uint8_t *ob = out + plane * plane_bytes;
+  for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
+    uint32_t byte = 0;
+#pragma unroll
+    for (int c = 0; c < kCW; c++) {
+      uint32_t v = xs[c * ld + j1];
+      v = v >= kP ? v - kP : v;  // exact coefficient in [0, n]
+      byte |= (v & 1u) << c;
+    }
+    ob[(uint64_t(j1) * N2 + c0) >> 3] = uint8_t(byte);
+  }
+}
+
+// Table generation (one-time per n).
+__global__ void qc_gen_twiddles(int lg, uint32_t root, uint2 *tw) {
+  const int half = 1 << (lg - 1);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < half; i += gridDim.x * blockDim.x)
+    tw[i] = shoup_pair(powmod(root, i));
+}
+__global__ void qc_gen_fourstep(int e1, int e2, uint32_t wn, uint2 *fs) {
+  const uint64_t n = 1ull << (e1 + e2);
+  const uint64_t N2 = 1ull << e2;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t r = i >> e2, j2 = i & (N2 - 1);
+    const uint64_t k1 = brev(unsigned(r), e1);
+    fs[i] = shoup_pair(powmod(wn, (j2 * k1) & (n - 1)));
+  }
+}
+// ahat[i] = pair(v * n^-1), from the forward transform of a.
+__global__ void qc_make_ahat(const uint32_t *v, uint64_t n, uint32_t ninv, uint2 *ahat) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t x = v[i] % kP;
+    ahat[i] = shoup_pair(mulmod(x, ninv));
+  }
+}
+
+// a = n bits of AES_key(make_block(i)): block i = (lo 4*floor(i/10), hi i%10).
+__global__ void qc_make_counters(Blk *b, uint64_t nb) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nb;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t lo = 4 * (i / 10), hi = i % 10;
+    b[i] = Blk{{uint32_t(lo), uint32_t(lo >> 32), uint32_t(hi), uint32_t(hi >> 32)}};
+  }
+}
+
+// Sparse encode: out = XOR_i rot(a, pos_i), one thread per output word.
+__global__ void qc_sparse(const uint64_t *__restrict__ a, const uint64_t *__restrict__ pos,
+                          int weight, uint64_t n, uint64_t *__restrict__ out) {
+  const uint64_t nw = n / 64;
+  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nw;
+       w += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t acc = 0;
+    for (int i = 0; i < weight; i++) {
+      const uint64_t p = __ldg(&pos[i]);
+      if (p >= n) continue;
+      const uint64_t ws = p >> 6, bs = p & 63;
+      // bit (64w + b) of rot(a, p) = bit (64w + b - p) mod n of a
+      const uint64_t src = (w + nw - ws) % nw;
+      uint64_t v = __ldg(&a[src]) << bs;
+      if (bs) v |= __ldg(&a[(src + nw - 1) % nw]) >> (64 - bs);
+      acc ^= v;
+    }
+    out[w] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+struct QcTables {
+  int e, e1, e2;
+  uint2 *tw1f, *tw1i, *tw2f, *tw2i, *fsf, *fsi;
+};
+
+static int split_e(int e, int *e1, int *e2) {
+  int a = e / 2;
+  if (a > 12) a = 12;
+  *e1 = a;
+  *e2 = e - a;
+  return CUOT_OK;
+}
+
+static int dev_alloc(void **p, size_t bytes) {
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ENOMEM, "QC table allocation of %zu bytes failed", bytes);
+  }
+  return CUOT_OK;
+}
+
+static void free_tables(QcTables *t) {
+  if (!t) return;
+  cudaFree(t->tw1f); cudaFree(t->tw1i); cudaFree(t->tw2f); cudaFree(t->tw2i);
+  cudaFree(t->fsf); cudaFree(t->fsi);
+  delete t;
+}
+
+// Builds (once per context and n) the twiddle tables.  Synchronises the
+// device the first time a size is used.
+static int get_tables(cuot_ctx *ctx, int e, QcTables **out) {
+  if (ctx->qc_tables[e]) {
+    *out = static_cast<QcTables *>(ctx->qc_tables[e]);
+    return CUOT_OK;
+  }
+  QcTables *t = new QcTables{};
+  t->e = e;
+  split_e(e, &t->e1, &t->e2);
+  const uint64_t n = 1ull << e, N1 = 1ull << t->e1, N2 = 1ull << t->e2;
+  int st = CUOT_OK;
+  if ((st = dev_alloc((void **)&t->tw1f, N1 / 2 * 8)) || (st = dev_alloc((void **)&t->tw1i, N1 / 2 * 8)) ||
+      (st = dev_alloc((void **)&t->tw2f, N2 / 2 * 8)) || (st = dev_alloc((void **)&t->tw2i, N2 / 2 * 8)) ||
+      (st = dev_alloc((void **)&t->fsf, n * 8)) || (st = dev_alloc((void **)&t->fsi, n * 8))) {
+    free_tables(t);
+    return st;
+  }
+  const uint32_t wn = powmod(kG, (kP - 1) >> e);
+  const uint32_t wni = powmod(wn, kP - 2);
+  const uint32_t w1 = powmod(wn, N2), w1i = powmod(w1, kP - 2);   // N1-th root
+  const uint32_t w2 = powmod(wn, N1), w2i = powmod(w2, kP - 2);   // N2-th root
+  qc_gen_twiddles<<<64, 256>>>(t->e1, w1, t->tw1f);
+  qc_gen_twiddles<<<64, 256>>>(t->e1, w1i, t->tw1i);
+  qc_gen_twiddles<<<64, 256>>>(t->e2, w2, t->tw2f);
+  qc_gen_twiddles<<<64, 256>>>(t->e2, w2i, t->tw2i);
+  qc_gen_fourstep<<<1024, 256>>>(t->e1, t->e2, wn, t->fsf);
+  qc_gen_fourstep<<<1024, 256>>>(t->e1, t->e2, wni, t->fsi);
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    free_tables(t);
+    return fail(CUOT_ECUDA, "QC table generation failed");
+  }
+  ctx->qc_tables[e] = t;
+  *out = t;
+  return CUOT_OK;
+}
+
+void qc_free_ctx_tables(cuot_ctx *ctx) {
+  for (int e = 0; e < 32; e++) {
+    free_tables(static_cast<QcTables *>(ctx->qc_tables[e]));
+    ctx->qc_tables[e] = nullptr;
+  }
+}
+
+static int col_smem(const QcTables *t) { return kCW * ((1 << t->e1) + 1) * 4; }
+static int row_rows(const QcTables *t) {
+  const int N2 = 1 << t->e2;
+  int r = 4096 / N2;
+  if (r < 1) r = 1;
+  if (r > (1 << t->e1)) r = 1 << t->e1;
+  return r;
+}
+static int row_smem(const QcTables *t) { return row_rows(t) * (1 << t->e2) * 4; }
+
+static int set_attrs(const QcTables *t) {
+  static bool done = false;
+  if (done) return CUOT_OK;
+  const int big = 200 * 1024;
+  if (cudaFuncSetAttribute(qc_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big) != cudaSuccess ||
+      cudaFuncSetAttribute(qc_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, big) != cudaSuccess ||
+      cudaFuncSetAttribute(qc_row, cudaFuncAttributeMaxDynamicSharedMemorySize, big) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "QC smem attribute failed");
+  }
+  done = true;
+  return CUOT_OK;
+}
+
+// Computes ahat (n Shoup pairs) from a (n bits) using Y (n words) as scratch.
+static int build_ahat(const QcTables *t, const uint64_t *a_d, uint32_t *Y, uint2 *ahat,
+                      cudaStream_t st) {
+  const int N1 = 1 << t->e1, N2 = 1 << t->e2;
+  const uint64_t n = 1ull << t->e;
+  qc_col_fwd<<<dim3(N2 / kCW, 1), kQcThreads, col_smem(t), st>>>(
+      reinterpret_cast<const uint32_t *>(a_d), n / 32, t->e1, t->e2, t->tw1f, t->fsf, Y);
+  qc_row<<<dim3(N1 / row_rows(t), 1), kQcThreads, row_smem(t), st>>>(
+      Y, t->e1, t->e2, row_rows(t), t->tw2f, t->tw2i, nullptr, 1);
+  const uint32_t ninv = powmod(uint32_t(n % kP), kP - 2);
+  qc_make_ahat<<<1024, 256, 0, st>>>(Y, n, ninv, ahat);
+  return launch_status(3);
+}
+
+// Encodes `nplanes` planes (n bits each, consecutive) in place, in batches.
+static int encode_planes(const QcTables *t, const uint2 *ahat, uint64_t *planes, int nplanes,
+                         uint32_t *Y, int batch, cudaStream_t st) {
+  const int N1 = 1 << t->e1, N2 = 1 << t->e2;
+  const uint64_t n = 1ull << t->e;
+  for (int p0 = 0; p0 < nplanes; p0 += batch) {
+    const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
+    uint64_t *pl = planes + uint64_t(p0) * (n / 64);
+    qc_col_fwd<<<dim3(N2 / kCW, nb), kQcThreads, col_smem(t), st>>>(
+        reinterpret_cast<const uint32_t *>(pl), n / 32, t->e1, t->e2, t->tw1f, t->fsf, Y);
+    qc_row<<<dim3(N1 / row_rows(t), nb), kQcThreads, row_smem(t), st>>>(
+        Y, t->e1, t->e2, row_rows(t), t->tw2f, t->tw2i, ahat, 0);
+    qc_col_inv<<<dim3(N2 / kCW, nb), kQcThreads, col_smem(t), st>>>(
+        Y, t->e1, t->e2, t->fsi, t->tw1i, reinterpret_cast<uint8_t *>(pl), n / 8);
+  }
+  return launch_status(3 * ((nplanes + batch - 1) / batch));
+}
+
+static int check_n(uint64_t n, int *e) {
+  if (n < 1024 || n > (1ull << 26) || (n & (n - 1)))
+    return fail(CUOT_EINVAL, "QC n=%llu must be a power of two in [2^10, 2^26]",
+                (unsigned long long)n);
+  *e = __builtin_ctzll(n);
+  return CUOT_OK;
+}
+
+// Planes per batch: keep the 4-byte intermediate near 64 MiB (L2-sized).
+static int default_batch(uint64_t n, int nplanes) {
+  uint64_t b = (64ull << 20) / (4 * n);
+  if (b < 1) b = 1;
+  if (b > uint64_t(nplanes)) b = nplanes;
+  return int(b);
+}
+
+int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
+                     uint64_t col_hi, void *out, cudaStream_t st);
+
+}  // namespace cuot
+
+using namespace cuot;
+
+struct cuot_qc_plan {
+  cuot_ctx *ctx;
+  int e;
+  uint64_t n;
+  uint2 *ahat;
+  int batch;
+};
+
+extern "C" {
+
+int cuot_qc_gen_a(cuot_ctx *ctx, const uint8_t key[16], uint64_t n, uint64_t *a_d, void *stream) {
+  if (!ctx || !key || !a_d) return fail(CUOT_EINVAL, "null argument");
+  if (n == 0 || n % 128) return fail(CUOT_EINVAL, "n=%llu must be a multiple of 128", (unsigned long long)n);
+  DeviceGuard g(ctx);
+  const uint64_t nb = n / 128;
+  qc_make_counters<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<Blk *>(a_d), nb);
+  CUOT_TRY(launch_status());
+  return cuot_aes128_ecb(ctx, key, reinterpret_cast<cuot_block *>(a_d), nb, stream);
+}
+
+int cuot_qc_plan_create(cuot_ctx *ctx, const uint64_t *a_d, uint64_t n, void *stream,
+                        cuot_qc_plan **out) {
+  if (!ctx || !a_d || !out) return fail(CUOT_EINVAL, "null argument");
+  *out = nullptr;
+  int e;
+  CUOT_TRY(check_n(n, &e));
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  CUOT_TRY(set_attrs(t));
+  cuot_qc_plan *pl = new cuot_qc_plan{ctx, e, n, nullptr, 0};
+  int st = dev_alloc((void **)&pl->ahat, n * 8);
+  if (st != CUOT_OK) { delete pl; return st; }
+  void *scr;
+  st = scratch(ctx, n * 4, &scr);
+  if (st == CUOT_OK)
+    st = build_ahat(t, a_d, static_cast<uint32_t *>(scr), pl->ahat, static_cast<cudaStream_t>(stream));
+  if (st != CUOT_OK) {
+    cudaFree(pl->ahat);
+    delete pl;
+    return st;
+  }
+  pl->batch = default_batch(n, 128);
+  *out = pl;
+  return CUOT_OK;
+}
+
+int cuot_qc_plan_destroy(cuot_qc_plan *pl) {
+  if (!pl) return CUOT_OK;
+  DeviceGuard g(pl->ctx);
+  cudaFree(pl->ahat);
+  delete pl;
+  return CUOT_OK;
+}
+
+int cuot_qc_plan_set_batch(cuot_qc_plan *pl, int planes_per_batch) {
+  if (!pl || planes_per_batch < 1) return fail(CUOT_EINVAL, "bad batch");
+  pl->batch = planes_per_batch;
+  return CUOT_OK;
+}
+
+int cuot_qc_plan_encode(cuot_qc_plan *pl, uint64_t *planes_io_d, int nplanes, void *stream) {
+  if (!pl || !planes_io_d || nplanes < 1) return fail(CUOT_EINVAL, "bad argument");
+  cuot_ctx *ctx = pl->ctx;
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, pl->e, &t));
+  const int batch = pl->batch < nplanes ? pl->batch : nplanes;
+  void *scr;
+  CUOT_TRY(scratch(ctx, uint64_t(batch) * pl->n * 4, &scr));
+  return encode_planes(t, pl->ahat, planes_io_d, nplanes, static_cast<uint32_t *>(scr), batch,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int cuot_qc_plan_dual_lpn(cuot_qc_plan *pl, cuot_block *io_d, void *stream) {
+  if (!pl || !io_d) return fail(CUOT_EINVAL, "bad argument");
+  cuot_ctx *ctx = pl->ctx;
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, pl->e, &t));
+  const uint64_t n = pl->n;
+  const int batch = pl->batch < 128 ? pl->batch : 128;
+  void *scr;
+  CUOT_TRY(scratch(ctx, n * 16 + uint64_t(batch) * n * 4, &scr));
+  uint8_t *planes = static_cast<uint8_t *>(scr);
+  uint32_t *Y = reinterpret_cast<uint32_t *>(planes + n * 16);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
+  CUOT_TRY(encode_planes(t, pl->ahat, reinterpret_cast<uint64_t *>(planes), 128, Y, batch, st));
+  return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
+}
+
+int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, uint64_t n,
+                   int nplanes, void *stream) {
+  if (!ctx || !a_d || !planes_io_d || nplanes < 1) return fail(CUOT_EINVAL, "bad argument");
+  int e;
+  CUOT_TRY(check_n(n, &e));
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  CUOT_TRY(set_attrs(t));
+  const int batch = default_batch(n, nplanes);
+  void *scr;
+  CUOT_TRY(scratch(ctx, n * 8 + uint64_t(batch) * n * 4, &scr));
+  uint2 *ahat = static_cast<uint2 *>(scr);
+  uint32_t *Y = reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(scr) + n * 8);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUOT_TRY(build_ahat(t, a_d, Y, ahat, st));
+  return encode_planes(t, ahat, planes_io_d, nplanes, Y, batch, st);
+}
+
+int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d, uint64_t n,
+                      void *stream) {
+  if (!ctx || !a_d || !io_d) return fail(CUOT_EINVAL, "bad argument");
+  int e;
+  CUOT_TRY(check_n(n, &e));
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  CUOT_TRY(set_attrs(t));
+  const int batch = default_batch(n, 128);
+  void *scr;
+  CUOT_TRY(scratch(ctx, n * 8 + n * 16 + uint64_t(batch) * n * 4, &scr));
+  uint2 *ahat = static_cast<uint2 *>(scr);
+  uint8_t *planes = static_cast<uint8_t *>(scr) + n * 8;
+  uint32_t *Y = reinterpret_cast<uint32_t *>(planes + n * 16);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUOT_TRY(build_ahat(t, a_d, Y, ahat, st));
+  CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
+  CUOT_TRY(encode_planes(t, ahat, reinterpret_cast<uint64_t *>(planes), 128, Y, batch, st));
+  return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
+}
+
+int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *pos_d, int weight,
+                          uint64_t n, uint64_t *out_d, void *stream) {
+  if (!ctx || !a_d || !out_d || (weight > 0 && !pos_d) || weight < 0)
+    return fail(CUOT_EINVAL, "bad argument");
+  if (n == 0 || n % 64) return fail(CUOT_EINVAL, "n must be a positive multiple of 64");
+  DeviceGuard g(ctx);
+  qc_sparse<<<1024, 256, 0, static_cast<cudaStream_t>(stream)>>>(a_d, pos_d, weight, n, out_d);
+  return launch_status();
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+/*
+ * cuot.h -- C ABI of libcuot, a B200 (sm_100a) silent-OT correlation engine.
+ *
+ * Drop-in boundary for cuOT's hot path (GGM PPRF expansion -> Ferret primal
+ * LPN or SOT quasi-cyclic encode -> 128-plane bit transpose).  Plain C types
+ * only: device pointers, sizes, an opaque context and a cudaStream_t passed
+ * as void*.  Every call is stream-ordered, returns a status code, and never
+ * synchronises the device unless its comment says so.
+ *
+ * Blocks are 16 bytes with the memory image of emp-tool's `block` and cuOT's
+ * `blk` (gpu/gpu_define.h:12-16).  Bit vectors are little-endian: bit j of a
+ * vector is bit (j % 8) of byte j / 8.
+ *
+ * The C++ adapter with the reference's own dev_layer.h signatures is in
+ * include/cuot_dev_layer.h.
+ */
+#ifndef CUOT_H
+#define CUOT_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CUOT_OK 0
+#define CUOT_EINVAL 1   /* bad argument (shape, alignment, null pointer) */
+#define CUOT_ENOMEM 2   /* device allocation failed */
+#define CUOT_ECUDA 3    /* a CUDA launch or runtime call failed */
+#define CUOT_ETIMEOUT 4 /* a bounded device or host wait ran out */
+#define CUOT_ENOTSUP 5  /* shape or mode this build does not support */
+
+typedef struct { uint32_t w[4]; } cuot_block;
+typedef struct cuot_ctx cuot_ctx;
+
+const char *cuot_version(void);
+const char *cuot_status_string(int status);
+/* Detail of the last failure on the calling thread ("" if none). */
+const char *cuot_last_error(void);
+/* Number of kernels this library has launched in the process (diagnostic). */
+unsigned long long cuot_launch_count(void);
+
+/* ---- context -------------------------------------------------------------
+ * A context binds one CUDA device, its AES tables and a grow-only scratch
+ * arena.  Replaces the per-call Aes / Mat set-up of the reference
+ * (gpu/aes_expand.cu:18-30, gpu/gpu_data.cu:7-15). */
+int cuot_ctx_create(int device, cuot_ctx **out);
+int cuot_ctx_destroy(cuot_ctx *ctx);
+/* Pre-size the scratch arena (call before capturing a CUDA graph). */
+int cuot_ctx_reserve(cuot_ctx *ctx, uint64_t bytes);
+uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
+
+/* ---- AES-128 ECB ---------------------------------------------------------
+ * In-place FIPS-197 AES-128 of `nblocks` blocks under `key` (host, 16 bytes).
+ * Replaces Aes::encrypt / aesEncrypt128 (gpu/aes_expand.cu:32-36,
+ * gpu/aes_op.cu:90-174); unlike the reference it uses the standard key
+ * schedule (the reference XORs Rcon[i-1], gpu/aes_expand.cu:59). */
+int cuot_aes128_ecb(cuot_ctx *ctx, const uint8_t key[16], cuot_block *io_d,
+                    uint64_t nblocks, void *stream);
+
+/* ---- Ferret MPCOT: t GGM trees of depth h --------------------------------
+ * Node function: emp-ot TwoKeyPRP (ferret/twokeyprp.h:7-63): left =
+ * AES_0(p) ^ p, right = AES_{makeBlock(0,1)}(p) ^ p.
+ *
+ * Sender (replaces cuda_mpcot_sender, dev_layer.cu:20-59; semantics of
+ * SPCOT_Sender::ggm_tree_gen, spcot_sender.h:47-86):
+ *   roots_d        [t]            tree roots
+ *   delta          host pointer to the correlation delta
+ *   leaves_d       [t][2^h]       out: leaves with the LSB cleared
+ *   lsum_d, rsum_d [t][h]         out: XOR of even / odd children per level
+ *   secret_sum_d   [t]            out: XOR(leaves) ^ delta
+ * Receiver (replaces cuda_mpcot_recver, dev_layer.cu:87-144; semantics of
+ * SPCOT_Recver, spcot_recver.h:33-95):
+ *   mc_d           [t][h]         chosen OT messages (ot_msg_{b})
+ *   choice_d       [t][h] bytes   b = 0 punctures the right child
+ *   secret_sum_d   [t]            the sender's secret sums
+ *   leaves_d       [t][2^h]       out: sender leaves, except the punctured
+ *                                 leaf = sender leaf ^ delta
+ * h in [1, 30]; t >= 1. */
+int cuot_ferret_pprf_sender(cuot_ctx *ctx, const cuot_block *roots_d,
+                            uint64_t t, int h, const cuot_block *delta,
+                            cuot_block *leaves_d, cuot_block *lsum_d,
+                            cuot_block *rsum_d, cuot_block *secret_sum_d,
+                            void *stream);
+int cuot_ferret_pprf_recver(cuot_ctx *ctx, const cuot_block *mc_d,
+                            const uint8_t *choice_d,
+                            const cuot_block *secret_sum_d, uint64_t t, int h,
+                            cuot_block *leaves_d, void *stream);
+
+/* ---- Ferret primal LPN -----------------------------------------------------
+ * e_io_d[i] ^= XOR_{j<d} kk_d[idx(i, j)] for i < n, with the index matrix of
+ * emp-ot LpnF2::task over [0, n) (lpn_f2.h:46-79) under AES key `seed`.
+ * Replaces cuda_primal_lpn (dev_layer.cu:161-186).  1 <= d <= 32,
+ * 1 <= k < 2^31. */
+int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16],
+                    const cuot_block *kk_d, int64_t k, int d,
+                    cuot_block *e_io_d, int64_t n, void *stream);
+
+/* ---- SOT PPRF ----------------------------------------------------------------
+ * Structure of SOTSender/SOTRecver::seed_expand (silent/sender.cu:76-108,
+ * silent/recver.cu:124-163) with the emp-ot node function above.
+ * Sender: base0_d/base1_d [h][t] base-OT messages; out m0_d/m1_d [h+1][t]:
+ *   m0[d] = base0[d] ^ L_d, m1[d] = base1[d] ^ R_d (d < h),
+ *   m0[h] = base0[h-1] ^ R_{h-1} ^ delta, m1[h] = base1[h-1] ^ L_{h-1} ^ delta.
+ * Receiver: mc_d [h][t] chosen base-OT messages, choice_d [h][t] bytes;
+ *   out leaves = sender leaves except the punctured one = sender leaf ^ delta.
+ */
+int cuot_sot_pprf_sender(cuot_ctx *ctx, const cuot_block *roots_d, uint64_t t,
+                         int h, const cuot_block *delta,
+                         const cuot_block *base0_d, const cuot_block *base1_d,
+                         cuot_block *leaves_d, cuot_block *m0_d,
+                         cuot_block *m1_d, void *stream);
+int cuot_sot_pprf_recver(cuot_ctx *ctx, const cuot_block *m0_d,
+                         const cuot_block *m1_d, const cuot_block *mc_d,
+                         const uint8_t *choice_d, uint64_t t, int h,
+                         cuot_block *leaves_d, void *stream);
+
+/* ---- bit transpose -----------------------------------------------------------
+ * Mat::bit_transpose (gpu/gpu_matrix.cu:95-121): input `rows` rows of
+ * `row_bytes` bytes; output row (c - col_lo) bit r = input row r bit c for
+ * c in [col_lo, col_hi).  Output rows are rows/8 bytes.  rows % 8 == 0,
+ * col_lo % 8 == 0, col_hi % 8 == 0, col_hi <= 8 * row_bytes. */
+int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
+                       uint64_t row_bytes, uint64_t col_lo, uint64_t col_hi,
+                       void *out_d, void *stream);
+
+/* ---- SOT quasi-cyclic dual LPN ------------------------------------------------
+ * a = n bits of AES_key(make_block counters) (silent/quasi_cyclic.cu:57-66,
+ * gpu/gpu_ops.cu:102-109).  encode: every plane r (n bits, planes
+ * consecutive) becomes a * plane_r mod (x^n - 1) over GF(2), exactly
+ * (replaces the float cuFFT path of QuasiCyclic::encode_dense,
+ * quasi_cyclic.cu:118-128).  n a power of two in [2^10, 2^26].
+ * encode_sparse: out = a * e mod (x^n - 1), e = indicator of pos_d[0..w)
+ * (QuasiCyclic::encode_sparse, quasi_cyclic.cu:130-161).
+ * dual_lpn: io_d holds n blocks; block j becomes XOR_{i: a_i = 1}
+ * io[(j - i) mod n], i.e. transpose -> encode 128 planes -> transpose back
+ * (SOTSender::dual_lpn, silent/sender.cu:110-119). */
+int cuot_qc_gen_a(cuot_ctx *ctx, const uint8_t key[16], uint64_t n,
+                  uint64_t *a_d, void *stream);
+int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d,
+                   uint64_t n, int nplanes, void *stream);
+int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d,
+                          const uint64_t *pos_d, int weight, uint64_t n,
+                          uint64_t *out_d, void *stream);
+int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d,
+                      uint64_t n, void *stream);
+
+/* QC plan: the counterpart of the QuasiCyclic object (quasi_cyclic.h:8-26,
+ * ctor quasi_cyclic.cu:51-106), which transforms `a` once and reuses it for
+ * every encode.  plan_create transforms a_d (n bits) on `stream` and keeps
+ * the transform in its own device buffer; the twiddle tables are cached in
+ * the context (the first use of a size synchronises the device).
+ * plan_encode / plan_dual_lpn do what cuot_qc_encode / cuot_sot_dual_lpn do
+ * without re-transforming `a`.  set_batch bounds how many planes share one
+ * intermediate pass (4 bytes per coefficient per plane of scratch). */
+typedef struct cuot_qc_plan cuot_qc_plan;
+int cuot_qc_plan_create(cuot_ctx *ctx, const uint64_t *a_d, uint64_t n,
+                        void *stream, cuot_qc_plan **out);
+int cuot_qc_plan_destroy(cuot_qc_plan *plan);
+int cuot_qc_plan_set_batch(cuot_qc_plan *plan, int planes_per_batch);
+int cuot_qc_plan_encode(cuot_qc_plan *plan, uint64_t *planes_io_d,
+                        int nplanes, void *stream);
+int cuot_qc_plan_dual_lpn(cuot_qc_plan *plan, cuot_block *io_d, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUOT_H */

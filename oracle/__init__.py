@@ -1,0 +1,199 @@
+"""CPU oracle for the silent-OT hot path -- TEST INFRASTRUCTURE ONLY.
+
+Loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline
+and reference legs as the checker.  The product (cuot_b200, libcuot.so) never
+imports this package.  Arrays are numpy; blocks are uint8 arrays of shape
+(..., 16) with the memory image of emp-tool's `block`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            import subprocess
+            subprocess.check_call(["make", "-s", "-C", _HERE])
+        _LIB = ctypes.CDLL(path)
+    return _LIB
+
+
+def ref_lib():
+    """oracle/_ref/libctref.so (reference cryptoTools, built from the
+    reference sources) or None when it was not built."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(_HERE, "_ref", "libctref.so")
+        if not os.path.exists(path):
+            return None
+        _REF = ctypes.CDLL(path)
+    return _REF
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _u8(a) -> np.ndarray:
+    return np.ascontiguousarray(np.frombuffer(bytes(a), dtype=np.uint8)) if isinstance(a, (bytes, bytearray)) else np.ascontiguousarray(a, dtype=np.uint8)
+
+
+C = ctypes
+I64, U64, SZ, INT = C.c_int64, C.c_uint64, C.c_size_t, C.c_int
+
+
+def aes_key_expand(key) -> np.ndarray:
+    rk = np.zeros(176, np.uint8)
+    lib().or_aes128_key_expand(_p(_u8(key)), _p(rk))
+    return rk
+
+
+def aes_ecb(key, blocks: np.ndarray, portable: bool = False) -> np.ndarray:
+    rk = aes_key_expand(key)
+    inp = np.ascontiguousarray(blocks, dtype=np.uint8).reshape(-1, 16)
+    out = np.empty_like(inp)
+    f = lib().or_aes128_encrypt_portable if portable else lib().or_aes128_encrypt
+    f(_p(rk), _p(inp), _p(out), SZ(inp.shape[0]))
+    return out
+
+
+def prg(seed, nblocks: int, offset: int = 0) -> np.ndarray:
+    out = np.empty((nblocks, 16), np.uint8)
+    lib().or_prg_fill(_p(_u8(seed)), U64(offset), _p(out), SZ(nblocks))
+    return out
+
+
+def ferret_pprf_sender(roots, h: int, delta, threads: int = 1):
+    roots = np.ascontiguousarray(roots, np.uint8).reshape(-1, 16)
+    t = roots.shape[0]
+    leaves = np.empty((t << h, 16), np.uint8)
+    lsum = np.empty((t * h, 16), np.uint8)
+    rsum = np.empty((t * h, 16), np.uint8)
+    ss = np.empty((t, 16), np.uint8)
+    d = _u8(delta)
+    lib().or_ferret_pprf_sender(_p(roots), I64(t), INT(h), *_blk_by_value(d), _p(leaves),
+                                _p(lsum), _p(rsum), _p(ss), INT(threads))
+    return leaves, lsum, rsum, ss
+
+
+class _Blk(C.Structure):
+    _fields_ = [("lo", C.c_uint64), ("hi", C.c_uint64)]
+
+
+def _blk_by_value(b: np.ndarray):
+    b = _u8(b)
+    return (_Blk(int.from_bytes(b[:8].tobytes(), "little"), int.from_bytes(b[8:16].tobytes(), "little")),)
+
+
+def ferret_pprf_recver(mc, choice, secret_sum, h: int, threads: int = 1):
+    mc = np.ascontiguousarray(mc, np.uint8).reshape(-1, 16)
+    ss = np.ascontiguousarray(secret_sum, np.uint8).reshape(-1, 16)
+    t = ss.shape[0]
+    ch = np.ascontiguousarray(choice, np.uint8).reshape(-1)
+    assert mc.shape[0] == t * h and ch.shape[0] == t * h
+    leaves = np.empty((t << h, 16), np.uint8)
+    lib().or_ferret_pprf_recver(_p(mc), _p(ch), _p(ss), I64(t), INT(h), _p(leaves), INT(threads))
+    return leaves
+
+
+def lpn_primal(seed, kk, nn, d: int = 10, threads: int = 1) -> np.ndarray:
+    kk = np.ascontiguousarray(kk, np.uint8).reshape(-1, 16)
+    out = np.array(nn, dtype=np.uint8, copy=True).reshape(-1, 16)
+    lib().or_lpn_primal(_p(_u8(seed)), _p(kk), I64(kk.shape[0]), INT(d), _p(out),
+                        I64(out.shape[0]), INT(threads))
+    return out
+
+
+def bit_transpose(inp: np.ndarray, rows: int, row_bytes: int, col_lo: int, col_hi: int) -> np.ndarray:
+    inp = np.ascontiguousarray(inp, np.uint8).reshape(-1)
+    out = np.empty((col_hi - col_lo) * (rows // 8), np.uint8)
+    lib().or_bit_transpose(_p(inp), U64(rows), U64(row_bytes), U64(col_lo), U64(col_hi), _p(out))
+    return out
+
+
+def qc_gen_a(key, n: int) -> np.ndarray:
+    a = np.zeros(n // 64, np.uint64)
+    lib().or_qc_gen_a(_p(_u8(key)), U64(n), _p(a))
+    return a
+
+
+def gf2_cyclic_mul(a: np.ndarray, b: np.ndarray, n: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.uint64)
+    b = np.ascontiguousarray(b, np.uint64)
+    out = np.empty(n // 64, np.uint64)
+    lib().or_gf2_cyclic_mul(_p(a), _p(b), U64(n), _p(out))
+    return out
+
+
+def qc_encode(a: np.ndarray, planes: np.ndarray, n: int, threads: int = 1) -> np.ndarray:
+    out = np.array(planes, dtype=np.uint64, copy=True).reshape(-1)
+    npl = out.shape[0] // (n // 64)
+    lib().or_qc_encode(_p(np.ascontiguousarray(a, np.uint64)), _p(out), U64(n), INT(npl), INT(threads))
+    return out.reshape(npl, n // 64)
+
+
+def qc_encode_sparse(a: np.ndarray, pos, n: int) -> np.ndarray:
+    pos = np.ascontiguousarray(pos, np.uint64)
+    out = np.empty(n // 64, np.uint64)
+    lib().or_qc_encode_sparse(_p(np.ascontiguousarray(a, np.uint64)), _p(pos), INT(pos.shape[0]),
+                              U64(n), _p(out))
+    return out
+
+
+def sot_dual_lpn(a: np.ndarray, io: np.ndarray, n: int, threads: int = 1) -> np.ndarray:
+    out = np.array(io, dtype=np.uint8, copy=True).reshape(n, 16)
+    lib().or_sot_dual_lpn(_p(np.ascontiguousarray(a, np.uint64)), _p(out), U64(n), INT(threads))
+    return out
+
+
+def sot_pprf_sender(roots, h: int, delta, base0, base1, threads: int = 1):
+    roots = np.ascontiguousarray(roots, np.uint8).reshape(-1, 16)
+    t = roots.shape[0]
+    b0 = np.ascontiguousarray(base0, np.uint8).reshape(h * t, 16)
+    b1 = np.ascontiguousarray(base1, np.uint8).reshape(h * t, 16)
+    leaves = np.empty((t << h, 16), np.uint8)
+    m0 = np.empty(((h + 1) * t, 16), np.uint8)
+    m1 = np.empty(((h + 1) * t, 16), np.uint8)
+    lib().or_sot_pprf_sender(_p(roots), I64(t), INT(h), *_blk_by_value(_u8(delta)), _p(b0), _p(b1),
+                             _p(leaves), _p(m0), _p(m1), INT(threads))
+    return leaves, m0, m1
+
+
+def sot_pprf_recver(m0, m1, mc, choice, t: int, h: int, threads: int = 1):
+    m0 = np.ascontiguousarray(m0, np.uint8).reshape((h + 1) * t, 16)
+    m1 = np.ascontiguousarray(m1, np.uint8).reshape((h + 1) * t, 16)
+    mc = np.ascontiguousarray(mc, np.uint8).reshape(h * t, 16)
+    ch = np.ascontiguousarray(choice, np.uint8).reshape(h * t)
+    leaves = np.empty((t << h, 16), np.uint8)
+    lib().or_sot_pprf_recver(_p(m0), _p(m1), _p(mc), _p(ch), I64(t), INT(h), _p(leaves), INT(threads))
+    return leaves
+
+
+def ref_aes_ecb(key, blocks: np.ndarray):
+    r = ref_lib()
+    if r is None:
+        return None
+    inp = np.ascontiguousarray(blocks, np.uint8).reshape(-1, 16)
+    out = np.empty_like(inp)
+    r.ref_aes_ecb(_p(_u8(key)), _p(inp), _p(out), C.c_ulonglong(inp.shape[0]))
+    return out
+
+
+def ref_prng(seed, nblocks: int):
+    r = ref_lib()
+    if r is None:
+        return None
+    out = np.empty((nblocks, 16), np.uint8)
+    r.ref_prng(_p(_u8(seed)), _p(out), C.c_ulonglong(nblocks))
+    return out

@@ -1,0 +1,81 @@
+/*
+ * cuot_oracle.h -- CPU oracle for the silent-OT hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the cuot_b200 package,
+ * libcuot.so, the C ABI in include/) links, loads or calls this code.  It is
+ * loaded by tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline
+ * and reference legs, where it is the checker (or the timed CPU baseline),
+ * never the thing measured on the GPU.
+ *
+ * Every routine restates the reference's CPU semantics for one step of the
+ * path (emp-ot / cryptoTools, FIPS-197 AES), citing the reference file:line it
+ * follows.  Blocks are 16 bytes with the same memory image as emp-tool's
+ * `block` (__m128i; makeBlock(hi, lo) puts `lo` in bytes 0..7) and cuOT's
+ * `blk` (4 x uint32, gpu/gpu_define.h:12-16).
+ */
+#ifndef CUOT_ORACLE_H
+#define CUOT_ORACLE_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { uint64_t lo, hi; } or_block;
+
+/* ---- AES-128 (FIPS-197) ------------------------------------------------ */
+void or_aes128_key_expand(const uint8_t key[16], uint8_t rk[176]);
+void or_aes128_encrypt(const uint8_t rk[176], const uint8_t *in, uint8_t *out,
+                       size_t nblocks);
+/* Portable (table-free, byte-wise) encryption, used to cross-check the
+ * AES-NI path. */
+void or_aes128_encrypt_portable(const uint8_t rk[176], const uint8_t *in,
+                                uint8_t *out, size_t nblocks);
+int or_have_aesni(void);
+
+/* ---- seeded host PRG (cryptoTools PRNG restated) ------------------------ */
+void or_prg_fill(const uint8_t seed[16], uint64_t block_offset, uint8_t *out,
+                 size_t nblocks);
+
+/* ---- Ferret GGM (emp-ot SPCOT sender/receiver) --------------------------- */
+void or_ggm_node(const or_block *parent, or_block *left, or_block *right);
+void or_ferret_pprf_sender(const or_block *roots, int64_t t, int h,
+                           or_block delta, or_block *leaves, or_block *lsum,
+                           or_block *rsum, or_block *secret_sum, int threads);
+void or_ferret_pprf_recver(const or_block *mc, const uint8_t *choice,
+                           const or_block *secret_sum, int64_t t, int h,
+                           or_block *leaves, int threads);
+
+/* ---- Ferret primal LPN (emp-ot LpnF2::task over [0, n)) ----------------- */
+void or_lpn_primal(const uint8_t seed[16], const or_block *kk, int64_t k,
+                   int d, or_block *nn, int64_t n, int threads);
+
+/* ---- bit transpose (cuOT bit_transposer semantics) ---------------------- */
+void or_bit_transpose(const uint8_t *in, uint64_t rows, uint64_t row_bytes,
+                      uint64_t col_lo, uint64_t col_hi, uint8_t *out);
+
+/* ---- SOT quasi-cyclic dual LPN ------------------------------------------ */
+void or_qc_gen_a(const uint8_t key[16], uint64_t n, uint64_t *a);
+void or_gf2_cyclic_mul(const uint64_t *a, const uint64_t *b, uint64_t n,
+                       uint64_t *out);
+void or_qc_encode(const uint64_t *a, uint64_t *planes, uint64_t n, int nplanes,
+                  int threads);
+void or_qc_encode_sparse(const uint64_t *a, const uint64_t *pos, int weight,
+                         uint64_t n, uint64_t *out);
+void or_sot_dual_lpn(const uint64_t *a, or_block *io, uint64_t n,
+                     int threads);
+
+/* ---- SOT PPRF (silent/sender.cu, silent/recver.cu structure) ------------ */
+void or_sot_pprf_sender(const or_block *roots, int64_t t, int h,
+                        or_block delta, const or_block *base0,
+                        const or_block *base1, or_block *leaves, or_block *m0,
+                        or_block *m1, int threads);
+void or_sot_pprf_recver(const or_block *m0, const or_block *m1,
+                        const or_block *mc, const uint8_t *choice, int64_t t,
+                        int h, or_block *leaves, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,289 @@
+"""GPU parity tests: every CUDA entry point, called through the C ABI, is
+bit-exact against the CPU oracle on seeded inputs and against the golden
+fixtures; full-size configurations are checked through size-independent
+properties (COT correlation, sender/receiver agreement, linearity)."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.util import blocks, hx, rng_blocks, delta_ferret, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def empty_blocks(n):
+    return torch.empty((n, 16), dtype=torch.uint8, device="cuda")
+
+
+# ---------------------------------------------------------------- AES
+@pytest.mark.parametrize("n", [1, 2, 3, 255, 4096, 100003])
+def test_aes_ecb(ctx, n):
+    rng = np.random.default_rng(n)
+    key, pt = rng_blocks(rng, 1)[0], rng_blocks(rng, n)
+    d = to_dev(pt)
+    ctx.aes128_ecb(key, d)
+    assert np.array_equal(to_host(d), oracle.aes_ecb(key, pt))
+
+
+def test_aes_golden(ctx, golden):
+    for c in golden["aes"]:
+        d = to_dev(blocks(c["pt"]))
+        ctx.aes128_ecb(hx(c["key"]), d)
+        assert to_host(d).tobytes().hex() == c["ct"]
+
+
+# ---------------------------------------------------------------- Ferret GGM
+def run_ferret_sender(ctx, roots, h, delta):
+    t = roots.shape[0]
+    leaves, lsum, rsum, ss = empty_blocks(t << h), empty_blocks(t * h), empty_blocks(t * h), empty_blocks(t)
+    ctx.ferret_pprf_sender(to_dev(roots), h, delta, leaves, lsum, rsum, ss)
+    return to_host(leaves), to_host(lsum), to_host(rsum), to_host(ss)
+
+
+def run_ferret_recver(ctx, mc, choice, ss, h):
+    t = ss.shape[0]
+    leaves = empty_blocks(t << h)
+    ctx.ferret_pprf_recver(to_dev(mc), to_dev(choice), to_dev(ss), h, leaves)
+    return to_host(leaves)
+
+
+def test_ferret_ggm_golden(ctx, golden):
+    for c in golden["ferret_ggm"]:
+        h = c["h"]
+        lv, ls, rs, ss = run_ferret_sender(ctx, blocks(c["roots"]), h, hx(c["delta"]))
+        assert lv.tobytes().hex() == c["leaves"]
+        assert ls.tobytes().hex() == c["lsum"]
+        assert rs.tobytes().hex() == c["rsum"]
+        assert ss.tobytes().hex() == c["secret_sum"]
+        ch = np.array(c["choice"], np.uint8)
+        mc = np.where(ch[:, None] == 0, ls, rs)
+        assert run_ferret_recver(ctx, mc, ch, ss, h).tobytes().hex() == c["recv_leaves"]
+
+
+@pytest.mark.parametrize("t,h", [(1, 1), (5, 2), (3, 7), (64, 10), (7, 13), (2, 16), (300, 9)])
+def test_ferret_ggm_vs_oracle(ctx, t, h):
+    rng = np.random.default_rng(1000 * t + h)
+    roots, delta = rng_blocks(rng, t), delta_ferret(rng)
+    got = run_ferret_sender(ctx, roots, h, delta)
+    exp = oracle.ferret_pprf_sender(roots, h, delta, threads=8)
+    for g, e in zip(got, exp):
+        assert np.array_equal(g, e)
+    ch = rng.integers(0, 2, t * h).astype(np.uint8)
+    mc = np.where(ch[:, None] == 0, exp[1], exp[2])
+    gr = run_ferret_recver(ctx, mc, ch, exp[3], h)
+    er = oracle.ferret_pprf_recver(mc, ch, exp[3], h, threads=8)
+    assert np.array_equal(gr, er)
+
+
+def test_ferret_full_size_b13(ctx):
+    """ferret_b13 (constants.h:25): t = 1280 trees of depth 13, bit-exact
+    against the multi-threaded oracle, plus the COT correlation."""
+    t, h = 1280, 13
+    rng = np.random.default_rng(13)
+    roots, delta = rng_blocks(rng, t), delta_ferret(rng)
+    got = run_ferret_sender(ctx, roots, h, delta)
+    exp = oracle.ferret_pprf_sender(roots, h, delta, threads=16)
+    for g, e in zip(got, exp):
+        assert np.array_equal(g, e)
+    ch = rng.integers(0, 2, t * h).astype(np.uint8)
+    mc = np.where(ch[:, None] == 0, exp[1], exp[2])
+    gr = run_ferret_recver(ctx, mc, ch, exp[3], h)
+    diff = gr ^ exp[0]
+    rows = np.nonzero(diff.any(axis=1))[0]
+    assert rows.shape[0] == t
+    assert (diff[rows] == delta).all()
+
+
+# ---------------------------------------------------------------- LPN
+def test_lpn_golden(ctx, golden):
+    for c in golden["lpn"]:
+        e = to_dev(blocks(c["e"]))
+        ctx.lpn_primal(hx(c["seed"]), to_dev(blocks(c["kk"])), e, d=c["d"])
+        assert to_host(e).tobytes().hex() == c["out"], (c["n"], c["k"], c["d"])
+
+
+@pytest.mark.parametrize("n,k,d", [(65536, 8192, 10), (1000, 999, 10), (12345, 4097, 10),
+                                   (9999, 511, 3), (777, 65, 16), (6, 2, 10)])
+def test_lpn_vs_oracle(ctx, n, k, d):
+    rng = np.random.default_rng(n + k + d)
+    seed, kk, e = rng_blocks(rng, 1)[0], rng_blocks(rng, k), rng_blocks(rng, n)
+    dev = to_dev(e)
+    ctx.lpn_primal(seed, to_dev(kk), dev, d=d)
+    assert np.array_equal(to_host(dev), oracle.lpn_primal(seed, kk, e, d=d, threads=8))
+
+
+def test_lpn_full_size_b13(ctx):
+    n, k = 10485760, 452000
+    rng = np.random.default_rng(452)
+    seed, kk, e = rng_blocks(rng, 1)[0], rng_blocks(rng, k), rng_blocks(rng, n)
+    dev = to_dev(e)
+    ctx.lpn_primal(seed, to_dev(kk), dev)
+    assert np.array_equal(to_host(dev), oracle.lpn_primal(seed, kk, e, threads=16))
+
+
+# ---------------------------------------------------------------- transpose
+def test_transpose_golden(ctx, golden):
+    for c in golden["transpose"]:
+        rows, rb, lo, hi = c["rows"], c["row_bytes"], c["lo"], c["hi"]
+        out = torch.empty((hi - lo) * rows // 8, dtype=torch.uint8, device="cuda")
+        ctx.bit_transpose(to_dev(hx(c["in"])), rows, rb, lo, hi, out)
+        assert to_host(out).tobytes().hex() == c["out"]
+
+
+@pytest.mark.parametrize("rows,rb,lo,hi", [(1 << 20, 16, 0, 128), (4096 + 32 * 5, 16, 32, 96),
+                                           (128, 1 << 14, 0, 1 << 17), (64, 1024, 0, 8192),
+                                           (96, 40, 16, 320), (8, 1, 0, 8)])
+def test_transpose_vs_oracle(ctx, rows, rb, lo, hi):
+    rng = np.random.default_rng(rows + rb)
+    m = rng.integers(0, 256, rows * rb, dtype=np.uint8)
+    out = torch.empty((hi - lo) * rows // 8, dtype=torch.uint8, device="cuda")
+    ctx.bit_transpose(to_dev(m), rows, rb, lo, hi, out)
+    exp = np.unpackbits(m.reshape(rows, rb), axis=1, bitorder="little")[:, lo:hi].T
+    exp = np.packbits(np.ascontiguousarray(exp), axis=1, bitorder="little").reshape(-1)
+    assert np.array_equal(to_host(out), exp)
+
+
+# ---------------------------------------------------------------- QC
+def test_qc_golden(ctx, golden):
+    for c in golden["qc"]:
+        n = c["n"]
+        a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+        ctx.qc_gen_a(hx(c["key"]), n, a)
+        if "a" in c:
+            assert to_host(a).tobytes().hex() == c["a"]
+            b = to_dev(hx(c["b"]).view(np.int64))
+            ctx.qc_encode(a, b, n, 1)
+            assert to_host(b).tobytes().hex() == c["ab"]
+            out = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+            ctx.qc_encode_sparse(a, to_dev(np.array(c["pos"], np.int64)), n, out)
+            assert to_host(out).tobytes().hex() == c["sparse"]
+        else:
+            io = to_dev(blocks(c["dual_in"]))
+            ctx.sot_dual_lpn(a, io, n)
+            assert hashlib.sha256(to_host(io).tobytes()).hexdigest() == c["dual_out_sha"]
+
+
+@pytest.mark.parametrize("e,nplanes", [(10, 3), (11, 1), (12, 5), (13, 2), (14, 7), (16, 2), (20, 2)])
+def test_qc_encode_vs_oracle(ctx, e, nplanes):
+    n = 1 << e
+    rng = np.random.default_rng(e)
+    key = rng_blocks(rng, 1)[0]
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(key, n, a)
+    a_np = oracle.qc_gen_a(key, n)
+    assert np.array_equal(to_host(a).view(np.uint64), a_np)
+    planes = rng.integers(0, 2**63, (nplanes, n // 64), dtype=np.uint64)
+    # include the extreme planes: all-zero and all-ones
+    planes[0, :] = 0
+    if nplanes > 2:
+        planes[2, :] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    d = to_dev(planes.view(np.int64))
+    ctx.qc_encode(a, d, n, nplanes)
+    exp = oracle.qc_encode(a_np, planes, n, threads=8)
+    assert np.array_equal(to_host(d).view(np.uint64), exp)
+
+
+def test_qc_plan_matches_one_shot(ctx):
+    n = 1 << 15
+    rng = np.random.default_rng(77)
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+    io = rng_blocks(rng, n)
+    d1, d2 = to_dev(io), to_dev(io)
+    ctx.sot_dual_lpn(a, d1, n)
+    plan = ctx.qc_plan(a, n)
+    plan.set_batch(5)
+    plan.dual_lpn(d2)
+    assert np.array_equal(to_host(d1), to_host(d2))
+    exp = oracle.sot_dual_lpn(to_host(a).view(np.uint64), io, n, threads=8)
+    assert np.array_equal(to_host(d1), exp)
+
+
+def test_qc_dual_lpn_full_size_linearity(ctx):
+    """n = 2^20, 128 planes: linearity of the encode and a spot check of
+    planes against the oracle."""
+    n = 1 << 20
+    rng = np.random.default_rng(20)
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+    x, y = rng_blocks(rng, n), rng_blocks(rng, n)
+    dx, dy, dxy = to_dev(x), to_dev(y), to_dev(x ^ y)
+    for d in (dx, dy, dxy):
+        ctx.sot_dual_lpn(a, d, n)
+    assert np.array_equal(to_host(dx) ^ to_host(dy), to_host(dxy))
+    planes = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    outp = oracle.bit_transpose(to_host(dx), n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    a_np = to_host(a).view(np.uint64)
+    for r in (0, 63, 127):
+        assert np.array_equal(outp[r], oracle.gf2_cyclic_mul(a_np, planes[r], n))
+
+
+# ---------------------------------------------------------------- SOT
+def sot_inputs(rng, t, h):
+    return (rng_blocks(rng, t), rng_blocks(rng, 1)[0], rng_blocks(rng, h * t), rng_blocks(rng, h * t),
+            rng.integers(0, 2, h * t).astype(np.uint8))
+
+
+def run_sot(ctx, roots, h, delta, b0, b1, choice):
+    t = roots.shape[0]
+    leaves, m0, m1 = empty_blocks(t << h), empty_blocks((h + 1) * t), empty_blocks((h + 1) * t)
+    ctx.sot_pprf_sender(to_dev(roots), h, delta, to_dev(b0), to_dev(b1), leaves, m0, m1)
+    mc = np.where(choice[:, None] == 0, b0, b1)
+    rleaves = empty_blocks(t << h)
+    ctx.sot_pprf_recver(m0, m1, to_dev(mc), to_dev(choice), t, h, rleaves)
+    return to_host(leaves), to_host(m0), to_host(m1), to_host(rleaves), mc
+
+
+def test_sot_pprf_golden(ctx, golden):
+    for c in golden["sot_pprf"]:
+        t, h = c["t"], c["h"]
+        ch = np.array(c["choice"], np.uint8)
+        lv, m0, m1, rl, _ = run_sot(ctx, blocks(c["roots"]), h, hx(c["delta"]), blocks(c["base0"]),
+                                    blocks(c["base1"]), ch)
+        assert lv.tobytes().hex() == c["leaves"]
+        assert m0.tobytes().hex() == c["m0"]
+        assert m1.tobytes().hex() == c["m1"]
+        assert np.array_equal(rl, oracle.sot_pprf_recver(m0, m1, blocks(c["mc"]), ch, t, h))
+
+
+@pytest.mark.parametrize("t,h", [(1, 1), (3, 5), (256, 12), (17, 10)])
+def test_sot_pprf_vs_oracle(ctx, t, h):
+    rng = np.random.default_rng(t * 7 + h)
+    roots, delta, b0, b1, ch = sot_inputs(rng, t, h)
+    lv, m0, m1, rl, mc = run_sot(ctx, roots, h, delta, b0, b1, ch)
+    el, e0, e1 = oracle.sot_pprf_sender(roots, h, delta, b0, b1, threads=8)
+    assert np.array_equal(lv, el) and np.array_equal(m0, e0) and np.array_equal(m1, e1)
+    assert np.array_equal(rl, oracle.sot_pprf_recver(e0, e1, mc, ch, t, h, threads=8))
+
+
+def test_sot_end_to_end_cot_n20(ctx):
+    """Plain SOT at n = 2^20 (256 trees of depth 12): PPRF -> transpose ->
+    exact QC encode -> transpose on both roles; the outputs form a COT:
+    w_j = v_j ^ c_j * delta with c = a * e (encode_sparse of the punctured
+    positions)."""
+    t, h = 256, 12
+    n = t << h
+    rng = np.random.default_rng(2020)
+    roots, delta, b0, b1, ch = sot_inputs(rng, t, h)
+    lv, m0, m1, rl, mc = run_sot(ctx, roots, h, delta, b0, b1, ch)
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+    v, w = to_dev(lv), to_dev(rl)
+    ctx.sot_dual_lpn(a, v, n)
+    ctx.sot_dual_lpn(a, w, n)
+    chm = ch.reshape(h, t)
+    pos = np.zeros(t, np.int64)
+    for d in range(h):
+        pos = pos * 2 + 1 - chm[d].astype(np.int64)
+    pos += np.arange(t) * (1 << h)
+    c = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_encode_sparse(a, to_dev(pos), n, c)
+    cbits = np.unpackbits(to_host(c).view(np.uint8), bitorder="little").astype(bool)
+    diff = to_host(v) ^ to_host(w)
+    assert not diff[~cbits].any()
+    assert (diff[cbits] == delta).all()
+    assert 0.4 < cbits.mean() < 0.6
