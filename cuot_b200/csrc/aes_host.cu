@@ -63,5 +63,6 @@ void host_aes_key_expand(const uint8_t key[16], AesKey *out) {
     for (int j = 0; j < 4; j++) rk[4 * i + j] = (uint8_t)(rk[4 * (i - 4) + j] ^ t[j]);
   }
   std::memcpy(out->rk, rk, 176);  // little-endian words
+  for (int i = 0; i < 44; i++) out->rkr[i] = (out->rk[i] >> 8) | (out->rk[i] << 24);
 }
 }  // namespace cuot

@@ -39,8 +39,10 @@ __device__ __forceinline__ void st_blk_cs(Blk *p, Blk b) {
 }
 
 // ---------------------------------------------------------------------------
-// AES-128 round keys: 44 little-endian words (FIPS-197 key schedule).
-struct AesKey { uint32_t rk[44]; };
+// AES-128 round keys: 44 little-endian words (FIPS-197 key schedule), and
+// rkr[i] = rotr8(rk[i]) so a round folds its key into the rotated half:
+// rotl8(x ^ rotr8(k)) = rotl8(x) ^ k saves one instruction per column.
+struct AesKey { uint32_t rk[44]; uint32_t rkr[44]; };
 
 // Host side (aes_host.cu): the S-box is computed from GF(2^8) inversion and
 // the affine map; T0[x] = 2S | S<<8 | S<<16 | 3S<<24 (MixColumns column of
@@ -88,9 +90,10 @@ __device__ __forceinline__ uint32_t t2(const TabRef &t, uint32_t s) {
 __device__ __forceinline__ uint32_t rotl8(uint32_t x) { return __funnelshift_l(x, x, 8); }
 
 // out_c = T0[b0(s_c)] ^ T1[b1(s_c+1)] ^ T2[b2(s_c+2)] ^ T3[b3(s_c+3)] ^ k_c
+//       = T0[..] ^ T2[..] ^ rotl8(T0[b1(s_c+1)] ^ T2[b3(s_c+3)] ^ rotr8(k_c))
 __device__ __forceinline__ uint32_t round_col(const TabRef &t, uint32_t a, uint32_t b,
-                                              uint32_t c, uint32_t d, uint32_t k) {
-  return t0<0>(t, a) ^ rotl8(t0<1>(t, b)) ^ t2<2>(t, c) ^ rotl8(t2<3>(t, d)) ^ k;
+                                              uint32_t c, uint32_t d, uint32_t kr) {
+  return t0<0>(t, a) ^ t2<2>(t, c) ^ rotl8(t0<1>(t, b) ^ t2<3>(t, d) ^ kr);
 }
 
 // Final round column: S[b0(a)] | S[b1(b)]<<8 | S[b2(c)]<<16 | S[b3(d)]<<24.
@@ -104,18 +107,18 @@ __device__ __forceinline__ uint32_t final_col(const TabRef &t, uint32_t a, uint3
   return __byte_perm(lo, hi, 0x7610u) ^ k;
 }
 
-// AES-128 encryption of one block.  `rk` is indexable with compile-time
-// indices after unrolling (kernel-parameter or __constant__ key schedules
-// then become constant-bank operands).
-template <typename RK>
-__device__ __forceinline__ void aes_enc(const TabRef &t, uint32_t (&x)[4], const RK &rk) {
+// AES-128 encryption of one block.  The key schedule is indexed with
+// compile-time indices after unrolling, so kernel-parameter or __constant__
+// schedules become constant-bank operands.
+__device__ __forceinline__ void aes_enc(const TabRef &t, uint32_t (&x)[4], const AesKey &key) {
+  const uint32_t *rk = key.rk, *kr = key.rkr;
   uint32_t s0 = x[0] ^ rk[0], s1 = x[1] ^ rk[1], s2 = x[2] ^ rk[2], s3 = x[3] ^ rk[3];
 #pragma unroll
   for (int r = 1; r < 10; r++) {
-    uint32_t o0 = round_col(t, s0, s1, s2, s3, rk[4 * r + 0]);
-    uint32_t o1 = round_col(t, s1, s2, s3, s0, rk[4 * r + 1]);
-    uint32_t o2 = round_col(t, s2, s3, s0, s1, rk[4 * r + 2]);
-    uint32_t o3 = round_col(t, s3, s0, s1, s2, rk[4 * r + 3]);
+    uint32_t o0 = round_col(t, s0, s1, s2, s3, kr[4 * r + 0]);
+    uint32_t o1 = round_col(t, s1, s2, s3, s0, kr[4 * r + 1]);
+    uint32_t o2 = round_col(t, s2, s3, s0, s1, kr[4 * r + 2]);
+    uint32_t o3 = round_col(t, s3, s0, s1, s2, kr[4 * r + 3]);
     s0 = o0; s1 = o1; s2 = o2; s3 = o3;
   }
   x[0] = final_col(t, s0, s1, s2, s3, rk[40]);
@@ -125,21 +128,21 @@ __device__ __forceinline__ void aes_enc(const TabRef &t, uint32_t (&x)[4], const
 }
 
 // Two independent blocks interleaved for instruction-level parallelism.
-template <typename RKA, typename RKB>
-__device__ __forceinline__ void aes_enc2(const TabRef &t, uint32_t (&a)[4], const RKA &ka,
-                                         uint32_t (&b)[4], const RKB &kb) {
+__device__ __forceinline__ void aes_enc2(const TabRef &t, uint32_t (&a)[4], const AesKey &KA,
+                                         uint32_t (&b)[4], const AesKey &KB) {
+  const uint32_t *ka = KA.rk, *kb = KB.rk, *kar = KA.rkr, *kbr = KB.rkr;
   uint32_t s0 = a[0] ^ ka[0], s1 = a[1] ^ ka[1], s2 = a[2] ^ ka[2], s3 = a[3] ^ ka[3];
   uint32_t u0 = b[0] ^ kb[0], u1 = b[1] ^ kb[1], u2 = b[2] ^ kb[2], u3 = b[3] ^ kb[3];
 #pragma unroll
   for (int r = 1; r < 10; r++) {
-    uint32_t o0 = round_col(t, s0, s1, s2, s3, ka[4 * r + 0]);
-    uint32_t p0 = round_col(t, u0, u1, u2, u3, kb[4 * r + 0]);
-    uint32_t o1 = round_col(t, s1, s2, s3, s0, ka[4 * r + 1]);
-    uint32_t p1 = round_col(t, u1, u2, u3, u0, kb[4 * r + 1]);
-    uint32_t o2 = round_col(t, s2, s3, s0, s1, ka[4 * r + 2]);
-    uint32_t p2 = round_col(t, u2, u3, u0, u1, kb[4 * r + 2]);
-    uint32_t o3 = round_col(t, s3, s0, s1, s2, ka[4 * r + 3]);
-    uint32_t p3 = round_col(t, u3, u0, u1, u2, kb[4 * r + 3]);
+    uint32_t o0 = round_col(t, s0, s1, s2, s3, kar[4 * r + 0]);
+    uint32_t p0 = round_col(t, u0, u1, u2, u3, kbr[4 * r + 0]);
+    uint32_t o1 = round_col(t, s1, s2, s3, s0, kar[4 * r + 1]);
+    uint32_t p1 = round_col(t, u1, u2, u3, u0, kbr[4 * r + 1]);
+    uint32_t o2 = round_col(t, s2, s3, s0, s1, kar[4 * r + 2]);
+    uint32_t p2 = round_col(t, u2, u3, u0, u1, kbr[4 * r + 2]);
+    uint32_t o3 = round_col(t, s3, s0, s1, s2, kar[4 * r + 3]);
+    uint32_t p3 = round_col(t, u3, u0, u1, u2, kbr[4 * r + 3]);
     s0 = o0; s1 = o1; s2 = o2; s3 = o3;
     u0 = p0; u1 = p1; u2 = p2; u3 = p3;
   }

@@ -46,9 +46,9 @@ __device__ __forceinline__ void lpn_group4(const LpnArgs &a, const TabRef &T, in
     uint32_t x[4] = {uint32_t(m), 0u, ilo, ihi};
     uint32_t y[4] = {uint32_t(m + 1), 0u, ilo, ihi};
     if (m + 1 < D) {
-      aes_enc2(T, x, a.key.rk, y, a.key.rk);
+      aes_enc2(T, x, a.key, y, a.key);
     } else {
-      aes_enc(T, x, a.key.rk);
+      aes_enc(T, x, a.key);
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -80,7 +80,7 @@ __device__ void lpn_group4_dyn(const LpnArgs &a, const TabRef &T, int64_t g) {
   const uint32_t ilo = uint32_t(uint64_t(i)), ihi = uint32_t(uint64_t(i) >> 32);
   for (int m = 0; m < a.d; m++) {
     uint32_t x[4] = {uint32_t(m), 0u, ilo, ihi};
-    aes_enc(T, x, a.key.rk);
+    aes_enc(T, x, a.key);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int word = 4 * m + q;
@@ -107,7 +107,7 @@ __device__ void lpn_row1(const LpnArgs &a, const TabRef &T, int64_t j) {
   int done = 0;
   for (int m = 0; m < nb; m++) {
     uint32_t x[4] = {uint32_t(m), 0u, jlo, jhi};
-    aes_enc(T, x, a.key.rk);
+    aes_enc(T, x, a.key);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       if (done < a.d) acc = blk_xor(acc, ldg_blk(a.kk + (x[q] % k)));
@@ -152,10 +152,10 @@ __global__ void __launch_bounds__(kLpnThreads) ecb_kernel(AesKey key, const uint
     if (j < n) {
       Blk q = ld_blk(io + j);
       uint32_t y[4] = {q.w[0], q.w[1], q.w[2], q.w[3]};
-      aes_enc2(T, x, key.rk, y, key.rk);
+      aes_enc2(T, x, key, y, key);
       st_blk(io + j, Blk{{y[0], y[1], y[2], y[3]}});
     } else {
-      aes_enc(T, x, key.rk);
+      aes_enc(T, x, key);
     }
     st_blk(io + i, Blk{{x[0], x[1], x[2], x[3]}});
   }

@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kPprfThreads, 3) pprf_tree_kernel(PprfArgs a) 
       const Blk p = (l == 0) ? root : ld_blk(in + i);
       uint32_t L[4] = {p.w[0], p.w[1], p.w[2], p.w[3]};
       uint32_t R[4] = {p.w[0], p.w[1], p.w[2], p.w[3]};
-      aes_enc2(T, L, c_ggm_rk[0].rk, R, c_ggm_rk[1].rk);
+      aes_enc2(T, L, c_ggm_rk[0], R, c_ggm_rk[1]);
       Blk cl{{L[0] ^ p.w[0], L[1] ^ p.w[1], L[2] ^ p.w[2], L[3] ^ p.w[3]}};
       Blk cr{{R[0] ^ p.w[0], R[1] ^ p.w[1], R[2] ^ p.w[2], R[3] ^ p.w[3]}};
       accL = blk_xor(accL, cl);

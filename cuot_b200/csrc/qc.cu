@@ -58,42 +58,108 @@ __device__ __forceinline__ uint32_t red2p(uint32_t x) { return x >= 2 * kP ? x -
 __device__ __forceinline__ unsigned brev(unsigned x, int bits) { return __brev(x) >> (32 - bits); }
 
 // ---------------------------------------------------------------------------
-// In-shared-memory transforms over `rows` rows of length N = 2^lg at stride
-// `ld` words.  DIF forward: natural in, bit-reversed out.  DIT inverse:
-// bit-reversed in, natural out (unscaled).  Values in [0, 2p).
-__device__ void smem_dif(uint32_t *x, int rows, int lg, int ld, const uint2 *tw) {
-  const int N = 1 << lg, half = N >> 1;
-  for (int s = lg - 1; s >= 0; s--) {
-    const int len = 1 << s;
-    const int tstride = half >> s;  // N / (2 len)
-    for (int idx = threadIdx.x; idx < rows * half; idx += blockDim.x) {
-      const int row = idx >> (lg - 1), i = idx & (half - 1);
-      const int off = i & (len - 1), base = (i >> s) << (s + 1);
-      uint32_t *px = x + row * ld + base + off;
-      const uint32_t u = px[0], v = px[len];
-      px[0] = red2p(u + v);
-      px[len] = shoup_mul(u - v + 2 * kP, __ldg(&tw[off * tstride]));
+// In-shared-memory transforms over `rows` rows of length N = 2^lg at row
+// stride `ld` words; element i of a row lives at word padi(i) = i + i/32 (the
+// padding keeps the strided accesses of the late passes conflict-free).
+// The lg radix-2 stages are grouped into passes of K <= 4 stages: a thread
+// loads the 2^K elements of one group into registers, runs K stages there,
+// and stores them back, so shared memory is touched once per pass instead of
+// once per stage.  Stage twiddles tw[i] = w_N^i (i < N/2) are Shoup pairs in
+// shared memory.  DIF forward: natural in, bit-reversed out.  DIT inverse:
+// bit-reversed in, natural out (unscaled).  Values stay in [0, 2p).
+__device__ __forceinline__ int padi(int i) { return i + (i >> 5); }
+__host__ __device__ constexpr int padded_len(int n) { return n + n / 32 + 1; }
+
+__device__ __forceinline__ uint32_t umin2p(uint32_t a) {
+  return min(a, a - 2 * kP);  // a in [0, 4p) -> [0, 2p)
+}
+__device__ __forceinline__ void bf_dif(uint32_t &u, uint32_t &v, uint2 w) {
+  const uint32_t a = umin2p(u + v);
+  v = shoup_mul(u - v + 2 * kP, w);
+  u = a;
+}
+__device__ __forceinline__ void bf_dit(uint32_t &u, uint32_t &v, uint2 w) {
+  const uint32_t t = shoup_mul(v, w);
+  v = umin2p(u - t + 2 * kP);
+  u = umin2p(u + t);
+}
+
+template <int K, bool DIF>
+__device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int lg, int ld, int s_lo,
+                                         const uint2 *tw) {
+  constexpr int R = 1 << K;
+  const int ngr_lg = lg - K;
+  const int lowmask = (1 << s_lo) - 1;
+  for (int w = threadIdx.x; w < (rows << ngr_lg); w += blockDim.x) {
+    const int row = w >> ngr_lg, g = w & ((1 << ngr_lg) - 1);
+    const int glo = g & lowmask;
+    const int base = glo | ((g >> s_lo) << (s_lo + K));
+    uint32_t *xr = x + row * ld;
+    uint32_t v[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) v[m] = xr[padi(base + (m << s_lo))];
+    if (DIF) {
+#pragma unroll
+      for (int j = K - 1; j >= 0; j--) {
+        const int s = s_lo + j;
+#pragma unroll
+        for (int m = 0; m < R; m++) {
+          if (m & (1 << j)) continue;
+          const int off = glo | ((m & ((1 << j) - 1)) << s_lo);
+          bf_dif(v[m], v[m | (1 << j)], tw[off << (lg - 1 - s)]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; j++) {
+        const int s = s_lo + j;
+#pragma unroll
+        for (int m = 0; m < R; m++) {
+          if (m & (1 << j)) continue;
+          const int off = glo | ((m & ((1 << j) - 1)) << s_lo);
+          bf_dit(v[m], v[m | (1 << j)], tw[off << (lg - 1 - s)]);
+        }
+      }
     }
-    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < R; m++) xr[padi(base + (m << s_lo))] = v[m];
+  }
+  __syncthreads();
+}
+
+template <bool DIF>
+__device__ void ntt_pass_k(int K, uint32_t *x, int rows, int lg, int ld, int s_lo, const uint2 *tw) {
+  switch (K) {
+    case 1: ntt_pass<1, DIF>(x, rows, lg, ld, s_lo, tw); break;
+    case 2: ntt_pass<2, DIF>(x, rows, lg, ld, s_lo, tw); break;
+    case 3: ntt_pass<3, DIF>(x, rows, lg, ld, s_lo, tw); break;
+    default: ntt_pass<4, DIF>(x, rows, lg, ld, s_lo, tw); break;
   }
 }
 
-__device__ void smem_dit(uint32_t *x, int rows, int lg, int ld, const uint2 *tw) {
-  const int N = 1 << lg, half = N >> 1;
-  for (int s = 0; s < lg; s++) {
-    const int len = 1 << s;
-    const int tstride = half >> s;
-    for (int idx = threadIdx.x; idx < rows * half; idx += blockDim.x) {
-      const int row = idx >> (lg - 1), i = idx & (half - 1);
-      const int off = i & (len - 1), base = (i >> s) << (s + 1);
-      uint32_t *px = x + row * ld + base + off;
-      const uint32_t u = px[0];
-      const uint32_t t = shoup_mul(px[len], __ldg(&tw[off * tstride]));
-      px[0] = red2p(u + t);
-      px[len] = red2p(u - t + 2 * kP);
+// Full transform: ceil(lg/4) passes of near-equal size.  Caller has synced.
+template <bool DIF>
+__device__ void ntt_smem(uint32_t *x, int rows, int lg, int ld, const uint2 *tw) {
+  const int P = (lg + 3) / 4;
+  if (DIF) {
+    int top = lg;  // stages [top-K, top)
+    for (int p = 0; p < P; p++) {
+      const int K = lg / P + (p < lg % P ? 1 : 0);
+      ntt_pass_k<true>(K, x, rows, lg, ld, top - K, tw);
+      top -= K;
     }
-    __syncthreads();
+  } else {
+    int lo = 0;
+    for (int p = 0; p < P; p++) {
+      const int K = lg / P + (p < lg % P ? 1 : 0);
+      ntt_pass_k<false>(K, x, rows, lg, ld, lo, tw);
+      lo += K;
+    }
   }
+}
+
+__device__ __forceinline__ void stage_tw(uint2 *dst, const uint2 *src, int cnt) {
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = __ldg(&src[i]);
 }
 
 // Pass A.  bits: plane-major, plane_words 32-bit words per plane.
@@ -102,7 +168,9 @@ __global__ void __launch_bounds__(kQcThreads) qc_col_fwd(
     const uint32_t *__restrict__ bits, uint64_t plane_words, int e1, int e2,
     const uint2 *__restrict__ tw1f, const uint2 *__restrict__ fsf, uint32_t *__restrict__ Y) {
   extern __shared__ uint32_t xs[];
-  const int N1 = 1 << e1, N2 = 1 << e2, ld = N1 + 1;
+  const int N1 = 1 << e1, N2 = 1 << e2, ld = padded_len(N1);
+  uint2 *tws = reinterpret_cast<uint2 *>(xs + kCW * ld + (kCW * ld & 1));
+  stage_tw(tws, tw1f, N1 / 2);
   const int c0 = blockIdx.x * kCW;
   const uint64_t plane = blockIdx.y;
   const uint32_t *pb = bits + plane * plane_words;
@@ -110,15 +178,15 @@ __global__ void __launch_bounds__(kQcThreads) qc_col_fwd(
     const uint64_t bit = uint64_t(j1) * N2 + c0;
     const uint32_t w = __ldg(&pb[bit >> 5]) >> (bit & 31);
 #pragma unroll
-    for (int c = 0; c < kCW; c++) xs[c * ld + j1] = (w >> c) & 1u;
+    for (int c = 0; c < kCW; c++) xs[c * ld + padi(j1)] = (w >> c) & 1u;
   }
   __syncthreads();
-  smem_dif(xs, kCW, e1, ld, tw1f);
+  ntt_smem<true>(xs, kCW, e1, ld, tws);
   uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
-    Yp[o] = shoup_mul(xs[c * ld + r], __ldg(&fsf[o]));
+    Yp[o] = shoup_mul(xs[c * ld + padi(r)], __ldg(&fsf[o]));
   }
 }
 
@@ -129,21 +197,28 @@ __global__ void __launch_bounds__(kQcThreads) qc_row(
     const uint2 *__restrict__ tw2f, const uint2 *__restrict__ tw2i,
     const uint2 *__restrict__ ahat, int mode) {
   extern __shared__ uint32_t xs[];
-  const int N1 = 1 << e1, N2 = 1 << e2;
+  const int N1 = 1 << e1, N2 = 1 << e2, ld = padded_len(N2);
+  uint2 *twf = reinterpret_cast<uint2 *>(xs + rows_per_cta * ld + (rows_per_cta * ld & 1));
+  uint2 *twi = twf + N2 / 2;
+  stage_tw(twf, tw2f, N2 / 2);
+  if (mode == 0) stage_tw(twi, tw2i, N2 / 2);
   const uint64_t plane = blockIdx.y;
   const int r0 = blockIdx.x * rows_per_cta;
   uint32_t *Yp = Y + (plane * N1 + r0) * uint64_t(N2);
   const int cnt = rows_per_cta * N2;
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[i] = Yp[i];
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[(i >> e2) * ld + padi(i & (N2 - 1))] = Yp[i];
   __syncthreads();
-  smem_dif(xs, rows_per_cta, e2, N2, tw2f);
+  ntt_smem<true>(xs, rows_per_cta, e2, ld, twf);
   if (mode == 0) {
     const uint2 *ah = ahat + uint64_t(r0) * N2;
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[i] = shoup_mul(xs[i], __ldg(&ah[i]));
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      uint32_t *p = &xs[(i >> e2) * ld + padi(i & (N2 - 1))];
+      *p = shoup_mul(*p, __ldg(&ah[i]));
+    }
     __syncthreads();
-    smem_dit(xs, rows_per_cta, e2, N2, tw2i);
+    ntt_smem<false>(xs, rows_per_cta, e2, ld, twi);
   }
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) Yp[i] = xs[i];
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) Yp[i] = xs[(i >> e2) * ld + padi(i & (N2 - 1))];
 }
 
 // Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits.
@@ -151,23 +226,25 @@ __global__ void __launch_bounds__(kQcThreads) qc_col_inv(
     const uint32_t *__restrict__ Y, int e1, int e2, const uint2 *__restrict__ fsi,
     const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes) {
   extern __shared__ uint32_t xs[];
-  const int N1 = 1 << e1, N2 = 1 << e2, ld = N1 + 1;
+  const int N1 = 1 << e1, N2 = 1 << e2, ld = padded_len(N1);
+  uint2 *tws = reinterpret_cast<uint2 *>(xs + kCW * ld + (kCW * ld & 1));
+  stage_tw(tws, tw1i, N1 / 2);
   const int c0 = blockIdx.x * kCW;
   const uint64_t plane = blockIdx.y;
   const uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
-    xs[c * ld + r] = shoup_mul(Yp[o], __ldg(&fsi[o]));
+    xs[c * ld + padi(r)] = shoup_mul(Yp[o], __ldg(&fsi[o]));
   }
   __syncthreads();
-  smem_dit(xs, kCW, e1, ld, tw1i);
+  ntt_smem<false>(xs, kCW, e1, ld, tws);
   uint8_t *ob = out + plane * plane_bytes;
   for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
     uint32_t byte = 0;
 #pragma unroll
     for (int c = 0; c < kCW; c++) {
-      uint32_t v = xs[c * ld + j1];
+      uint32_t v = xs[c * ld + padi(j1)];
       v = v >= kP ? v - kP : v;  // exact coefficient in [0, n]
       byte |= (v & 1u) << c;
     }
@@ -303,7 +380,10 @@ void qc_free_ctx_tables(cuot_ctx *ctx) {
   }
 }
 
-static int col_smem(const QcTables *t) { return kCW * ((1 << t->e1) + 1) * 4; }
+static int col_smem(const QcTables *t) {
+  const int ld = padded_len(1 << t->e1);
+  return (kCW * ld + 1) * 4 + (1 << t->e1) / 2 * 8;
+}
 static int row_rows(const QcTables *t) {
   const int N2 = 1 << t->e2;
   int r = 4096 / N2;
@@ -311,7 +391,10 @@ static int row_rows(const QcTables *t) {
   if (r > (1 << t->e1)) r = 1 << t->e1;
   return r;
 }
-static int row_smem(const QcTables *t) { return row_rows(t) * (1 << t->e2) * 4; }
+static int row_smem(const QcTables *t) {
+  const int ld = padded_len(1 << t->e2);
+  return (row_rows(t) * ld + 1) * 4 + (1 << t->e2) * 8;
+}
 
 static int set_attrs(const QcTables *t) {
   static bool done = false;
