@@ -18,8 +18,11 @@ struct LpnArgs {
   AesKey key;
   const uint32_t *t0;
   const Blk *kk;
-  Blk *e;
-  int64_t n, k, tail, ngroups, ntail;
+  Blk *e;                 // row `row_lo` of the n-row matrix
+  int64_t n, k, tail;     // tail: first row handled by the one-row path
+  int64_t row_lo;         // first row held in e (a multiple of 4)
+  int64_t g0, ngroups;    // 4-row groups [g0, g0 + ngroups)
+  int64_t j0, ntail;      // one-row rows [j0, j0 + ntail)
   uint32_t mask;
   int d;
 };
@@ -67,7 +70,7 @@ __device__ __forceinline__ void lpn_group4(const LpnArgs &a, const TabRef &T, in
   }
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    Blk *p = a.e + i + m;
+    Blk *p = a.e + (i - a.row_lo) + m;
     st_blk_cs(p, blk_xor(ld_blk(p), acc[m]));
   }
 }
@@ -93,7 +96,7 @@ __device__ void lpn_group4_dyn(const LpnArgs &a, const TabRef &T, int64_t g) {
   }
 #pragma unroll
   for (int m = 0; m < 4; m++) {
-    Blk *p = a.e + i + m;
+    Blk *p = a.e + (i - a.row_lo) + m;
     st_blk_cs(p, blk_xor(ld_blk(p), acc[m]));
   }
 }
@@ -114,7 +117,7 @@ __device__ void lpn_row1(const LpnArgs &a, const TabRef &T, int64_t j) {
       done++;
     }
   }
-  Blk *p = a.e + j;
+  Blk *p = a.e + (j - a.row_lo);
   st_blk(p, blk_xor(ld_blk(p), acc));
 }
 
@@ -128,10 +131,10 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(LpnArgs a) {
   for (int64_t w = int64_t(blockIdx.x) * kLpnThreads + threadIdx.x; w < total;
        w += int64_t(gridDim.x) * kLpnThreads) {
     if (w < a.ngroups) {
-      if (D > 0) lpn_group4<(D > 0 ? D : 1)>(a, T, w);
-      else lpn_group4_dyn(a, T, w);
+      if (D > 0) lpn_group4<(D > 0 ? D : 1)>(a, T, a.g0 + w);
+      else lpn_group4_dyn(a, T, a.g0 + w);
     } else {
-      lpn_row1(a, T, a.tail + (w - a.ngroups));
+      lpn_row1(a, T, a.j0 + (w - a.ngroups));
     }
   }
 }
@@ -188,28 +191,36 @@ using namespace cuot;
 
 extern "C" {
 
-int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
-                    int64_t k, int d, cuot_block *e_io_d, int64_t n, void *stream) {
-  if (!ctx || !seed || !kk_d || !e_io_d) return fail(CUOT_EINVAL, "null argument");
+int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
+                          int64_t k, int d, cuot_block *e_rows_d, int64_t row_lo, int64_t row_hi,
+                          int64_t n, void *stream) {
+  if (!ctx || !seed || !kk_d || !e_rows_d) return fail(CUOT_EINVAL, "null argument");
   if (k < 1 || k > 0x7fffffffll) return fail(CUOT_EINVAL, "k=%lld out of range", (long long)k);
   if (d < 1 || d > 32) return fail(CUOT_EINVAL, "d=%d out of range [1,32]", d);
-  if (n < 0) return fail(CUOT_EINVAL, "n < 0");
-  if (n == 0) return CUOT_OK;
+  if (n < 0 || row_lo < 0 || row_hi < row_lo || row_hi > n)
+    return fail(CUOT_EINVAL, "bad row range [%lld,%lld) of n=%lld", (long long)row_lo,
+                (long long)row_hi, (long long)n);
+  if (row_lo % 4 || (row_hi % 4 && row_hi != n))
+    return fail(CUOT_EINVAL, "row range must start at a multiple of 4 and end at one or at n");
+  if (row_hi == row_lo) return CUOT_OK;
   DeviceGuard g(ctx);
   LpnArgs a{};
   host_aes_key_expand(seed, &a.key);
   a.t0 = ctx->t0_d;
   a.kk = reinterpret_cast<const Blk *>(kk_d);
-  a.e = reinterpret_cast<Blk *>(e_io_d);
-  a.n = n; a.k = k; a.d = d;
+  a.e = reinterpret_cast<Blk *>(e_rows_d);
+  a.n = n; a.k = k; a.d = d; a.row_lo = row_lo;
   uint32_t mask = 1;
   while (int64_t(mask) < k) mask = (mask << 1) | 1u;  // lpn_f2.h:27-31
   a.mask = mask;
   int64_t tail = 0;
-  if (n > 4) tail = ((n - 4) + 3) / 4 * 4;  // first j = 0 mod 4 with j >= n-4
+  if (n > 4) tail = ((n - 4) + 3) / 4 * 4;  // lpn_f2.h:75: groups while j < n - 4
   a.tail = tail;
-  a.ngroups = tail / 4;
-  a.ntail = n - tail;
+  const int64_t gend = (row_hi < tail ? row_hi : tail);
+  a.g0 = row_lo / 4;
+  a.ngroups = gend > row_lo ? (gend - row_lo) / 4 : 0;
+  a.j0 = row_lo > tail ? row_lo : tail;
+  a.ntail = row_hi > a.j0 ? row_hi - a.j0 : 0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int grid = 1;
   if (d == 10) {
@@ -222,6 +233,11 @@ int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_
     lpn_kernel<0><<<grid, kLpnThreads, kTableBytes, st>>>(a);
   }
   return launch_status();
+}
+
+int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
+                    int64_t k, int d, cuot_block *e_io_d, int64_t n, void *stream) {
+  return cuot_lpn_primal_range(ctx, seed, kk_d, k, d, e_io_d, 0, n, n, stream);
 }
 
 int cuot_aes128_ecb(cuot_ctx *ctx, const uint8_t key[16], cuot_block *io_d,

@@ -95,6 +95,15 @@ int cuot_ferret_pprf_recver(cuot_ctx *ctx, const cuot_block *mc_d,
 int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16],
                     const cuot_block *kk_d, int64_t k, int d,
                     cuot_block *e_io_d, int64_t n, void *stream);
+/* Rows [row_lo, row_hi) of the same n-row LPN (e_rows_d holds those rows),
+ * for splitting the rows over GPUs with kk replicated (the reference splits
+ * rows per GPU and offsets the counters, dev_layer.cu:166-176).  row_lo is a
+ * multiple of 4; row_hi is a multiple of 4 or n.  Shards computed this way
+ * are bit-identical to the unsplit result. */
+int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16],
+                          const cuot_block *kk_d, int64_t k, int d,
+                          cuot_block *e_rows_d, int64_t row_lo,
+                          int64_t row_hi, int64_t n, void *stream);
 
 /* ---- SOT PPRF ----------------------------------------------------------------
  * Structure of SOTSender/SOTRecver::seed_expand (silent/sender.cu:76-108,
