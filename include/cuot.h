@@ -87,6 +87,27 @@ int cuot_ferret_pprf_recver(cuot_ctx *ctx, const cuot_block *mc_d,
                             const cuot_block *secret_sum_d, uint64_t t, int h,
                             cuot_block *leaves_d, void *stream);
 
+/* Allocation-free Ferret sender.  No counterpart in the reference.
+ * Same arguments and results as cuot_ferret_pprf_sender, without a context,
+ * on the calling thread's current device, and it never allocates device
+ * memory (no cudaMalloc/cudaFree, no allocating library call).  It is for
+ * callers that cannot allocate at call time: a serving process whose HBM is
+ * owned by its own pool allocator, or a latency-critical path that cannot
+ * afford the implicit device synchronisation of cudaMalloc/cudaFree.
+ * Scratch lives in a fixed 16 MiB device array inside libcuot (held by every
+ * GPU that loads the library until the process exits), so t * 2^h may not
+ * exceed 2^20 leaves; larger requests return CUOT_EINVAL.
+ * The first call on a device does a one-time set-up (uploads the AES keys
+ * and table, looks up the array's device address), which synchronises; make
+ * that first call before any stream capture.  All calls on a device share
+ * the one scratch array: calls that overlap on the GPU (other streams, other
+ * host threads) race, so order them (e.g. one stream). */
+int cuot_ferret_pprf_sender_noalloc(const cuot_block *roots_d, uint64_t t,
+                                    int h, const cuot_block *delta,
+                                    cuot_block *leaves_d, cuot_block *lsum_d,
+                                    cuot_block *rsum_d,
+                                    cuot_block *secret_sum_d, void *stream);
+
 /* ---- Ferret primal LPN -----------------------------------------------------
  * e_io_d[i] ^= XOR_{j<d} kk_d[idx(i, j)] for i < n, with the index matrix of
  * emp-ot LpnF2::task over [0, n) (lpn_f2.h:46-79) under AES key `seed`.
