@@ -146,6 +146,11 @@ class Context:
                                         C.c_int(d), _ptr(e_io), C.c_int64(_nblocks(e_io)), _stream(stream)),
                "cuot_lpn_primal")
 
+    def lpn_primal_range(self, seed, kk, e_rows, row_lo: int, row_hi: int, n: int, d: int = 10, stream=None):
+        _check(self.lib.cuot_lpn_primal_range(self.h, _host_block(seed), _ptr(kk), C.c_int64(_nblocks(kk)),
+                                              C.c_int(d), _ptr(e_rows), C.c_int64(row_lo), C.c_int64(row_hi),
+                                              C.c_int64(n), _stream(stream)), "cuot_lpn_primal_range")
+
     # ---- SOT ---------------------------------------------------------------
     def sot_pprf_sender(self, roots, h: int, delta, base0, base1, leaves, m0, m1, stream=None):
         t = _nblocks(roots)

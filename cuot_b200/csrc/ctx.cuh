@@ -33,4 +33,12 @@ int scratch(cuot_ctx *ctx, uint64_t bytes, void **out);
 int pprf_init_device();
 // Frees the context's cached QC tables (qc.cu).
 void qc_free_ctx_tables(cuot_ctx *ctx);
+// QC helpers used by the batched engine (qc.cu).
+int qc_prepare(cuot_ctx *ctx, int e);
+int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, uint32_t *Y, uint2 *ahat, cudaStream_t st);
+int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const uint2 *const *ahats,
+                   uint32_t *Y, int batch, cudaStream_t st);
+int qc_default_batch(uint64_t n, int nplanes);
+int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
+                     uint64_t col_hi, void *out, cudaStream_t st);
 }  // namespace cuot

@@ -52,19 +52,24 @@ __device__ __forceinline__ Blk mask_lsb(Blk b) {
   return b;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kPprfThreads, 3) pprf_tree_kernel(PprfArgs a) {
-  extern __shared__ __align__(16) uint32_t smem_tab[];
-  __shared__ Blk red[2][kPprfThreads / 32];
-  __shared__ unsigned long long s_ap;
+// Shared-memory state of one tree expansion.
+struct PprfSmem {
+  Blk red[2][kPprfThreads / 32];
+  unsigned long long ap;
+};
 
-  stage_table(smem_tab, a.t0);
-  const uint64_t tree = blockIdx.x;
+// Expands tree `tree` of the instance described by `a` with the whole CTA
+// (kPprfThreads threads).  scratch_tree: 2^h blocks for the level ping-pong.
+// The T-table must already be staged (and synced) in shared memory.
+template <int MODE>
+__device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk *scratch_tree,
+                                          const TabRef &T, PprfSmem &sm) {
+  Blk (&red)[2][kPprfThreads / 32] = sm.red;
+  unsigned long long &s_ap = sm.ap;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const TabRef T{reinterpret_cast<const char *>(smem_tab), uint32_t(lane) * 4u};
   const int h = a.h;
   const uint64_t W = 1ull << h;
-  Blk *const bufs[2] = {a.leaves + tree * W, a.scratch + tree * W};
+  Blk *const bufs[2] = {a.leaves + tree * W, scratch_tree};
   Blk root{{0, 0, 0, 0}};
   if (MODE == FERRET_SEND || MODE == SOT_SEND) root = ldg_blk(a.roots + tree);
   if (tid == 0) s_ap = 0;
@@ -169,6 +174,17 @@ __global__ void __launch_bounds__(kPprfThreads, 3) pprf_tree_kernel(PprfArgs a) 
     }
     __syncthreads();
   }
+}
+
+// One CTA per tree of a single instance.
+template <int MODE>
+__global__ void __launch_bounds__(kPprfThreads, 3) pprf_tree_kernel(PprfArgs a) {
+  extern __shared__ __align__(16) uint32_t smem_tab[];
+  __shared__ PprfSmem sm;
+  stage_table(smem_tab, a.t0);
+  const TabRef T{reinterpret_cast<const char *>(smem_tab), uint32_t(threadIdx.x & 31) * 4u};
+  const uint64_t tree = blockIdx.x;
+  pprf_tree<MODE>(a, tree, a.scratch + (tree << a.h), T, sm);
 }
 
 }  // namespace

@@ -59,16 +59,42 @@ __device__ __forceinline__ unsigned brev(unsigned x, int bits) { return __brev(x
 
 // ---------------------------------------------------------------------------
 // In-shared-memory transforms over `rows` rows of length N = 2^lg at row
-// stride `ld` words; element i of a row lives at word padi(i) = i + i/32 (the
-// padding keeps the strided accesses of the late passes conflict-free).
+// stride `ld` = N + 4 words (so the column kernels' row-interleaved
+// accesses hit distinct banks); element i of a row lives at word swz(i), an
+// XOR swizzle of its low five bits by the bits above, which keeps every radix
+// pass's strided accesses conflict-free (2-way at most for some 16-point
+// passes).
 // The lg radix-2 stages are grouped into passes of K <= 4 stages: a thread
 // loads the 2^K elements of one group into registers, runs K stages there,
 // and stores them back, so shared memory is touched once per pass instead of
-// once per stage.  Stage twiddles tw[i] = w_N^i (i < N/2) are Shoup pairs in
-// shared memory.  DIF forward: natural in, bit-reversed out.  DIT inverse:
+// once per stage.  Stage twiddles are Shoup pairs in shared memory, stored
+// per stage: stage s (pairs 2^s apart) reads tw[2^s - 1 + off] =
+// w_N^(off * N / 2^(s+1)) for off < 2^s, so a warp's twiddle reads are
+// consecutive.  DIF forward: natural in, bit-reversed out.  DIT inverse:
 // bit-reversed in, natural out (unscaled).  Values stay in [0, 2p).
-__device__ __forceinline__ int padi(int i) { return i + (i >> 5); }
-__host__ __device__ constexpr int padded_len(int n) { return n + n / 32 + 1; }
+__host__ __device__ constexpr int swz(int i) {
+  return i ^ (((i >> 5) & 7) | ((((i >> 5) >> 1) & 3) << 3));
+}
+// swz is linear over GF(2) (an XOR of bit fields), and within a radix group
+// the element offsets (m << s_lo) occupy bits disjoint from the group base,
+// so swz(base ^ (m << s_lo)) = swz(base) ^ swz(m << s_lo): one XOR with a
+// compile-time constant per element.
+__host__ __device__ constexpr int padded_len(int n) { return n + 4; }
+
+// Per-plane `a` transforms for one row pass (passed by value).
+constexpr int kAhatTab = 16;
+struct AhatTab {
+  const uint2 *p[kAhatTab];
+  int per;    // planes per entry
+  int first;  // plane offset of launch plane 0 inside entry 0
+};
+__host__ inline AhatTab single_ahat(const uint2 *a) {
+  AhatTab t{};
+  t.p[0] = a;
+  t.per = 1 << 30;
+  t.first = 0;
+  return t;
+}
 
 __device__ __forceinline__ uint32_t umin2p(uint32_t a) {
   return min(a, a - 2 * kP);  // a in [0, 4p) -> [0, 2p)
@@ -84,77 +110,59 @@ __device__ __forceinline__ void bf_dit(uint32_t &u, uint32_t &v, uint2 w) {
   u = umin2p(u + t);
 }
 
-template <int K, bool DIF>
-__device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int lg, int ld, int s_lo,
-                                         const uint2 *tw) {
+// One pass of K radix-2 stages [S_LO, S_LO + K) of a 2^LG-point transform on
+// `rows` rows, everything but the row count known at compile time.
+template <int LG, int K, int S_LO, bool DIF>
+__device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const uint2 *tw) {
   constexpr int R = 1 << K;
-  const int ngr_lg = lg - K;
-  const int lowmask = (1 << s_lo) - 1;
-  for (int w = threadIdx.x; w < (rows << ngr_lg); w += blockDim.x) {
-    const int row = w >> ngr_lg, g = w & ((1 << ngr_lg) - 1);
-    const int glo = g & lowmask;
-    const int base = glo | ((g >> s_lo) << (s_lo + K));
+  constexpr int NGR_LG = LG - K;
+  constexpr int LOWMASK = (1 << S_LO) - 1;
+  for (int w = threadIdx.x; w < (rows << NGR_LG); w += blockDim.x) {
+    const int row = w >> NGR_LG, g = w & ((1 << NGR_LG) - 1);
+    const int glo = g & LOWMASK;
+    const int base = glo | ((g >> S_LO) << (S_LO + K));
+    const int sb = swz(base);
     uint32_t *xr = x + row * ld;
+    const uint2 *twg = tw + glo;
     uint32_t v[R];
 #pragma unroll
-    for (int m = 0; m < R; m++) v[m] = xr[padi(base + (m << s_lo))];
+    for (int m = 0; m < R; m++) v[m] = xr[sb ^ swz(m << S_LO)];
     if (DIF) {
 #pragma unroll
       for (int j = K - 1; j >= 0; j--) {
-        const int s = s_lo + j;
 #pragma unroll
         for (int m = 0; m < R; m++) {
           if (m & (1 << j)) continue;
-          const int off = glo | ((m & ((1 << j) - 1)) << s_lo);
-          bf_dif(v[m], v[m | (1 << j)], tw[off << (lg - 1 - s)]);
+          // stage s = S_LO + j reads tw[2^s - 1 + off], off = glo | low j bits of m << S_LO
+          bf_dif(v[m], v[m | (1 << j)], twg[(1 << (S_LO + j)) - 1 + ((m & ((1 << j) - 1)) << S_LO)]);
         }
       }
     } else {
 #pragma unroll
       for (int j = 0; j < K; j++) {
-        const int s = s_lo + j;
 #pragma unroll
         for (int m = 0; m < R; m++) {
           if (m & (1 << j)) continue;
-          const int off = glo | ((m & ((1 << j) - 1)) << s_lo);
-          bf_dit(v[m], v[m | (1 << j)], tw[off << (lg - 1 - s)]);
+          bf_dit(v[m], v[m | (1 << j)], twg[(1 << (S_LO + j)) - 1 + ((m & ((1 << j) - 1)) << S_LO)]);
         }
       }
     }
 #pragma unroll
-    for (int m = 0; m < R; m++) xr[padi(base + (m << s_lo))] = v[m];
+    for (int m = 0; m < R; m++) xr[sb ^ swz(m << S_LO)] = v[m];
   }
   __syncthreads();
 }
 
-template <bool DIF>
-__device__ void ntt_pass_k(int K, uint32_t *x, int rows, int lg, int ld, int s_lo, const uint2 *tw) {
-  switch (K) {
-    case 1: ntt_pass<1, DIF>(x, rows, lg, ld, s_lo, tw); break;
-    case 2: ntt_pass<2, DIF>(x, rows, lg, ld, s_lo, tw); break;
-    case 3: ntt_pass<3, DIF>(x, rows, lg, ld, s_lo, tw); break;
-    default: ntt_pass<4, DIF>(x, rows, lg, ld, s_lo, tw); break;
-  }
-}
-
-// Full transform: ceil(lg/4) passes of near-equal size.  Caller has synced.
-template <bool DIF>
-__device__ void ntt_smem(uint32_t *x, int rows, int lg, int ld, const uint2 *tw) {
-  const int P = (lg + 3) / 4;
-  if (DIF) {
-    int top = lg;  // stages [top-K, top)
-    for (int p = 0; p < P; p++) {
-      const int K = lg / P + (p < lg % P ? 1 : 0);
-      ntt_pass_k<true>(K, x, rows, lg, ld, top - K, tw);
-      top -= K;
-    }
-  } else {
-    int lo = 0;
-    for (int p = 0; p < P; p++) {
-      const int K = lg / P + (p < lg % P ? 1 : 0);
-      ntt_pass_k<false>(K, x, rows, lg, ld, lo, tw);
-      lo += K;
-    }
+// Full 2^LG-point transform as ceil(LG/4) passes of near-equal size (DIF
+// from the top stage down, DIT from stage 0 up).  Caller has synced.
+template <int LG, bool DIF, int PIDX = 0, int DONE = 0>
+__device__ __forceinline__ void ntt_smem(uint32_t *x, int rows, int ld, const uint2 *tw) {
+  constexpr int P = (LG + 3) / 4;
+  if constexpr (PIDX < P) {
+    constexpr int K = LG / P + (PIDX < LG % P ? 1 : 0);
+    constexpr int S_LO = DIF ? (LG - DONE - K) : DONE;
+    ntt_pass<LG, K, S_LO, DIF>(x, rows, ld, tw);
+    ntt_smem<LG, DIF, PIDX + 1, DONE + K>(x, rows, ld, tw);
   }
 }
 
@@ -164,87 +172,101 @@ __device__ __forceinline__ void stage_tw(uint2 *dst, const uint2 *src, int cnt) 
 
 // Pass A.  bits: plane-major, plane_words 32-bit words per plane.
 // grid (N2 / kCW, nplanes_batch).  Y: [plane][N1][N2].
-__global__ void __launch_bounds__(kQcThreads) qc_col_fwd(
-    const uint32_t *__restrict__ bits, uint64_t plane_words, int e1, int e2,
+template <int E1>
+__global__ void __launch_bounds__(kQcThreads, 4) qc_col_fwd(
+    const uint32_t *__restrict__ bits, uint64_t plane_words, int e2,
     const uint2 *__restrict__ tw1f, const uint2 *__restrict__ fsf, uint32_t *__restrict__ Y) {
   extern __shared__ uint32_t xs[];
-  const int N1 = 1 << e1, N2 = 1 << e2, ld = padded_len(N1);
+  constexpr int N1 = 1 << E1, ld = padded_len(N1);
+  const int N2 = 1 << e2;
   uint2 *tws = reinterpret_cast<uint2 *>(xs + kCW * ld + (kCW * ld & 1));
-  stage_tw(tws, tw1f, N1 / 2);
+  stage_tw(tws, tw1f, N1 - 1);
   const int c0 = blockIdx.x * kCW;
   const uint64_t plane = blockIdx.y;
   const uint32_t *pb = bits + plane * plane_words;
+#pragma unroll 4
   for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
     const uint64_t bit = uint64_t(j1) * N2 + c0;
     const uint32_t w = __ldg(&pb[bit >> 5]) >> (bit & 31);
 #pragma unroll
-    for (int c = 0; c < kCW; c++) xs[c * ld + padi(j1)] = (w >> c) & 1u;
+    for (int c = 0; c < kCW; c++) xs[c * ld + swz(j1)] = (w >> c) & 1u;
   }
   __syncthreads();
-  ntt_smem<true>(xs, kCW, e1, ld, tws);
+  ntt_smem<E1, true>(xs, kCW, ld, tws);
   uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
-    Yp[o] = shoup_mul(xs[c * ld + padi(r)], __ldg(&fsf[o]));
+    Yp[o] = shoup_mul(xs[c * ld + swz(r)], __ldg(&fsf[o]));
   }
 }
 
 // Pass B.  grid (N1 / rows_per_cta, nplanes_batch).  mode 0: forward,
-// pointwise by ahat, inverse.  mode 1: forward only (used to build ahat).
-__global__ void __launch_bounds__(kQcThreads) qc_row(
-    uint32_t *__restrict__ Y, int e1, int e2, int rows_per_cta,
+// pointwise by the plane's ahat, inverse.  mode 1: forward only (used to
+// build ahat).  Plane y of the launch uses ahat.p[(ahat.first + y) / ahat.per]
+// (planes of several encodes, each with its own `a`, can share a launch).
+template <int E2>
+__global__ void __launch_bounds__(kQcThreads, 4) qc_row(
+    uint32_t *__restrict__ Y, int e1, int rows_per_cta,
     const uint2 *__restrict__ tw2f, const uint2 *__restrict__ tw2i,
-    const uint2 *__restrict__ ahat, int mode) {
+    AhatTab ahat_tab, int mode) {
   extern __shared__ uint32_t xs[];
-  const int N1 = 1 << e1, N2 = 1 << e2, ld = padded_len(N2);
+  constexpr int N2 = 1 << E2, ld = padded_len(N2);
+  const int N1 = 1 << e1;
   uint2 *twf = reinterpret_cast<uint2 *>(xs + rows_per_cta * ld + (rows_per_cta * ld & 1));
-  uint2 *twi = twf + N2 / 2;
-  stage_tw(twf, tw2f, N2 / 2);
-  if (mode == 0) stage_tw(twi, tw2i, N2 / 2);
+  uint2 *twi = twf + N2;
+  stage_tw(twf, tw2f, N2 - 1);
+  if (mode == 0) stage_tw(twi, tw2i, N2 - 1);
   const uint64_t plane = blockIdx.y;
   const int r0 = blockIdx.x * rows_per_cta;
   uint32_t *Yp = Y + (plane * N1 + r0) * uint64_t(N2);
   const int cnt = rows_per_cta * N2;
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[(i >> e2) * ld + padi(i & (N2 - 1))] = Yp[i];
+#pragma unroll 4
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[(i >> E2) * ld + swz(i & (N2 - 1))] = Yp[i];
   __syncthreads();
-  ntt_smem<true>(xs, rows_per_cta, e2, ld, twf);
+  ntt_smem<E2, true>(xs, rows_per_cta, ld, twf);
   if (mode == 0) {
-    const uint2 *ah = ahat + uint64_t(r0) * N2;
+    const uint2 *ah = ahat_tab.p[(ahat_tab.first + blockIdx.y) / ahat_tab.per] + uint64_t(r0) * N2;
+#pragma unroll 4
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      uint32_t *p = &xs[(i >> e2) * ld + padi(i & (N2 - 1))];
+      uint32_t *p = &xs[(i >> E2) * ld + swz(i & (N2 - 1))];
       *p = shoup_mul(*p, __ldg(&ah[i]));
     }
     __syncthreads();
-    ntt_smem<false>(xs, rows_per_cta, e2, ld, twi);
+    ntt_smem<E2, false>(xs, rows_per_cta, ld, twi);
   }
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) Yp[i] = xs[(i >> e2) * ld + padi(i & (N2 - 1))];
+#pragma unroll 4
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) Yp[i] = xs[(i >> E2) * ld + swz(i & (N2 - 1))];
 }
 
 // Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits.
-__global__ void __launch_bounds__(kQcThreads) qc_col_inv(
-    const uint32_t *__restrict__ Y, int e1, int e2, const uint2 *__restrict__ fsi,
+template <int E1>
+__global__ void __launch_bounds__(kQcThreads, 4) qc_col_inv(
+    const uint32_t *__restrict__ Y, int e2, const uint2 *__restrict__ fsi,
     const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes) {
   extern __shared__ uint32_t xs[];
-  const int N1 = 1 << e1, N2 = 1 << e2, ld = padded_len(N1);
+  constexpr int N1 = 1 << E1, ld = padded_len(N1);
+  const int N2 = 1 << e2;
   uint2 *tws = reinterpret_cast<uint2 *>(xs + kCW * ld + (kCW * ld & 1));
-  stage_tw(tws, tw1i, N1 / 2);
+  stage_tw(tws, tw1i, N1 - 1);
   const int c0 = blockIdx.x * kCW;
   const uint64_t plane = blockIdx.y;
   const uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
-    xs[c * ld + padi(r)] = shoup_mul(Yp[o], __ldg(&fsi[o]));
+    xs[c * ld + swz(r)] = shoup_mul(Yp[o], __ldg(&fsi[o]));
   }
   __syncthreads();
-  ntt_smem<false>(xs, kCW, e1, ld, tws);
+  ntt_smem<E1, false>(xs, kCW, ld, tws);
   uint8_t *ob = out + plane * plane_bytes;
   for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
     uint32_t byte = 0;
 #pragma unroll
     for (int c = 0; c < kCW; c++) {
-      uint32_t v = xs[c * ld + padi(j1)];
+      uint32_t v = xs[c * ld + swz(j1)];
       v = v >= kP ? v - kP : v;  // exact coefficient in [0, n]
       byte |= (v & 1u) << c;
     }
@@ -253,10 +275,13 @@ __global__ void __launch_bounds__(kQcThreads) qc_col_inv(
 }
 
 // Table generation (one-time per n).
+// Per-stage layout: entry 2^s - 1 + off (off < 2^s) = root^(off * N / 2^(s+1)).
 __global__ void qc_gen_twiddles(int lg, uint32_t root, uint2 *tw) {
-  const int half = 1 << (lg - 1);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < half; i += gridDim.x * blockDim.x)
-    tw[i] = shoup_pair(powmod(root, i));
+  const int N = 1 << lg;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N - 1; i += gridDim.x * blockDim.x) {
+    const int s = 31 - __clz(i + 1), off = i + 1 - (1 << s);
+    tw[i] = shoup_pair(powmod(root, uint64_t(off) * uint64_t(N >> (s + 1))));
+  }
 }
 __global__ void qc_gen_fourstep(int e1, int e2, uint32_t wn, uint2 *fs) {
   const uint64_t n = 1ull << (e1 + e2);
@@ -348,8 +373,8 @@ static int get_tables(cuot_ctx *ctx, int e, QcTables **out) {
   split_e(e, &t->e1, &t->e2);
   const uint64_t n = 1ull << e, N1 = 1ull << t->e1, N2 = 1ull << t->e2;
   int st = CUOT_OK;
-  if ((st = dev_alloc((void **)&t->tw1f, N1 / 2 * 8)) || (st = dev_alloc((void **)&t->tw1i, N1 / 2 * 8)) ||
-      (st = dev_alloc((void **)&t->tw2f, N2 / 2 * 8)) || (st = dev_alloc((void **)&t->tw2i, N2 / 2 * 8)) ||
+  if ((st = dev_alloc((void **)&t->tw1f, N1 * 8)) || (st = dev_alloc((void **)&t->tw1i, N1 * 8)) ||
+      (st = dev_alloc((void **)&t->tw2f, N2 * 8)) || (st = dev_alloc((void **)&t->tw2i, N2 * 8)) ||
       (st = dev_alloc((void **)&t->fsf, n * 8)) || (st = dev_alloc((void **)&t->fsi, n * 8))) {
     free_tables(t);
     return st;
@@ -382,7 +407,7 @@ void qc_free_ctx_tables(cuot_ctx *ctx) {
 
 static int col_smem(const QcTables *t) {
   const int ld = padded_len(1 << t->e1);
-  return (kCW * ld + 1) * 4 + (1 << t->e1) / 2 * 8;
+  return (kCW * ld + 1) * 4 + (1 << t->e1) * 8;
 }
 static int row_rows(const QcTables *t) {
   const int N2 = 1 << t->e2;
@@ -393,21 +418,59 @@ static int row_rows(const QcTables *t) {
 }
 static int row_smem(const QcTables *t) {
   const int ld = padded_len(1 << t->e2);
-  return (row_rows(t) * ld + 1) * 4 + (1 << t->e2) * 8;
+  return (row_rows(t) * ld + 1) * 4 + (1 << t->e2) * 16;
 }
 
+// Compile-time transform sizes: e1 in [5, 12], e2 in [5, 14].
+#define CUOT_E1_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
+#define CUOT_E2_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
+
 static int set_attrs(const QcTables *t) {
-  static bool done = false;
-  if (done) return CUOT_OK;
+  (void)t;
+  static bool done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && done[dev]) return CUOT_OK;
   const int big = 200 * 1024;
-  if (cudaFuncSetAttribute(qc_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big) != cudaSuccess ||
-      cudaFuncSetAttribute(qc_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, big) != cudaSuccess ||
-      cudaFuncSetAttribute(qc_row, cudaFuncAttributeMaxDynamicSharedMemorySize, big) != cudaSuccess) {
+  bool ok = true;
+#define SET1(E)                                                                              \
+  ok &= cudaFuncSetAttribute(qc_col_fwd<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) == cudaSuccess; \
+  ok &= cudaFuncSetAttribute(qc_col_inv<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) == cudaSuccess;
+#define SET2(E) ok &= cudaFuncSetAttribute(qc_row<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, big) == cudaSuccess;
+  CUOT_E1_CASES(SET1)
+  CUOT_E2_CASES(SET2)
+#undef SET1
+#undef SET2
+  if (!ok) {
     cudaGetLastError();
     return fail(CUOT_ECUDA, "QC smem attribute failed");
   }
-  done = true;
+  if (dev < 64) done[dev] = true;
   return CUOT_OK;
+}
+
+static void launch_col_fwd(const QcTables *t, dim3 grid, cudaStream_t st, const uint32_t *bits,
+                           uint64_t plane_words, uint32_t *Y) {
+  switch (t->e1) {
+#define L1(E) case E: qc_col_fwd<E><<<grid, kQcThreads, col_smem(t), st>>>(bits, plane_words, t->e2, t->tw1f, t->fsf, Y); break;
+    CUOT_E1_CASES(L1)
+#undef L1
+  }
+}
+static void launch_row(const QcTables *t, dim3 grid, cudaStream_t st, uint32_t *Y, const AhatTab &ahat, int mode) {
+  switch (t->e2) {
+#define L2(E) case E: qc_row<E><<<grid, kQcThreads, row_smem(t), st>>>(Y, t->e1, row_rows(t), t->tw2f, t->tw2i, ahat, mode); break;
+    CUOT_E2_CASES(L2)
+#undef L2
+  }
+}
+static void launch_col_inv(const QcTables *t, dim3 grid, cudaStream_t st, const uint32_t *Y, uint8_t *out,
+                           uint64_t plane_bytes) {
+  switch (t->e1) {
+#define L3(E) case E: qc_col_inv<E><<<grid, kQcThreads, col_smem(t), st>>>(Y, t->e2, t->fsi, t->tw1i, out, plane_bytes); break;
+    CUOT_E1_CASES(L3)
+#undef L3
+  }
 }
 
 // Computes ahat (n Shoup pairs) from a (n bits) using Y (n words) as scratch.
@@ -415,10 +478,8 @@ static int build_ahat(const QcTables *t, const uint64_t *a_d, uint32_t *Y, uint2
                       cudaStream_t st) {
   const int N1 = 1 << t->e1, N2 = 1 << t->e2;
   const uint64_t n = 1ull << t->e;
-  qc_col_fwd<<<dim3(N2 / kCW, 1), kQcThreads, col_smem(t), st>>>(
-      reinterpret_cast<const uint32_t *>(a_d), n / 32, t->e1, t->e2, t->tw1f, t->fsf, Y);
-  qc_row<<<dim3(N1 / row_rows(t), 1), kQcThreads, row_smem(t), st>>>(
-      Y, t->e1, t->e2, row_rows(t), t->tw2f, t->tw2i, nullptr, 1);
+  launch_col_fwd(t, dim3(N2 / kCW, 1), st, reinterpret_cast<const uint32_t *>(a_d), n / 32, Y);
+  launch_row(t, dim3(N1 / row_rows(t), 1), st, Y, single_ahat(nullptr), 1);
   const uint32_t ninv = powmod(uint32_t(n % kP), kP - 2);
   qc_make_ahat<<<1024, 256, 0, st>>>(Y, n, ninv, ahat);
   return launch_status(3);
@@ -432,12 +493,9 @@ static int encode_planes(const QcTables *t, const uint2 *ahat, uint64_t *planes,
   for (int p0 = 0; p0 < nplanes; p0 += batch) {
     const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
     uint64_t *pl = planes + uint64_t(p0) * (n / 64);
-    qc_col_fwd<<<dim3(N2 / kCW, nb), kQcThreads, col_smem(t), st>>>(
-        reinterpret_cast<const uint32_t *>(pl), n / 32, t->e1, t->e2, t->tw1f, t->fsf, Y);
-    qc_row<<<dim3(N1 / row_rows(t), nb), kQcThreads, row_smem(t), st>>>(
-        Y, t->e1, t->e2, row_rows(t), t->tw2f, t->tw2i, ahat, 0);
-    qc_col_inv<<<dim3(N2 / kCW, nb), kQcThreads, col_smem(t), st>>>(
-        Y, t->e1, t->e2, t->fsi, t->tw1i, reinterpret_cast<uint8_t *>(pl), n / 8);
+    launch_col_fwd(t, dim3(N2 / kCW, nb), st, reinterpret_cast<const uint32_t *>(pl), n / 32, Y);
+    launch_row(t, dim3(N1 / row_rows(t), nb), st, Y, single_ahat(ahat), 0);
+    launch_col_inv(t, dim3(N2 / kCW, nb), st, Y, reinterpret_cast<uint8_t *>(pl), n / 8);
   }
   return launch_status(3 * ((nplanes + batch - 1) / batch));
 }
@@ -460,6 +518,48 @@ static int default_batch(uint64_t n, int nplanes) {
 
 int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
                      uint64_t col_hi, void *out, cudaStream_t st);
+
+// ---- helpers for the batched engine (batch.cu) ----------------------------
+int qc_prepare(cuot_ctx *ctx, int e) {
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  return set_attrs(t);
+}
+
+int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, uint32_t *Y, uint2 *ahat, cudaStream_t st) {
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  return build_ahat(t, a_d, Y, ahat, st);
+}
+
+// Encodes `njobs` consecutive groups of 128 planes in place; group j uses
+// ahats[j] (host array of device pointers).  Y holds `batch` planes.
+int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const uint2 *const *ahats,
+                   uint32_t *Y, int batch, cudaStream_t st) {
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  const int N1 = 1 << t->e1, N2 = 1 << t->e2;
+  const uint64_t n = 1ull << e;
+  const int nplanes = 128 * njobs;
+  // a launch may span at most kAhatTab jobs
+  if (batch > 128 * (kAhatTab - 1)) batch = 128 * (kAhatTab - 1);
+  int launches = 0;
+  for (int p0 = 0; p0 < nplanes; p0 += batch) {
+    const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
+    uint64_t *pl = planes + uint64_t(p0) * (n / 64);
+    AhatTab tab{};
+    tab.per = 128;
+    tab.first = p0 % 128;
+    for (int j = 0; j < kAhatTab && p0 / 128 + j < njobs; j++) tab.p[j] = ahats[p0 / 128 + j];
+    launch_col_fwd(t, dim3(N2 / kCW, nb), st, reinterpret_cast<const uint32_t *>(pl), n / 32, Y);
+    launch_row(t, dim3(N1 / row_rows(t), nb), st, Y, tab, 0);
+    launch_col_inv(t, dim3(N2 / kCW, nb), st, Y, reinterpret_cast<uint8_t *>(pl), n / 8);
+    launches += 3;
+  }
+  return launch_status(launches);
+}
+
+int qc_default_batch(uint64_t n, int nplanes) { return default_batch(n, nplanes); }
 
 }  // namespace cuot
 

@@ -287,3 +287,41 @@ def test_sot_end_to_end_cot_n20(ctx):
     assert not diff[~cbits].any()
     assert (diff[cbits] == delta).all()
     assert 0.4 < cbits.mean() < 0.6
+
+
+# ---------------------------------------------------------------- row-range LPN / sharding
+@pytest.mark.parametrize("n,k,cuts", [(4096, 1000, [0, 1024, 2048, 4096]), (1003, 77, [0, 500, 1003]),
+                                      (10, 5, [0, 4, 8, 10])])
+def test_lpn_row_ranges_equal_unsplit(ctx, n, k, cuts):
+    rng = np.random.default_rng(n)
+    seed, kk, e = rng_blocks(rng, 1)[0], rng_blocks(rng, k), rng_blocks(rng, n)
+    exp = oracle.lpn_primal(seed, kk, e, threads=4)
+    dkk = to_dev(kk)
+    for lo, hi in zip(cuts[:-1], cuts[1:]):
+        part = to_dev(e[lo:hi])
+        ctx.lpn_primal_range(seed, dkk, part, lo, hi, n)
+        assert np.array_equal(to_host(part), exp[lo:hi])
+
+
+def test_sharded_ferret_extend_equals_unsplit(ctx):
+    """The per-rank share computation of cuot_b200.shard, run for each of 3
+    ranks in turn on this GPU, concatenates to the unsplit extension."""
+    from cuot_b200.shard import ShardPlan, ferret_extend_rank
+    t, h, k = 10, 8, 999
+    rng = np.random.default_rng(31)
+    roots, delta = rng_blocks(rng, t), delta_ferret(rng)
+    choice = rng.integers(0, 2, t * h).astype(np.uint8)
+    seed, kk_s, kk_r = rng_blocks(rng, 1)[0], rng_blocks(rng, k), rng_blocks(rng, k)
+    plan = ShardPlan(t, h, 3)
+    vs, ws = [], []
+    for r in range(3):
+        f, tr = plan.first_tree(r), plan.trees(r)
+        v, w = ferret_extend_rank(ctx, plan, r, to_dev(roots[f:f + tr]), delta,
+                                  to_dev(choice[f * h:(f + tr) * h]), seed, to_dev(kk_s), to_dev(kk_r))
+        vs.append(to_host(v))
+        ws.append(to_host(w))
+    leaves, lsum, rsum, ss = oracle.ferret_pprf_sender(roots, h, delta, threads=4)
+    mc = np.where(choice[:, None] == 0, lsum, rsum)
+    rleaves = oracle.ferret_pprf_recver(mc, choice, ss, h, threads=4)
+    assert np.array_equal(np.concatenate(vs), oracle.lpn_primal(seed, kk_s, leaves))
+    assert np.array_equal(np.concatenate(ws), oracle.lpn_primal(seed, kk_r, rleaves))
