@@ -5,6 +5,10 @@ receiver) of one OT-extension instance, seeded synthetic inputs of the named
 shape.
 
 Workloads (--workload):
+  mixed64     batched mix: 64 instances, half SOT and
+              half Ferret-style, log2 n uniform in [16, 22], depth 10-14; run
+              as one CUDA-graph device program (value) and one instance at a
+              time through the plain entry points (plain.value).
   sot_n20     plain SOT, n = 2^20: 256 GGM trees of depth 12 (both roles),
               exact quasi-cyclic encode of the 128 bit planes of the 2n-bit
               (zero-padded) noise vector, transposes both ways, plus the
@@ -39,15 +43,24 @@ sys.path.insert(0, ROOT)
 import numpy as np
 
 WORKLOADS = {
+    "mixed64": dict(kind="batch", count=64, lo=16, hi=22),
     "sot_n20": dict(kind="sot", t=256, h=12),
     "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
     "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
 }
 CONFIG_TEXT = {
+    "mixed64": "batched mix: 64 instances (32 SOT, 32 Ferret-style), log2 n uniform in [16,22], depth 10-14, "
+               "both roles, one CUDA-graph program vs the plain one-instance-at-a-time path",
     "sot_n20": "plain SOT n=2^20: 256 GGM trees depth 12, exact QC encode of 128 planes, transposes (both roles)",
     "ferret_b13": "plain Ferret ferret_b13: n=10485760, t=1280, h=13, k=452000, d=10 (both roles)",
     "ferret_c1": "plain Ferret small: n=65536, t=64, h=10, k=8192, d=10 (both roles)",
 }
+
+
+def metric_name(workload: str) -> str:
+    if WORKLOADS[workload]["kind"] == "batch":
+        return "COTs/sec on 1 B200, batched vs plain path (bit-exact)"
+    return "COTs/sec on 1 B200 (plain path, bit-exact)"
 
 
 def log(*a):
@@ -321,14 +334,32 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     vals = []
     sample = ""
+    spec = WORKLOADS[name]
+    if spec["kind"] == "batch":
+        # the mix's COTs split by kind (same generator as the GPU arm, no device)
+        rng = np.random.default_rng(2024)
+        n_sot = n_fer = 0
+        for i in range(spec["count"]):
+            e = int(rng.integers(spec["lo"], spec["hi"] + 1))
+            rng.integers(10, min(14, e) + 1)
+            if i % 2 == 0:
+                n_sot += 1 << e
+            else:
+                n_fer += 1 << e
     for i in range(args.warmup + args.steps):
-        v, sample = cpu_sample(name, threads, budget_s=5.0)
+        if spec["kind"] == "batch":
+            v1, s1 = cpu_sample("sot_n20", threads, budget_s=2.0)
+            v2, s2 = cpu_sample("ferret_b13", threads, budget_s=2.0)
+            v = (n_sot + n_fer) / (n_sot / v1 + n_fer / v2)
+            sample = f"SOT: {s1}; Ferret: {s2}; weighted by the mix's COTs"
+        else:
+            v, sample = cpu_sample(name, threads, budget_s=5.0)
         if i >= args.warmup:
             vals.append(v)
     v = statistics.median(vals)
     unit = "COTs/s"
     print(json.dumps({
-        "impl": "reference", "metric": "COTs/sec on 1 B200 (plain path, bit-exact)", "value": v, "unit": unit,
+        "impl": "reference", "metric": metric_name(name), "value": v, "unit": unit,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
         "config": {"workload": name, "what": CONFIG_TEXT[name]},
@@ -340,9 +371,144 @@ def run_reference(args):
     return 0
 
 
+def run_batch(args):
+    """the mixed batch, batched (graph) vs plain."""
+    import torch
+    import cuot_b200
+    from cuot_b200.batch import KIND_FERRET, Batch, mixed_workload
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    spec = WORKLOADS[args.workload]
+    ctx = cuot_b200.Context(local)
+    insts = mixed_workload(ctx, count=spec["count"], seed=2024 + rank, lo=spec["lo"], hi=spec["hi"])
+    cots = sum(i.n for i in insts)
+    stream = torch.cuda.Stream()
+    batch = Batch(ctx, insts, use_graph=True)
+    for _ in range(args.warmup):
+        batch.run(stream)
+        batch.run_plain(stream)
+    torch.cuda.synchronize()
+    launches = batch.kernels_per_run()
+    phases = batch.run_phases(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            evs[i][0].record(stream)
+            fn(stream)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        if dist:
+            tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = tt.item()
+        return ms
+
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    ms = timed(batch.run)
+    clocks = clk.stop()
+    ms_plain = timed(batch.run_plain)
+
+    # e2e: inputs from pinned host memory, outputs back, through the public API
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    host_in, host_out = [], []
+    for i in insts:
+        ins = [(pin(i.roots), i.d_roots), (pin(i.choice), i.d_choice)]
+        if i.kind == KIND_FERRET:
+            ins += [(pin(i.kk_s), i.d_kk_s), (pin(i.kk_r), i.d_kk_r)]
+        else:
+            ins += [(pin(i.base0), i.d_b0), (pin(i.base1), i.d_b1), (pin(i.mc), i.d_mc)]
+        outs = [(torch.empty_like(i.v, device="cpu").pin_memory(), i.v), (torch.empty_like(i.w, device="cpu").pin_memory(), i.w)]
+        if i.kind != KIND_FERRET:
+            outs.append((torch.empty_like(i.cbits, device="cpu").pin_memory(), i.cbits))
+        host_in += ins
+        host_out += outs
+    h2d = sum(hs.numel() * hs.element_size() for hs, _ in host_in)
+    d2h = sum(hs.numel() * hs.element_size() for hs, _ in host_out)
+
+    def e2e(st):
+        with torch.cuda.stream(st):
+            for hs, dv in host_in:
+                dv.copy_(hs, non_blocking=True)
+        batch.run(st)
+        with torch.cuda.stream(st):
+            for hs, dv in host_out:
+                hs.copy_(dv, non_blocking=True)
+    e2e(stream)
+    e2e_ms = timed(e2e)
+
+    names = ["pprf_send", "pprf_recv", "lpn", "sot_encode"]
+    stages = dict(zip(names, phases))
+    n_sot = sum(i.n for i in insts if i.kind != KIND_FERRET)
+    n_fer = cots - n_sot
+    k_fer = sum(i.k for i in insts if i.kind == KIND_FERRET)
+    alg = {"pprf_send": 16 * cots, "pprf_recv": 16 * cots, "lpn": 2 * 32 * n_fer + 2 * 16 * k_fer,
+           "sot_encode": 2 * 3 * 32 * n_sot}
+    dom = max(stages, key=lambda k: stages[k])
+    peaks, peak_kind = measured_peaks()
+    achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
+    out = {
+        "metric": metric_name(args.workload),
+        "value": world * cots / (ms / 1e3), "unit": "COTs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "instances": len(insts),
+                   "cots_per_step_per_gpu": cots, "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed steps (L2 flush)"},
+        "plain": {"value": world * cots / (ms_plain / 1e3), "ms_per_step": ms_plain,
+                  "batched_over_plain": ms_plain / ms},
+        "stages_ms": stages,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "algorithmic_bytes_per_step": alg[dom]},
+        "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sample = cpu_sample("sot_n20", threads, budget_s=5.0)
+        v2, sample2 = cpu_sample("ferret_b13", threads, budget_s=5.0)
+        # per-COT CPU cost of each kind, weighted by the mix
+        cpu_ms = (n_sot / v + n_fer / v2) * 1e3
+        out["cpu_baseline"] = {"value": cots / (cpu_ms / 1e3), "unit": "COTs/s", "cores": threads, "kind": "port",
+                               "sample": f"SOT: {sample}; Ferret: {sample2}; weighted by the mix's COTs"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    batch.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
     import cuot_b200
+
+    if WORKLOADS[args.workload]["kind"] == "batch":
+        return run_batch(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -433,7 +599,7 @@ def run_ours(args):
         with open(tp) as f:
             traffic = json.load(f).get(f"{args.workload}:{dom}")
     out = {
-        "metric": "COTs/sec on 1 B200 (plain path, bit-exact)",
+        "metric": metric_name(args.workload),
         "value": value, "unit": "COTs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded)",
@@ -469,7 +635,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sot_n20", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

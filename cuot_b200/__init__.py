@@ -127,6 +127,11 @@ class Context:
                                         _stream(stream)), "cuot_aes128_ecb")
         return io
 
+    def prg_fill(self, seed, out, block_offset: int = 0, stream=None):
+        _check(self.lib.cuot_prg_fill(self.h, _host_block(seed), C.c_uint64(block_offset), _ptr(out),
+                                      C.c_uint64(_nblocks(out)), _stream(stream)), "cuot_prg_fill")
+        return out
+
     # ---- Ferret ------------------------------------------------------------
     def ferret_pprf_sender(self, roots, h: int, delta, leaves, lsum, rsum, secret_sum, stream=None):
         t = _nblocks(roots)

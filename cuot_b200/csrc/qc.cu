@@ -311,6 +311,15 @@ __global__ void qc_make_counters(Blk *b, uint64_t nb) {
   }
 }
 
+// Counter blocks of the cryptoTools PRNG stream: block i = (lo = off + i, hi = 0).
+__global__ void prg_make_counters(Blk *b, uint64_t nb, uint64_t off) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nb;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t c = off + i;
+    b[i] = Blk{{uint32_t(c), uint32_t(c >> 32), 0u, 0u}};
+  }
+}
+
 // Sparse encode: out = XOR_i rot(a, pos_i), one thread per output word.
 __global__ void qc_sparse(const uint64_t *__restrict__ a, const uint64_t *__restrict__ pos,
                           int weight, uint64_t n, uint64_t *__restrict__ out) {
@@ -583,6 +592,17 @@ int cuot_qc_gen_a(cuot_ctx *ctx, const uint8_t key[16], uint64_t n, uint64_t *a_
   qc_make_counters<<<256, 256, 0, static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<Blk *>(a_d), nb);
   CUOT_TRY(launch_status());
   return cuot_aes128_ecb(ctx, key, reinterpret_cast<cuot_block *>(a_d), nb, stream);
+}
+
+int cuot_prg_fill(cuot_ctx *ctx, const uint8_t seed[16], uint64_t block_offset, cuot_block *out_d,
+                  uint64_t nblocks, void *stream) {
+  if (!ctx || !seed || (!out_d && nblocks)) return fail(CUOT_EINVAL, "null argument");
+  if (nblocks == 0) return CUOT_OK;
+  DeviceGuard g(ctx);
+  prg_make_counters<<<512, 256, 0, static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<Blk *>(out_d), nblocks,
+                                                                        block_offset);
+  CUOT_TRY(launch_status());
+  return cuot_aes128_ecb(ctx, seed, out_d, nblocks, stream);
 }
 
 int cuot_qc_plan_create(cuot_ctx *ctx, const uint64_t *a_d, uint64_t n, void *stream,

@@ -58,6 +58,13 @@ uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
 int cuot_aes128_ecb(cuot_ctx *ctx, const uint8_t key[16], cuot_block *io_d,
                     uint64_t nblocks, void *stream);
 
+/* Seeded PRG on the device: blocks [block_offset, +nblocks) of the
+ * cryptoTools PRNG stream for `seed` (block i = AES_seed(i as a little-endian
+ * 128-bit counter), silent/lib/cryptoTools/Crypto/PRNG.cpp:44-56,100-106).
+ * Used to derive request inputs without a host round-trip. */
+int cuot_prg_fill(cuot_ctx *ctx, const uint8_t seed[16], uint64_t block_offset,
+                  cuot_block *out_d, uint64_t nblocks, void *stream);
+
 /* ---- Ferret MPCOT: t GGM trees of depth h --------------------------------
  * Node function: emp-ot TwoKeyPRP (ferret/twokeyprp.h:7-63): left =
  * AES_0(p) ^ p, right = AES_{makeBlock(0,1)}(p) ^ p.
@@ -191,6 +198,72 @@ int cuot_qc_plan_set_batch(cuot_qc_plan *plan, int planes_per_batch);
 int cuot_qc_plan_encode(cuot_qc_plan *plan, uint64_t *planes_io_d,
                         int nplanes, void *stream);
 int cuot_qc_plan_dual_lpn(cuot_qc_plan *plan, cuot_block *io_d, void *stream);
+
+/* ---- batched engine ------------------------------------------------------
+ * Many OT-extension instances of uneven n and depth, both roles each, run as
+ * one device program: one persistent PPRF launch over all trees of all
+ * senders (per-tree work queue, deepest trees first), one over all
+ * receivers, one persistent LPN launch over all Ferret rows of both roles,
+ * and for SOT one set of NTT passes per transform size spanning the planes
+ * of every instance of that size.  On first run the whole program is
+ * captured into a CUDA graph (cfg.use_graph) and replayed afterwards.
+ * No counterpart call in the reference, which runs one instance per call
+ * (FerretCOT::extend, ferret_cot.hpp:80-91; SOT roles, silent/roles.h).
+ * Each item produces v (sender) and w (receiver) with w = v except on the
+ * COT positions (Ferret: w_i = v_i ^ delta at the punctured leaves' images
+ * after LPN; SOT: w_j = v_j ^ c_j * delta with c = a * e). */
+#define CUOT_KIND_FERRET 0
+#define CUOT_KIND_SOT 1
+
+typedef struct {
+  int kind;                       /* CUOT_KIND_* */
+  int h;                          /* tree depth, 1..20 */
+  uint64_t t;                     /* trees; n = t << h */
+  cuot_block delta;               /* correlation delta */
+  const cuot_block *roots_d;      /* [t] sender tree roots */
+  const uint8_t *choice_d;        /* Ferret [t][h], SOT [h][t] */
+  cuot_block *v_d;                /* [n] out: sender output */
+  cuot_block *w_d;                /* [n] out: receiver output */
+  /* Ferret */
+  int64_t k;                      /* LPN inputs */
+  int d;                          /* LPN terms per row */
+  uint8_t lpn_seed[16];
+  const cuot_block *kk_send_d;    /* [k] */
+  const cuot_block *kk_recv_d;    /* [k] */
+  /* SOT (n a power of two in [2^10, 2^26]) */
+  const cuot_block *base0_d;      /* [h][t] sender base-OT messages */
+  const cuot_block *base1_d;      /* [h][t] */
+  const cuot_block *mc_d;         /* [h][t] receiver's chosen messages */
+  const uint64_t *a_d;            /* [n/64] QC polynomial */
+  const uint64_t *punct_d;        /* [t] receiver's punctured leaf indices */
+  uint64_t *cbits_d;              /* [n/64] out: receiver choice bits a*e */
+} cuot_batch_item;
+
+typedef struct {
+  int ctas_per_sm;         /* persistent PPRF/LPN grid: CTAs per SM (0: 3) */
+  int lpn_rows_per_task;   /* LPN work-queue granularity, multiple of 4 (0: 65536) */
+  int qc_planes_per_pass;  /* planes per NTT pass (0: ~64 MiB of intermediate) */
+  int use_graph;           /* capture into a CUDA graph on first run */
+} cuot_batch_config;
+
+typedef struct cuot_batch cuot_batch;
+/* Validates the items, allocates the batch's device state and transforms
+ * every SOT item's `a` (synchronises the device). */
+int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
+                      const cuot_batch_config *cfg, cuot_batch **out);
+/* One step: every item, both roles, on `stream` (the same stream for every
+ * run when graphs are used). */
+int cuot_batch_run(cuot_batch *b, void *stream);
+/* The same items through the single-instance entry points, one instance at
+ * a time (the plain path the batched form is compared with). */
+int cuot_batch_run_plain(cuot_batch *b, void *stream);
+int cuot_batch_destroy(cuot_batch *b);
+/* Kernels launched by one batched run (known after the first run). */
+int cuot_batch_kernels_per_run(const cuot_batch *b);
+/* Diagnostic: the batched program without a graph, timed per phase with
+ * events (synchronises): phase_ms[0..3] = sender PPRF (+ OT selection),
+ * receiver PPRF, LPN, SOT encodes. */
+int cuot_batch_run_phases(cuot_batch *b, void *stream, float *phase_ms);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,70 @@
+"""Batched engine: a mixed batch (Ferret-style and SOT instances of uneven n
+and depth) run as one device program (CUDA graph) must give, for every
+instance, exactly the single-instance path's outputs and the oracle's."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+from cuot_b200.batch import KIND_FERRET, KIND_SOT, Batch, Instance, mixed_workload  # noqa: E402
+
+
+def oracle_outputs(inst):
+    if inst.kind == KIND_FERRET:
+        lv, ls, rs, ss = oracle.ferret_pprf_sender(inst.roots, inst.h, inst.delta, threads=8)
+        mc = np.where(inst.choice[:, None] == 0, ls, rs)
+        rl = oracle.ferret_pprf_recver(mc, inst.choice, ss, inst.h, threads=8)
+        return (oracle.lpn_primal(inst.seed, inst.kk_s, lv, d=inst.d, threads=8),
+                oracle.lpn_primal(inst.seed, inst.kk_r, rl, d=inst.d, threads=8), None)
+    lv, m0, m1 = oracle.sot_pprf_sender(inst.roots, inst.h, inst.delta, inst.base0, inst.base1, threads=8)
+    rl = oracle.sot_pprf_recver(m0, m1, inst.mc, inst.choice, inst.t, inst.h, threads=8)
+    a = inst.a.cpu().numpy().view(np.uint64)
+    return (oracle.sot_dual_lpn(a, lv, inst.n, threads=8), oracle.sot_dual_lpn(a, rl, inst.n, threads=8),
+            oracle.qc_encode_sparse(a, inst.punct.astype(np.uint64), inst.n))
+
+
+def snapshot(insts):
+    torch.cuda.synchronize()
+    return [(i.v.cpu().numpy().copy(), i.w.cpu().numpy().copy(),
+             None if i.kind == KIND_FERRET else i.cbits.cpu().numpy().view(np.uint64).copy()) for i in insts]
+
+
+def test_mixed_batch_equals_plain_and_oracle(ctx):
+    specs = [(KIND_FERRET, 8, 10, 1000), (KIND_SOT, 4, 10, 0), (KIND_FERRET, 3, 12, 77), (KIND_SOT, 16, 10, 0),
+             (KIND_FERRET, 64, 10, 8192), (KIND_SOT, 2, 11, 0), (KIND_FERRET, 5, 1, 9), (KIND_SOT, 1, 12, 0)]
+    insts = [Instance(ctx, kd, t, h, 100 + i, k=k) for i, (kd, t, h, k) in enumerate(specs)]
+    stream = torch.cuda.Stream()
+    b = Batch(ctx, insts, use_graph=True)
+    b.run(stream)        # captures the graph and runs it
+    b.run(stream)        # replays: a second run must give the same outputs
+    got = snapshot(insts)
+    assert b.kernels_per_run() > 0
+    for inst in insts:   # clobber the outputs before the plain run
+        inst.v.zero_(); inst.w.zero_()
+    b.run_plain(stream)
+    plain = snapshot(insts)
+    for inst, g, p in zip(insts, got, plain):
+        ev, ew, ec = oracle_outputs(inst)
+        assert np.array_equal(g[0], ev) and np.array_equal(g[1], ew)
+        assert np.array_equal(p[0], ev) and np.array_equal(p[1], ew)
+        if ec is not None:
+            assert np.array_equal(g[2], ec) and np.array_equal(p[2], ec)
+    b.close()
+
+
+def test_configs3_shaped_mix_is_a_cot_everywhere(ctx):
+    """A smaller configs[3]-shaped mix (log2 n in [12, 16]); every instance's
+    outputs satisfy the COT correlation against its own delta."""
+    insts = mixed_workload(ctx, count=10, seed=7, lo=12, hi=16)
+    stream = torch.cuda.Stream()
+    b = Batch(ctx, insts, use_graph=True)
+    b.run(stream)
+    torch.cuda.synchronize()
+    for inst in insts:
+        v, w = inst.v.cpu().numpy(), inst.w.cpu().numpy()
+        ev, ew, ec = oracle_outputs(inst)
+        assert np.array_equal(v, ev) and np.array_equal(w, ew)
+    b.close()
