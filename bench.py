@@ -391,7 +391,13 @@ def run_batch(args):
     insts = mixed_workload(ctx, count=spec["count"], seed=2024 + rank, lo=spec["lo"], hi=spec["hi"])
     cots = sum(i.n for i in insts)
     stream = torch.cuda.Stream()
-    batch = Batch(ctx, insts, use_graph=True)
+    tuned = {}
+    if not args.no_autotune:
+        from cuot_b200.autotune import DEFAULT_TABLE, TuningTable, tune_batch
+        out_dir = os.path.join(ROOT, "gpurun_out")
+        path = os.path.join(out_dir, "tuning.json") if os.path.isdir(out_dir) else DEFAULT_TABLE
+        tuned, _ = tune_batch(ctx, insts, table=TuningTable(path))
+    batch = Batch(ctx, insts, use_graph=True, **tuned)
     for _ in range(args.warmup):
         batch.run(stream)
         batch.run_plain(stream)
@@ -476,6 +482,7 @@ def run_batch(args):
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "plain": {"value": world * cots / (ms_plain / 1e3), "ms_per_step": ms_plain,
                   "batched_over_plain": ms_plain / ms},
+        "autotuned": tuned,
         "stages_ms": stages,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": None,
@@ -486,6 +493,9 @@ def run_batch(args):
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }
+    batch.close()
+    if args.serve_requests > 0:
+        out["served"] = run_served(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample("sot_n20", threads, budget_s=5.0)
@@ -496,11 +506,40 @@ def run_batch(args):
                                "sample": f"SOT: {sample}; Ferret: {sample2}; weighted by the mix's COTs"}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    batch.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_served(args, device: int) -> dict:
+    """served request stream.  Saturation throughput of the
+    continuous-batching server sets the sustained rate (90 % of it); the
+    same Poisson stream is then served by the continuous-batching server and
+    by plain per-request execution (one request at a time)."""
+    import torch
+    from cuot_b200.serve import GpuExecutor, Server, make_stream, sustained_rate
+
+    lo, hi = 14, 24
+    cont = GpuExecutor(slots=args.serve_slots, device=device, max_log_n=hi)
+    probe = make_stream(min(100, args.serve_requests), rate=0.0, seed=5, lo=lo, hi=hi)
+    rate = sustained_rate(cont, probe)
+    reqs = make_stream(args.serve_requests, rate=rate, seed=6, lo=lo, hi=hi)
+    rep = Server(cont, budget_bytes=120e9).run(reqs)
+    del cont
+    torch.cuda.synchronize()
+    plain = GpuExecutor(slots=1, device=device, max_log_n=hi)
+    for r in reqs:
+        r.status, r.result = "pending", None
+    rep_plain = Server(plain, budget_bytes=120e9).run(reqs)
+    del plain
+    keys = ("done", "cots_per_s", "p50_ms", "p99_ms", "mean_ms", "wall_s")
+    return {"requests": args.serve_requests, "slots": args.serve_slots, "budget_gb": 120,
+            "log2_n": [lo, hi], "rate_rps": rate,
+            "continuous": {k: rep[k] for k in keys},
+            "plain_per_request": {k: rep_plain[k] for k in keys},
+            "note": "latency = arrival -> outputs in device memory; rate = 0.9 x saturation throughput "
+                    "of the continuous-batching server"}
 
 
 def run_ours(args):
@@ -637,6 +676,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=300,
+                    help="requests of the served stream reported with mixed64 (0: skip; configs[4] uses 10000)")
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -121,6 +121,11 @@ class Context:
     def scratch_bytes(self) -> int:
         return int(self.lib.cuot_ctx_scratch_bytes(self.h))
 
+    TUNE_PPRF_THREADS, TUNE_QC_PLANES = 1, 2
+
+    def set_tuning(self, key: int, value: int):
+        _check(self.lib.cuot_ctx_set_tuning(self.h, C.c_int(key), C.c_int64(value)), "cuot_ctx_set_tuning")
+
     # ---- AES ---------------------------------------------------------------
     def aes128_ecb(self, key, io, stream=None):
         _check(self.lib.cuot_aes128_ecb(self.h, _host_block(key), _ptr(io), C.c_uint64(_nblocks(io)),

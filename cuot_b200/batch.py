@@ -28,8 +28,8 @@ class BatchItem(C.Structure):
 
 
 class BatchConfig(C.Structure):
-    _fields_ = [("ctas_per_sm", C.c_int), ("lpn_rows_per_task", C.c_int), ("qc_planes_per_pass", C.c_int),
-                ("use_graph", C.c_int)]
+    _fields_ = [("pprf_threads", C.c_int), ("ctas_per_sm", C.c_int), ("lpn_rows_per_task", C.c_int),
+                ("qc_planes_per_pass", C.c_int), ("use_graph", C.c_int)]
 
 
 class Instance:
@@ -83,11 +83,11 @@ class Instance:
 
 
 class Batch:
-    def __init__(self, ctx, instances, ctas_per_sm: int = 0, lpn_rows_per_task: int = 0,
+    def __init__(self, ctx, instances, pprf_threads: int = 0, ctas_per_sm: int = 0, lpn_rows_per_task: int = 0,
                  qc_planes_per_pass: int = 0, use_graph: bool = True):
         self.lib, self.ctx, self.instances = load(), ctx, list(instances)
         arr = (BatchItem * len(self.instances))(*[i.item() for i in self.instances])
-        cfg = BatchConfig(ctas_per_sm, lpn_rows_per_task, qc_planes_per_pass, int(use_graph))
+        cfg = BatchConfig(pprf_threads, ctas_per_sm, lpn_rows_per_task, qc_planes_per_pass, int(use_graph))
         h = C.c_void_p()
         _check(self.lib.cuot_batch_create(ctx.h, arr, C.c_int(len(self.instances)), C.byref(cfg), C.byref(h)),
                "cuot_batch_create")

@@ -165,6 +165,7 @@ struct cuot_batch {
   // PPRF
   PprfBatchArgs send{}, recv{};
   int pprf_grid = 0;
+  int pprf_threads = 256;
   // Ferret selection
   SelItem *sel_d = nullptr;
   int nsel = 0;
@@ -269,7 +270,7 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
   int launches = 0;
   mark(0);
   if (b->send.ntasks) {
-    pprf_batch_kernel<<<b->pprf_grid, kPprfThreads, kTableBytes, st>>>(b->send);
+    pprf_batch_kernel<<<b->pprf_grid, b->pprf_threads, kTableBytes, st>>>(b->send);
     launches++;
   }
   if (b->nsel) {
@@ -279,7 +280,7 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
   }
   mark(1);
   if (b->recv.ntasks) {
-    pprf_batch_kernel<<<b->pprf_grid, kPprfThreads, kTableBytes, st>>>(b->recv);
+    pprf_batch_kernel<<<b->pprf_grid, b->pprf_threads, kTableBytes, st>>>(b->recv);
     launches++;
   }
   mark(2);
@@ -335,6 +336,9 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   const int per_sm = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : 3;
+  if (b->cfg.pprf_threads != 0 && b->cfg.pprf_threads != 128 && b->cfg.pprf_threads != 256)
+    return cleanup(fail(CUOT_EINVAL, "pprf_threads must be 128 or 256"));
+  b->pprf_threads = b->cfg.pprf_threads ? b->cfg.pprf_threads : 256;
 
   // ---- per-item device state
   b->lsum.assign(count, nullptr); b->rsum.assign(count, nullptr); b->ss.assign(count, nullptr);

@@ -87,6 +87,8 @@ int cuot_ctx_create(int device, cuot_ctx **out) {
   }
   cuot_ctx *c = new cuot_ctx{};
   c->device = device;
+  c->pprf_threads = 256;
+  c->qc_planes_per_pass = 0;
   int st = CUOT_OK;
   if (cudaMalloc(&c->t0_d, 256 * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
@@ -128,5 +130,21 @@ int cuot_ctx_reserve(cuot_ctx *c, uint64_t bytes) {
 }
 
 uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *c) { return c ? c->scratch_bytes : 0; }
+
+int cuot_ctx_set_tuning(cuot_ctx *c, int key, int64_t value) {
+  if (!c) return fail(CUOT_EINVAL, "ctx is null");
+  switch (key) {
+    case CUOT_TUNE_PPRF_THREADS:
+      if (value != 128 && value != 256) return fail(CUOT_EINVAL, "threads per tree must be 128 or 256");
+      c->pprf_threads = int(value);
+      return CUOT_OK;
+    case CUOT_TUNE_QC_PLANES:
+      if (value < 0 || value > 4096) return fail(CUOT_EINVAL, "planes per pass out of range");
+      c->qc_planes_per_pass = int(value);
+      return CUOT_OK;
+    default:
+      return fail(CUOT_EINVAL, "unknown tuning key %d", key);
+  }
+}
 
 }  // extern "C"

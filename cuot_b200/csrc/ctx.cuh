@@ -8,6 +8,8 @@ struct cuot_ctx {
   void *scratch;           // grow-only scratch arena
   uint64_t scratch_bytes;
   void *qc_tables[32];     // NTT twiddle tables per log2(n) (qc.cu)
+  int pprf_threads;        // threads per tree CTA (128 or 256)
+  int qc_planes_per_pass;  // 0: automatic
 };
 
 namespace cuot {

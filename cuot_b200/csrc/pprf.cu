@@ -44,7 +44,7 @@ static int launch_pprf(cuot_ctx *ctx, PprfArgs &a, cudaStream_t st) {
   void *scr = nullptr;
   CUOT_TRY(scratch(ctx, (a.t << a.h) * sizeof(Blk), &scr));
   a.scratch = static_cast<Blk *>(scr);
-  pprf_tree_kernel<MODE><<<dim3((unsigned)a.t), kPprfThreads, kTableBytes, st>>>(a);
+  pprf_tree_kernel<MODE><<<dim3((unsigned)a.t), ctx->pprf_threads, kTableBytes, st>>>(a);
   return launch_status();
 }
 

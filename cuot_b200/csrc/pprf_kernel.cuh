@@ -45,6 +45,8 @@ struct PprfArgs {
   const Blk *m0_in, *m1_in;
 };
 
+// Threads per tree (CTA size): 256 by default, 128 selectable (tuning);
+// the kernels are compiled for at most kPprfThreads.
 constexpr int kPprfThreads = 256;
 
 __device__ __forceinline__ Blk mask_lsb(Blk b) {
@@ -59,7 +61,7 @@ struct PprfSmem {
 };
 
 // Expands tree `tree` of the instance described by `a` with the whole CTA
-// (kPprfThreads threads).  scratch_tree: 2^h blocks for the level ping-pong.
+// (blockDim.x <= kPprfThreads threads, a multiple of 32).  scratch_tree: 2^h blocks for the level ping-pong.
 // The T-table must already be staged (and synced) in shared memory.
 template <int MODE>
 __device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk *scratch_tree,
@@ -81,7 +83,7 @@ __device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk 
     const bool last = (l == h - 1);
     const uint64_t np = 1ull << l;
     Blk accL{{0, 0, 0, 0}}, accR{{0, 0, 0, 0}};
-    for (uint64_t i = tid; i < np; i += kPprfThreads) {
+    for (uint64_t i = tid; i < np; i += blockDim.x) {
       const Blk p = (l == 0) ? root : ld_blk(in + i);
       uint32_t L[4] = {p.w[0], p.w[1], p.w[2], p.w[3]};
       uint32_t R[4] = {p.w[0], p.w[1], p.w[2], p.w[3]};
@@ -112,7 +114,7 @@ __device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk 
     if (tid == 0) {
       Blk S[2] = {{{0, 0, 0, 0}}, {{0, 0, 0, 0}}};
 #pragma unroll
-      for (int w = 0; w < kPprfThreads / 32; w++) {
+      for (int w = 0; w < int(blockDim.x >> 5); w++) {
         S[0] = blk_xor(S[0], red[0][w]);
         S[1] = blk_xor(S[1], red[1][w]);
       }

@@ -627,7 +627,7 @@ int cuot_qc_plan_create(cuot_ctx *ctx, const uint64_t *a_d, uint64_t n, void *st
     delete pl;
     return st;
   }
-  pl->batch = default_batch(n, 128);
+  pl->batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
   *out = pl;
   return CUOT_OK;
 }
@@ -686,7 +686,8 @@ int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, ui
   QcTables *t;
   CUOT_TRY(get_tables(ctx, e, &t));
   CUOT_TRY(set_attrs(t));
-  const int batch = default_batch(n, nplanes);
+  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, nplanes);
+  if (batch > nplanes) batch = nplanes;
   void *scr;
   CUOT_TRY(scratch(ctx, n * 8 + uint64_t(batch) * n * 4, &scr));
   uint2 *ahat = static_cast<uint2 *>(scr);
@@ -705,7 +706,8 @@ int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d, uint
   QcTables *t;
   CUOT_TRY(get_tables(ctx, e, &t));
   CUOT_TRY(set_attrs(t));
-  const int batch = default_batch(n, 128);
+  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
+  if (batch > 128) batch = 128;
   void *scr;
   CUOT_TRY(scratch(ctx, n * 8 + n * 16 + uint64_t(batch) * n * 4, &scr));
   uint2 *ahat = static_cast<uint2 *>(scr);

@@ -49,6 +49,13 @@ int cuot_ctx_destroy(cuot_ctx *ctx);
 /* Pre-size the scratch arena (call before capturing a CUDA graph). */
 int cuot_ctx_reserve(cuot_ctx *ctx, uint64_t bytes);
 uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
+/* Tuning knobs of the single-instance calls made on this context (the
+ * autotuner in cuot_b200/autotune.py sets them from its measurements):
+ *   CUOT_TUNE_PPRF_THREADS  threads per tree CTA, 128 or 256 (default 256)
+ *   CUOT_TUNE_QC_PLANES     planes per NTT pass, 0 = automatic (~64 MiB) */
+#define CUOT_TUNE_PPRF_THREADS 1
+#define CUOT_TUNE_QC_PLANES 2
+int cuot_ctx_set_tuning(cuot_ctx *ctx, int key, int64_t value);
 
 /* ---- AES-128 ECB ---------------------------------------------------------
  * In-place FIPS-197 AES-128 of `nblocks` blocks under `key` (host, 16 bytes).
@@ -240,6 +247,7 @@ typedef struct {
 } cuot_batch_item;
 
 typedef struct {
+  int pprf_threads;        /* threads per tree CTA: 128 or 256 (0: 256) */
   int ctas_per_sm;         /* persistent PPRF/LPN grid: CTAs per SM (0: 3) */
   int lpn_rows_per_task;   /* LPN work-queue granularity, multiple of 4 (0: 65536) */
   int qc_planes_per_pass;  /* planes per NTT pass (0: ~64 MiB of intermediate) */

@@ -325,3 +325,27 @@ def test_sharded_ferret_extend_equals_unsplit(ctx):
     rleaves = oracle.ferret_pprf_recver(mc, choice, ss, h, threads=4)
     assert np.array_equal(np.concatenate(vs), oracle.lpn_primal(seed, kk_s, leaves))
     assert np.array_equal(np.concatenate(ws), oracle.lpn_primal(seed, kk_r, rleaves))
+
+
+def test_pprf_128_threads_per_tree_matches_oracle(ctx):
+    """The tuning knob CUOT_TUNE_PPRF_THREADS = 128 changes the CTA size only."""
+    ctx.set_tuning(ctx.TUNE_PPRF_THREADS, 128)
+    try:
+        for t, h in [(3, 7), (20, 11), (1, 1)]:
+            rng = np.random.default_rng(t + 100 * h)
+            roots, delta = rng_blocks(rng, t), delta_ferret(rng)
+            got = run_ferret_sender(ctx, roots, h, delta)
+            exp = oracle.ferret_pprf_sender(roots, h, delta, threads=8)
+            for g, e in zip(got, exp):
+                assert np.array_equal(g, e)
+            ch = rng.integers(0, 2, t * h).astype(np.uint8)
+            mc = np.where(ch[:, None] == 0, exp[1], exp[2])
+            assert np.array_equal(run_ferret_recver(ctx, mc, ch, exp[3], h),
+                                  oracle.ferret_pprf_recver(mc, ch, exp[3], h, threads=8))
+            r2, d2, b0, b1, ch2 = sot_inputs(rng, t, h)
+            lv, m0, m1, rl, mc2 = run_sot(ctx, r2, h, d2, b0, b1, ch2)
+            el, e0, e1 = oracle.sot_pprf_sender(r2, h, d2, b0, b1, threads=8)
+            assert np.array_equal(lv, el) and np.array_equal(m0, e0)
+            assert np.array_equal(rl, oracle.sot_pprf_recver(e0, e1, mc2, ch2, t, h, threads=8))
+    finally:
+        ctx.set_tuning(ctx.TUNE_PPRF_THREADS, 256)
