@@ -72,14 +72,18 @@ __device__ __forceinline__ unsigned brev(unsigned x, int bits) { return __brev(x
 // w_N^(off * N / 2^(s+1)) for off < 2^s, so a warp's twiddle reads are
 // consecutive.  DIF forward: natural in, bit-reversed out.  DIT inverse:
 // bit-reversed in, natural out (unscaled).  Values stay in [0, 2p).
-__host__ __device__ constexpr int swz(int i) {
-  return i ^ (((i >> 5) & 7) | ((((i >> 5) >> 1) & 3) << 3));
+__host__ __device__ constexpr int swz(int i) { return i + 3 * (i >> 5); }
+// Additive padding: 3 words after every 32.  Within a radix group the
+// element offsets (m << s_lo) occupy bits disjoint from the group base and
+// the sum never carries across a 32-word boundary, so
+// swz(base + (m << s_lo)) = swz(base) + swz(m << s_lo): the element address
+// is the group's base address plus a compile-time immediate (no per-element
+// arithmetic).  Conflict-free or 2-way for every pass shape used here.
+// Row stride: padded length rounded to 4 (mod 32) words, so the column
+// kernels' row-interleaved accesses hit distinct banks.
+__host__ __device__ constexpr int padded_len(int n) {
+  return (swz(n - 1) + 1) + ((4 - (swz(n - 1) + 1)) % 32 + 32) % 32;
 }
-// swz is linear over GF(2) (an XOR of bit fields), and within a radix group
-// the element offsets (m << s_lo) occupy bits disjoint from the group base,
-// so swz(base ^ (m << s_lo)) = swz(base) ^ swz(m << s_lo): one XOR with a
-// compile-time constant per element.
-__host__ __device__ constexpr int padded_len(int n) { return n + 4; }
 
 // Per-plane `a` transforms for one row pass (passed by value).
 constexpr int kAhatTab = 16;
@@ -104,10 +108,14 @@ __device__ __forceinline__ void bf_dif(uint32_t &u, uint32_t &v, uint2 w) {
   v = shoup_mul(u - v + 2 * kP, w);
   u = a;
 }
-__device__ __forceinline__ void bf_dit(uint32_t &u, uint32_t &v, uint2 w) {
+__device__ __forceinline__ uint32_t umin4p(uint32_t a) {
+  return min(a, a - 4 * kP);  // a in [0, 8p) -> [0, 4p)
+}
+// DIT butterfly without reductions: u + t and u - t + 2p, t = v * w in [0, 2p).
+__device__ __forceinline__ void bf_dit_lazy(uint32_t &u, uint32_t &v, uint2 w) {
   const uint32_t t = shoup_mul(v, w);
-  v = umin2p(u - t + 2 * kP);
-  u = umin2p(u + t);
+  v = u - t + 2 * kP;
+  u = u + t;
 }
 
 // One pass of K radix-2 stages [S_LO, S_LO + K) of a 2^LG-point transform on
@@ -121,12 +129,11 @@ __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const ui
     const int row = w >> NGR_LG, g = w & ((1 << NGR_LG) - 1);
     const int glo = g & LOWMASK;
     const int base = glo | ((g >> S_LO) << (S_LO + K));
-    const int sb = swz(base);
-    uint32_t *xr = x + row * ld;
+    uint32_t *xr = x + row * ld + swz(base);
     const uint2 *twg = tw + glo;
     uint32_t v[R];
 #pragma unroll
-    for (int m = 0; m < R; m++) v[m] = xr[sb ^ swz(m << S_LO)];
+    for (int m = 0; m < R; m++) v[m] = xr[swz(m << S_LO)];
     if (DIF) {
 #pragma unroll
       for (int j = K - 1; j >= 0; j--) {
@@ -138,17 +145,27 @@ __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const ui
         }
       }
     } else {
+      // Lazy DIT: skip the per-butterfly reductions; with inputs in [0, 2p)
+      // values grow by at most 2p per stage (u + t, u - t + 2p with t < 2p),
+      // and 8p < 2^32, so three stages run unreduced; a 4-stage pass brings
+      // values back under 4p after its second stage.  Outputs in [0, 2p).
 #pragma unroll
       for (int j = 0; j < K; j++) {
 #pragma unroll
         for (int m = 0; m < R; m++) {
           if (m & (1 << j)) continue;
-          bf_dit(v[m], v[m | (1 << j)], twg[(1 << (S_LO + j)) - 1 + ((m & ((1 << j) - 1)) << S_LO)]);
+          bf_dit_lazy(v[m], v[m | (1 << j)], twg[(1 << (S_LO + j)) - 1 + ((m & ((1 << j) - 1)) << S_LO)]);
+        }
+        if (K == 4 && j == 1) {
+#pragma unroll
+          for (int m = 0; m < R; m++) v[m] = umin4p(v[m]);
         }
       }
+#pragma unroll
+      for (int m = 0; m < R; m++) v[m] = umin2p(umin4p(v[m]));
     }
 #pragma unroll
-    for (int m = 0; m < R; m++) xr[sb ^ swz(m << S_LO)] = v[m];
+    for (int m = 0; m < R; m++) xr[swz(m << S_LO)] = v[m];
   }
   __syncthreads();
 }
