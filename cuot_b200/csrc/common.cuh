@@ -156,6 +156,36 @@ __device__ __forceinline__ void aes_enc2(const TabRef &t, uint32_t (&a)[4], cons
   b[3] = final_col(t, u3, u0, u1, u2, kb[43]);
 }
 
+// Rounds 2..10 of two blocks given their states after round 1 (round key 1
+// included).
+__device__ __forceinline__ void aes_enc2_from_round2(const TabRef &t, uint32_t (&a)[4],
+                                                     uint32_t (&b)[4], const AesKey &K) {
+  const uint32_t *kr = K.rkr, *rk = K.rk;
+  uint32_t s0 = a[0], s1 = a[1], s2 = a[2], s3 = a[3];
+  uint32_t u0 = b[0], u1 = b[1], u2 = b[2], u3 = b[3];
+#pragma unroll
+  for (int r = 2; r < 10; r++) {
+    uint32_t o0 = round_col(t, s0, s1, s2, s3, kr[4 * r + 0]);
+    uint32_t p0 = round_col(t, u0, u1, u2, u3, kr[4 * r + 0]);
+    uint32_t o1 = round_col(t, s1, s2, s3, s0, kr[4 * r + 1]);
+    uint32_t p1 = round_col(t, u1, u2, u3, u0, kr[4 * r + 1]);
+    uint32_t o2 = round_col(t, s2, s3, s0, s1, kr[4 * r + 2]);
+    uint32_t p2 = round_col(t, u2, u3, u0, u1, kr[4 * r + 2]);
+    uint32_t o3 = round_col(t, s3, s0, s1, s2, kr[4 * r + 3]);
+    uint32_t p3 = round_col(t, u3, u0, u1, u2, kr[4 * r + 3]);
+    s0 = o0; s1 = o1; s2 = o2; s3 = o3;
+    u0 = p0; u1 = p1; u2 = p2; u3 = p3;
+  }
+  a[0] = final_col(t, s0, s1, s2, s3, rk[40]);
+  b[0] = final_col(t, u0, u1, u2, u3, rk[40]);
+  a[1] = final_col(t, s1, s2, s3, s0, rk[41]);
+  b[1] = final_col(t, u1, u2, u3, u0, rk[41]);
+  a[2] = final_col(t, s2, s3, s0, s1, rk[42]);
+  b[2] = final_col(t, u2, u3, u0, u1, rk[42]);
+  a[3] = final_col(t, s3, s0, s1, s2, rk[43]);
+  b[3] = final_col(t, u3, u0, u1, u2, rk[43]);
+}
+
 // ---------------------------------------------------------------------------
 // Warp / block XOR reductions of a block value.
 __device__ __forceinline__ Blk warp_xor(Blk v) {

@@ -28,24 +28,33 @@ __device__ __forceinline__ uint32_t lpn_idx(uint32_t w, uint32_t mask, uint32_t 
 }
 
 // Rows 4g..4g+3 for d = D known at compile time.
+// The D plaintexts makeBlock(i, m) = {m, 0, i_lo, i_hi} (m < D < 256) differ
+// only in byte 0, so after AddRoundKey they differ only in byte 0 of column
+// 0.  Round 1 reads that byte only for output column 0 (ShiftRows keeps row
+// 0 in place); output columns 1..3 and three of column 0's four lookups are
+// the same for all D blocks and are computed once per group.
 template <int D>
 __device__ __forceinline__ void lpn_group4(const LpnArgs &a, const TabRef &T, int64_t g) {
+  static_assert(D <= 256, "the round-1 sharing needs m < 256");
   const int64_t i = 4 * g;
   const uint32_t k = uint32_t(a.k), mask = a.mask;
+  const AesKey &K = a.key;
   Blk acc[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) acc[m] = Blk{{0, 0, 0, 0}};
   // makeBlock(i, m): low qword m, high qword i.
   const uint32_t ilo = uint32_t(uint64_t(i)), ihi = uint32_t(uint64_t(i) >> 32);
+  const uint32_t s1 = K.rk[1], s2 = ilo ^ K.rk[2], s3 = ihi ^ K.rk[3];
+  const uint32_t s0hi = K.rk[0];  // bytes 1..3 of column 0 for every m
+  const uint32_t c1 = round_col(T, s1, s2, s3, s0hi, K.rkr[5]);
+  const uint32_t c2 = round_col(T, s2, s3, s0hi, s1, K.rkr[6]);
+  const uint32_t c3 = round_col(T, s3, s0hi, s1, s2, K.rkr[7]);
+  const uint32_t c0x = t2<2>(T, s2) ^ rotl8(t0<1>(T, s1) ^ t2<3>(T, s3) ^ K.rkr[4]);
 #pragma unroll
   for (int m = 0; m < D; m += 2) {
-    uint32_t x[4] = {uint32_t(m), 0u, ilo, ihi};
-    uint32_t y[4] = {uint32_t(m + 1), 0u, ilo, ihi};
-    if (m + 1 < D) {
-      aes_enc2(T, x, a.key, y, a.key);
-    } else {
-      aes_enc(T, x, a.key);
-    }
+    uint32_t x[4] = {t0<0>(T, uint32_t(m) ^ K.rk[0]) ^ c0x, c1, c2, c3};
+    uint32_t y[4] = {t0<0>(T, uint32_t(m + 1) ^ K.rk[0]) ^ c0x, c1, c2, c3};
+    aes_enc2_from_round2(T, x, y, K);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int word = 4 * m + q;  // compile-time after unrolling

@@ -120,8 +120,11 @@ __device__ __forceinline__ void bf_dit_lazy(uint32_t &u, uint32_t &v, uint2 w) {
 
 // One pass of K radix-2 stages [S_LO, S_LO + K) of a 2^LG-point transform on
 // `rows` rows, everything but the row count known at compile time.
+// ah (optional, the last DIF pass only): after its stages, element `pos` of
+// row `row` is multiplied by ah[row * 2^LG + pos] (the pointwise product).
 template <int LG, int K, int S_LO, bool DIF>
-__device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const uint2 *tw) {
+__device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const uint2 *tw,
+                                         const uint2 *__restrict__ ah = nullptr) {
   constexpr int R = 1 << K;
   constexpr int NGR_LG = LG - K;
   constexpr int LOWMASK = (1 << S_LO) - 1;
@@ -144,11 +147,21 @@ __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const ui
           bf_dif(v[m], v[m | (1 << j)], twg[(1 << (S_LO + j)) - 1 + ((m & ((1 << j) - 1)) << S_LO)]);
         }
       }
+      if (S_LO == 0 && ah != nullptr) {
+        const uint4 *a4 = reinterpret_cast<const uint4 *>(ah + (row << LG) + base);
+#pragma unroll
+        for (int m = 0; m < R; m += 2) {
+          const uint4 q = __ldg(a4 + m / 2);
+          v[m] = shoup_mul(v[m], make_uint2(q.x, q.y));
+          v[m + 1] = shoup_mul(v[m + 1], make_uint2(q.z, q.w));
+        }
+      }
     } else {
       // Lazy DIT: skip the per-butterfly reductions; with inputs in [0, 2p)
       // values grow by at most 2p per stage (u + t, u - t + 2p with t < 2p),
-      // and 8p < 2^32, so three stages run unreduced; a 4-stage pass brings
-      // values back under 4p after its second stage.  Outputs in [0, 2p).
+      // and 8p < 2^32, so three stages run unreduced; 4- and 5-stage passes
+      // bring values back under 4p after their second (and fourth) stage.
+      // Outputs in [0, 2p).
 #pragma unroll
       for (int j = 0; j < K; j++) {
 #pragma unroll
@@ -156,7 +169,7 @@ __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const ui
           if (m & (1 << j)) continue;
           bf_dit_lazy(v[m], v[m | (1 << j)], twg[(1 << (S_LO + j)) - 1 + ((m & ((1 << j) - 1)) << S_LO)]);
         }
-        if (K == 4 && j == 1) {
+        if ((K == 4 && j == 1) || (K == 5 && (j == 1 || j == 3))) {
 #pragma unroll
           for (int m = 0; m < R; m++) v[m] = umin4p(v[m]);
         }
@@ -173,13 +186,14 @@ __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const ui
 // Full 2^LG-point transform as ceil(LG/4) passes of near-equal size (DIF
 // from the top stage down, DIT from stage 0 up).  Caller has synced.
 template <int LG, bool DIF, int PIDX = 0, int DONE = 0>
-__device__ __forceinline__ void ntt_smem(uint32_t *x, int rows, int ld, const uint2 *tw) {
+__device__ __forceinline__ void ntt_smem(uint32_t *x, int rows, int ld, const uint2 *tw,
+                                         const uint2 *ah = nullptr) {
   constexpr int P = (LG + 3) / 4;
   if constexpr (PIDX < P) {
     constexpr int K = LG / P + (PIDX < LG % P ? 1 : 0);
     constexpr int S_LO = DIF ? (LG - DONE - K) : DONE;
-    ntt_pass<LG, K, S_LO, DIF>(x, rows, ld, tw);
-    ntt_smem<LG, DIF, PIDX + 1, DONE + K>(x, rows, ld, tw);
+    ntt_pass<LG, K, S_LO, DIF>(x, rows, ld, tw, DIF && S_LO == 0 ? ah : nullptr);
+    ntt_smem<LG, DIF, PIDX + 1, DONE + K>(x, rows, ld, tw, ah);
   }
 }
 
@@ -210,6 +224,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_fwd(
   }
   __syncthreads();
   ntt_smem<E1, true>(xs, kCW, ld, tws);
+  // x w_n^(j2 * rev(r)) on the way out; fsf is [r][j2], read coalesced
   uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
 #pragma unroll 4
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
@@ -238,23 +253,30 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_row(
   const uint64_t plane = blockIdx.y;
   const int r0 = blockIdx.x * rows_per_cta;
   uint32_t *Yp = Y + (plane * N1 + r0) * uint64_t(N2);
-  const int cnt = rows_per_cta * N2;
-#pragma unroll 4
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) xs[(i >> E2) * ld + swz(i & (N2 - 1))] = Yp[i];
+  const int cnt4 = rows_per_cta * N2 / 4;
+  // 4 consecutive elements per thread: they share a 32-word chunk, so one
+  // padded base address serves all four
+#pragma unroll 2
+  for (int i4 = threadIdx.x; i4 < cnt4; i4 += blockDim.x) {
+    const int i = 4 * i4;
+    const uint4 q = reinterpret_cast<const uint4 *>(Yp)[i4];
+    uint32_t *d = xs + (i >> E2) * ld + swz(i & (N2 - 1));
+    d[0] = q.x; d[1] = q.y; d[2] = q.z; d[3] = q.w;
+  }
   __syncthreads();
-  ntt_smem<E2, true>(xs, rows_per_cta, ld, twf);
   if (mode == 0) {
     const uint2 *ah = ahat_tab.p[(ahat_tab.first + blockIdx.y) / ahat_tab.per] + uint64_t(r0) * N2;
-#pragma unroll 4
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-      uint32_t *p = &xs[(i >> E2) * ld + swz(i & (N2 - 1))];
-      *p = shoup_mul(*p, __ldg(&ah[i]));
-    }
-    __syncthreads();
+    ntt_smem<E2, true>(xs, rows_per_cta, ld, twf, ah);  // forward, then x ahat / n in registers
     ntt_smem<E2, false>(xs, rows_per_cta, ld, twi);
+  } else {
+    ntt_smem<E2, true>(xs, rows_per_cta, ld, twf);
   }
-#pragma unroll 4
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) Yp[i] = xs[(i >> E2) * ld + swz(i & (N2 - 1))];
+#pragma unroll 2
+  for (int i4 = threadIdx.x; i4 < cnt4; i4 += blockDim.x) {
+    const int i = 4 * i4;
+    const uint32_t *d = xs + (i >> E2) * ld + swz(i & (N2 - 1));
+    reinterpret_cast<uint4 *>(Yp)[i4] = make_uint4(d[0], d[1], d[2], d[3]);
+  }
 }
 
 // Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits.
@@ -274,7 +296,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_inv(
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
-    xs[c * ld + swz(r)] = shoup_mul(Yp[o], __ldg(&fsi[o]));
+    xs[c * ld + swz(r)] = shoup_mul(Yp[o], __ldg(&fsi[o]));  // x w_n^-(j2 * rev(r))
   }
   __syncthreads();
   ntt_smem<E1, false>(xs, kCW, ld, tws);
@@ -300,6 +322,7 @@ __global__ void qc_gen_twiddles(int lg, uint32_t root, uint2 *tw) {
     tw[i] = shoup_pair(powmod(root, uint64_t(off) * uint64_t(N >> (s + 1))));
   }
 }
+// Four-step twiddles, [r][j2]: entry r * N2 + j2 = wn^(j2 * rev(r)).
 __global__ void qc_gen_fourstep(int e1, int e2, uint32_t wn, uint2 *fs) {
   const uint64_t n = 1ull << (e1 + e2);
   const uint64_t N2 = 1ull << e2;
