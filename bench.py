@@ -11,8 +11,11 @@ Workloads (--workload):
               time through the plain entry points (plain.value).
   sot_n20     plain SOT, n = 2^20: 256 GGM trees of depth 12 (both roles),
               exact quasi-cyclic encode of the 128 bit planes of the 2n-bit
-              (zero-padded) noise vector, transposes both ways, plus the
-              receiver's choice-bit encode.            [default]
+              noise vector, transposes both ways, plus the
+              receiver's choice-bit encode.
+  sot_n20_r2  SOT rate-1/2 form with n = 2^20 outputs: 512 trees of depth
+              12 give 2n noise blocks e = (e0, e1) per role, encoded as
+              e0 ^ a * e1 (the flagged second SOT configuration).
   ferret_b13  plain Ferret at full size (ferret_b13): n = 10,485,760,
               t = 1280 trees of depth 13, k = 452,000, d = 10 (both roles:
               MPCOT + primal LPN).
@@ -45,6 +48,7 @@ import numpy as np
 WORKLOADS = {
     "mixed64": dict(kind="batch", count=64, lo=16, hi=22),
     "sot_n20": dict(kind="sot", t=256, h=12),
+    "sot_n20_r2": dict(kind="sot", t=512, h=12, r2=True),
     "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
     "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
 }
@@ -52,6 +56,8 @@ CONFIG_TEXT = {
     "mixed64": "batched mix: 64 instances (32 SOT, 32 Ferret-style), log2 n uniform in [16,22], depth 10-14, "
                "both roles, one CUDA-graph program vs the plain one-instance-at-a-time path",
     "sot_n20": "plain SOT n=2^20: 256 GGM trees depth 12, exact QC encode of 128 planes, transposes (both roles)",
+    "sot_n20_r2": "plain SOT rate-1/2, n=2^20 outputs: 512 GGM trees depth 12 (2n noise blocks), "
+                  "out = e0 ^ a*e1 exact on 128 planes, transposes (both roles)",
     "ferret_b13": "plain Ferret ferret_b13: n=10485760, t=1280, h=13, k=452000, d=10 (both roles)",
     "ferret_c1": "plain Ferret small: n=65536, t=64, h=10, k=8192, d=10 (both roles)",
 }
@@ -136,7 +142,9 @@ class Instance:
         self.torch, self.cb = torch, cuot_b200
         s = self.spec
         self.t, self.h = s["t"], s["h"]
-        self.n = self.t << self.h
+        self.r2 = bool(s.get("r2"))
+        self.nleaves = self.t << self.h
+        self.n = self.nleaves // 2 if self.r2 else self.nleaves  # COTs per role
         rng = np.random.default_rng(seed)
         blk = lambda m: rng.integers(0, 256, (m, 16), dtype=np.uint8)
         dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
@@ -151,7 +159,7 @@ class Instance:
         self.rctx = cuot_b200.Context(torch.cuda.current_device())
         self.d_roots = dev(self.roots)
         self.d_choice = dev(self.choice)
-        self.leaves_s, self.leaves_r = emp(n), emp(n)
+        self.leaves_s, self.leaves_r = emp(self.nleaves), emp(self.nleaves)
         if s["kind"] == "ferret":
             k = s["k"]
             self.k, self.d = k, s["d"]
@@ -201,9 +209,14 @@ class Instance:
                                       self.m0, self.m1)
             self.rctx.sot_pprf_recver(self.m0, self.m1, self.d_mc, self.d_choice, t, h, self.leaves_r)
             mark("pprf1")
-            self.plan_s.dual_lpn(self.leaves_s)
-            self.plan_r.dual_lpn(self.leaves_r)
-            self.rctx.qc_encode_sparse(self.a, self.d_pos, n, self.cbits)
+            if self.r2:
+                self.plan_s.dual_lpn_r2(self.leaves_s, self.leaves_s[:n])
+                self.plan_r.dual_lpn_r2(self.leaves_r, self.leaves_r[:n])
+                self.rctx.qc_encode_sparse_r2(self.a, self.d_pos, n, self.cbits)
+            else:
+                self.plan_s.dual_lpn(self.leaves_s)
+                self.plan_r.dual_lpn(self.leaves_r)
+                self.rctx.qc_encode_sparse(self.a, self.d_pos, n, self.cbits)
             mark("lpn1")
 
     def launches_per_step(self) -> int:
@@ -211,6 +224,36 @@ class Instance:
         self.step()
         self.torch.cuda.synchronize()
         return self.cb.launch_count() - before
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
+# stage's kernels per step, summed from one ncu launch capture of the same
+# bench command (ncu starts every kernel with cold caches, so the NTT
+# intermediate that steady state keeps in L2 is counted).
+NCU_TRAFFIC_PER_STEP = {
+    "ferret_b13:lpn": 570.44e6,
+    "sot_n20:dual_lpn": 2892.64e6,
+}
+
+AES_PEAK_MODEL = ("T-table AES: 160 shared-memory lookups per block (10 rounds x 16), one conflict-free "
+                  "32-lane lookup wavefront per clock per SM; peak = SMs x 32 x median SM clock / 160")
+
+
+def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
+    """AES blocks per second of the AES-bound stages against the T-table
+    lookup roofline (the integer-pipe figure that bounds the PPRF and the
+    LPN index generation)."""
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    peak = props.multi_processor_count * 32 * mhz * 1e6 / 160
+    t, h = inst.t, inst.h
+    counts = {"pprf": 4 * t * ((1 << h) - 1)}  # 2 AES per internal node, both roles
+    if inst.spec["kind"] == "ferret":
+        counts["lpn"] = 2 * inst.n * inst.d // 4  # d index blocks per 4 rows, both roles
+    res = {"peak_aes_per_s": peak, "model": AES_PEAK_MODEL}
+    for k, cnt in counts.items():
+        a = cnt / (stages[k][0] / 1e3)
+        res[k] = {"aes_per_step": cnt, "aes_per_s": a, "frac": a / peak}
+    return res
 
 
 def e2e_step(inst: Instance, host, stream):
@@ -248,13 +291,19 @@ def e2e_step(inst: Instance, host, stream):
                                       inst.m0, inst.m1, stream=stream)
             inst.rctx.sot_pprf_recver(inst.m0, inst.m1, inst.d_mc, inst.d_choice, inst.t, inst.h, inst.leaves_r,
                                       stream=stream)
-            inst.plan_s.dual_lpn(inst.leaves_s, stream=stream)
-            inst.plan_r.dual_lpn(inst.leaves_r, stream=stream)
-            inst.rctx.qc_encode_sparse(inst.a, inst.d_pos, inst.n, inst.cbits, stream=stream)
+            if inst.r2:
+                n = inst.n
+                inst.plan_s.dual_lpn_r2(inst.leaves_s, inst.leaves_s[:n], stream=stream)
+                inst.plan_r.dual_lpn_r2(inst.leaves_r, inst.leaves_r[:n], stream=stream)
+                inst.rctx.qc_encode_sparse_r2(inst.a, inst.d_pos, n, inst.cbits, stream=stream)
+            else:
+                inst.plan_s.dual_lpn(inst.leaves_s, stream=stream)
+                inst.plan_r.dual_lpn(inst.leaves_r, stream=stream)
+                inst.rctx.qc_encode_sparse(inst.a, inst.d_pos, inst.n, inst.cbits, stream=stream)
             host["c"].copy_(inst.cbits, non_blocking=True)
             d2h += host["c"].numel() * 8
-        host["v"].copy_(inst.leaves_s, non_blocking=True)
-        host["w"].copy_(inst.leaves_r, non_blocking=True)
+        host["v"].copy_(inst.leaves_s[:inst.n], non_blocking=True)
+        host["w"].copy_(inst.leaves_r[:inst.n], non_blocking=True)
         d2h += host["v"].numel() + host["w"].numel()
     return h2d, d2h
 
@@ -306,7 +355,9 @@ def cpu_sample(name: str, threads: int, budget_s: float = 10.0):
                 break
         return reps * n / el, f"{t} of {t_full} trees (n={n}), both roles, MPCOT + LPN (k={spec['k']}), {reps} reps"
     # SOT: PPRF both roles on all trees; QC encode on a subset of planes, scaled
-    n = t_full << h
+    r2 = bool(spec.get("r2"))
+    nl = t_full << h
+    n = nl // 2 if r2 else nl
     roots, delta = blk(t_full), blk(1)[0]
     b0, b1 = blk(h * t_full), blk(h * t_full)
     ch = rng.integers(0, 2, h * t_full).astype(np.uint8)
@@ -318,8 +369,10 @@ def cpu_sample(name: str, threads: int, budget_s: float = 10.0):
     rl = oracle.sot_pprf_recver(m0, m1, mc, ch, t_full, h, threads=threads)
     t_pprf = time.perf_counter() - t0
     t0 = time.perf_counter()
-    pl = oracle.bit_transpose(lv, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
-    oracle.qc_encode(a, pl[:nplanes].copy(), n, threads=threads)
+    pl = oracle.bit_transpose(lv, nl, 16, 0, 128).view(np.uint64).reshape(128, nl // 64)
+    enc = oracle.qc_encode(a, pl[:nplanes, nl // 64 - n // 64:].copy(), n, threads=threads)
+    if r2:
+        enc ^= pl[:nplanes, :n // 64]
     t_qc = (time.perf_counter() - t0) * (128 / nplanes) * 2  # both roles
     el = t_pprf + t_qc
     return n / el, f"both roles PPRF on all {t_full} trees; QC encode timed on {nplanes} of 128 planes (one role) and scaled x{128 / nplanes * 2:g}"
@@ -626,17 +679,15 @@ def run_ours(args):
         pprf_bytes = 2 * (16 * n + 32 * inst.t * inst.h)
         stages = {"pprf": (pprf_ms, pprf_bytes), "lpn": (lpn_ms, lpn_bytes)}
     else:
-        # dual LPN: two transposes (32n each) + encode in/out (32n) per role
-        stages = {"pprf": (pprf_ms, 2 * (16 * n + 32 * inst.t * (inst.h + 1))),
-                  "dual_lpn": (lpn_ms, 2 * (3 * 32 * n))}
+        # dual LPN per role: two transposes (32 B per block each way) + encode
+        # planes in/out (32n); rate-1/2: 2n blocks in (64n), e0 XOR (48n), n out (32n)
+        dual = 2 * (144 * n if inst.r2 else 3 * 32 * n)
+        stages = {"pprf": (pprf_ms, 2 * (16 * inst.nleaves + 32 * inst.t * (inst.h + 1))),
+                  "dual_lpn": (lpn_ms, dual)}
     dom = max(stages, key=lambda s: stages[s][0])
     dms, dbytes = stages[dom]
     achieved = dbytes / (dms / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get(f"{args.workload}:{dom}")
+    traffic = NCU_TRAFFIC_PER_STEP.get(f"{args.workload}:{dom}")
     out = {
         "metric": metric_name(args.workload),
         "value": value, "unit": "COTs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -649,12 +700,15 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                     "algorithmic_bytes_per_step": dbytes},
+                     "algorithmic_bytes_per_step": dbytes,
+                     "basis": "stage totals per step (both roles): algorithmic bytes / stage time; "
+                              "traffic = ncu DRAM bytes of the stage's kernels per step"},
         "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }
+    out["aes_roofline"] = aes_roofline(inst, stages, clocks, torch.cuda.get_device_properties(local))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample(args.workload, threads)

@@ -194,6 +194,15 @@ class Context:
         _check(self.lib.cuot_sot_dual_lpn(self.h, _ptr(a), _ptr(io), C.c_uint64(n), _stream(stream)),
                "cuot_sot_dual_lpn")
 
+    def sot_dual_lpn_r2(self, a, inp, n: int, out, stream=None):
+        """Rate-1/2 form: out[:n] = inp[:n] ^ (a * inp[n:2n]) per bit plane."""
+        _check(self.lib.cuot_sot_dual_lpn_r2(self.h, _ptr(a), _ptr(inp), C.c_uint64(n), _ptr(out),
+                                             _stream(stream)), "cuot_sot_dual_lpn_r2")
+
+    def qc_encode_sparse_r2(self, a, pos, n: int, out, stream=None):
+        _check(self.lib.cuot_qc_encode_sparse_r2(self.h, _ptr(a), _ptr(pos), C.c_int(pos.numel()), C.c_uint64(n),
+                                                 _ptr(out), _stream(stream)), "cuot_qc_encode_sparse_r2")
+
     def qc_plan(self, a, n: int, stream=None) -> "QcPlan":
         return QcPlan(self, a, n, stream)
 
@@ -217,6 +226,10 @@ class QcPlan:
 
     def dual_lpn(self, io, stream=None):
         _check(self.ctx.lib.cuot_qc_plan_dual_lpn(self.h, _ptr(io), _stream(stream)), "cuot_qc_plan_dual_lpn")
+
+    def dual_lpn_r2(self, inp, out, stream=None):
+        _check(self.ctx.lib.cuot_qc_plan_dual_lpn_r2(self.h, _ptr(inp), _ptr(out), _stream(stream)),
+               "cuot_qc_plan_dual_lpn_r2")
 
     def close(self):
         if getattr(self, "h", None):

@@ -279,11 +279,12 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_row(
   }
 }
 
-// Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits.
+// Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits, written
+// (accumulate == 0) or XORed into (accumulate == 1; the rate-1/2 form).
 template <int E1>
 __global__ void __launch_bounds__(kQcThreads, 4) qc_col_inv(
     const uint32_t *__restrict__ Y, int e2, const uint2 *__restrict__ fsi,
-    const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes) {
+    const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes, int accumulate) {
   extern __shared__ uint32_t xs[];
   constexpr int N1 = 1 << E1, ld = padded_len(N1);
   const int N2 = 1 << e2;
@@ -309,7 +310,8 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_inv(
       v = v >= kP ? v - kP : v;  // exact coefficient in [0, n]
       byte |= (v & 1u) << c;
     }
-    ob[(uint64_t(j1) * N2 + c0) >> 3] = uint8_t(byte);
+    uint8_t *o = ob + ((uint64_t(j1) * N2 + c0) >> 3);
+    *o = uint8_t(accumulate ? (*o ^ byte) : byte);
   }
 }
 
@@ -361,14 +363,23 @@ __global__ void prg_make_counters(Blk *b, uint64_t nb, uint64_t off) {
 }
 
 // Sparse encode: out = XOR_i rot(a, pos_i), one thread per output word.
+// r2 (rate-1/2 noise of 2n positions): positions p < n contribute x^p
+// itself, positions p in [n, 2n) contribute rot(a, p - n).
 __global__ void qc_sparse(const uint64_t *__restrict__ a, const uint64_t *__restrict__ pos,
-                          int weight, uint64_t n, uint64_t *__restrict__ out) {
+                          int weight, uint64_t n, uint64_t *__restrict__ out, int r2) {
   const uint64_t nw = n / 64;
   for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nw;
        w += uint64_t(gridDim.x) * blockDim.x) {
     uint64_t acc = 0;
     for (int i = 0; i < weight; i++) {
-      const uint64_t p = __ldg(&pos[i]);
+      uint64_t p = __ldg(&pos[i]);
+      if (r2) {
+        if (p < n) {
+          if ((p >> 6) == w) acc ^= 1ull << (p & 63);
+          continue;
+        }
+        p -= n;
+      }
       if (p >= n) continue;
       const uint64_t ws = p >> 6, bs = p & 63;
       // bit (64w + b) of rot(a, p) = bit (64w + b - p) mod n of a
@@ -514,9 +525,9 @@ static void launch_row(const QcTables *t, dim3 grid, cudaStream_t st, uint32_t *
   }
 }
 static void launch_col_inv(const QcTables *t, dim3 grid, cudaStream_t st, const uint32_t *Y, uint8_t *out,
-                           uint64_t plane_bytes) {
+                           uint64_t plane_bytes, int accumulate = 0) {
   switch (t->e1) {
-#define L3(E) case E: qc_col_inv<E><<<grid, kQcThreads, col_smem(t), st>>>(Y, t->e2, t->fsi, t->tw1i, out, plane_bytes); break;
+#define L3(E) case E: qc_col_inv<E><<<grid, kQcThreads, col_smem(t), st>>>(Y, t->e2, t->fsi, t->tw1i, out, plane_bytes, accumulate); break;
     CUOT_E1_CASES(L3)
 #undef L3
   }
@@ -534,19 +545,43 @@ static int build_ahat(const QcTables *t, const uint64_t *a_d, uint32_t *Y, uint2
   return launch_status(3);
 }
 
-// Encodes `nplanes` planes (n bits each, consecutive) in place, in batches.
-static int encode_planes(const QcTables *t, const uint2 *ahat, uint64_t *planes, int nplanes,
-                         uint32_t *Y, int batch, cudaStream_t st) {
+int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
+                     uint64_t col_hi, void *out, cudaStream_t st);
+
+// Encodes `nplanes` planes of n bits in batches: plane p is read from
+// in + p * stride (64-bit words) and its product written to (accumulate:
+// XORed into) out + p * stride.  in == out encodes in place.
+static int encode_planes_strided(const QcTables *t, const uint2 *ahat, const uint64_t *in,
+                                 uint64_t *out, uint64_t stride, int accumulate, int nplanes,
+                                 uint32_t *Y, int batch, cudaStream_t st) {
   const int N1 = 1 << t->e1, N2 = 1 << t->e2;
-  const uint64_t n = 1ull << t->e;
   for (int p0 = 0; p0 < nplanes; p0 += batch) {
     const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
-    uint64_t *pl = planes + uint64_t(p0) * (n / 64);
-    launch_col_fwd(t, dim3(N2 / kCW, nb), st, reinterpret_cast<const uint32_t *>(pl), n / 32, Y);
+    launch_col_fwd(t, dim3(N2 / kCW, nb), st, reinterpret_cast<const uint32_t *>(in + uint64_t(p0) * stride),
+                   stride * 2, Y);
     launch_row(t, dim3(N1 / row_rows(t), nb), st, Y, single_ahat(ahat), 0);
-    launch_col_inv(t, dim3(N2 / kCW, nb), st, Y, reinterpret_cast<uint8_t *>(pl), n / 8);
+    launch_col_inv(t, dim3(N2 / kCW, nb), st, Y, reinterpret_cast<uint8_t *>(out + uint64_t(p0) * stride),
+                   stride * 8, accumulate);
   }
   return launch_status(3 * ((nplanes + batch - 1) / batch));
+}
+
+// Encodes `nplanes` planes (n bits each, consecutive) in place.
+static int encode_planes(const QcTables *t, const uint2 *ahat, uint64_t *planes, int nplanes,
+                         uint32_t *Y, int batch, cudaStream_t st) {
+  const uint64_t n = 1ull << t->e;
+  return encode_planes_strided(t, ahat, planes, planes, n / 64, 0, nplanes, Y, batch, st);
+}
+
+// Rate-1/2 dual LPN: out[i] = in[i] ^ (a * in[n..2n))[i] blockwise, i < n.
+// planes: 128 planes of 2n bits (stride n/32 words); Y: batch planes.
+static int dual_lpn_r2(const QcTables *t, const uint2 *ahat, const cuot_block *in_d, cuot_block *out_d,
+                       uint8_t *planes, uint32_t *Y, int batch, cudaStream_t st) {
+  const uint64_t n = 1ull << t->e;
+  uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
+  CUOT_TRY(transpose_launch(in_d, 2 * n, 16, 0, 128, planes, st));
+  CUOT_TRY(encode_planes_strided(t, ahat, pl + n / 64, pl, n / 32, 1, 128, Y, batch, st));
+  return transpose_launch(planes, 128, n / 4, 0, n, out_d, st);
 }
 
 static int check_n(uint64_t n, int *e) {
@@ -564,9 +599,6 @@ static int default_batch(uint64_t n, int nplanes) {
   if (b > uint64_t(nplanes)) b = nplanes;
   return int(b);
 }
-
-int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
-                     uint64_t col_hi, void *out, cudaStream_t st);
 
 // ---- helpers for the batched engine (batch.cu) ----------------------------
 int qc_prepare(cuot_ctx *ctx, int e) {
@@ -717,6 +749,21 @@ int cuot_qc_plan_dual_lpn(cuot_qc_plan *pl, cuot_block *io_d, void *stream) {
   return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
 }
 
+int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *pl, const cuot_block *in_d, cuot_block *out_d, void *stream) {
+  if (!pl || !in_d || !out_d) return fail(CUOT_EINVAL, "bad argument");
+  cuot_ctx *ctx = pl->ctx;
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, pl->e, &t));
+  const uint64_t n = pl->n;
+  const int batch = pl->batch < 128 ? pl->batch : 128;
+  void *scr;
+  CUOT_TRY(scratch(ctx, n * 32 + uint64_t(batch) * n * 4, &scr));
+  uint8_t *planes = static_cast<uint8_t *>(scr);
+  return dual_lpn_r2(t, pl->ahat, in_d, out_d, planes, reinterpret_cast<uint32_t *>(planes + n * 32), batch,
+                     static_cast<cudaStream_t>(stream));
+}
+
 int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, uint64_t n,
                    int nplanes, void *stream) {
   if (!ctx || !a_d || !planes_io_d || nplanes < 1) return fail(CUOT_EINVAL, "bad argument");
@@ -760,13 +807,44 @@ int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d, uint
   return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
 }
 
+int cuot_sot_dual_lpn_r2(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *in_d, uint64_t n,
+                         cuot_block *out_d, void *stream) {
+  if (!ctx || !a_d || !in_d || !out_d) return fail(CUOT_EINVAL, "bad argument");
+  int e;
+  CUOT_TRY(check_n(n, &e));
+  DeviceGuard g(ctx);
+  QcTables *t;
+  CUOT_TRY(get_tables(ctx, e, &t));
+  CUOT_TRY(set_attrs(t));
+  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
+  if (batch > 128) batch = 128;
+  void *scr;
+  CUOT_TRY(scratch(ctx, n * 8 + n * 32 + uint64_t(batch) * n * 4, &scr));
+  uint2 *ahat = static_cast<uint2 *>(scr);
+  uint8_t *planes = static_cast<uint8_t *>(scr) + n * 8;
+  uint32_t *Y = reinterpret_cast<uint32_t *>(planes + n * 32);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUOT_TRY(build_ahat(t, a_d, Y, ahat, st));
+  return dual_lpn_r2(t, ahat, in_d, out_d, planes, Y, batch, st);
+}
+
 int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *pos_d, int weight,
                           uint64_t n, uint64_t *out_d, void *stream) {
   if (!ctx || !a_d || !out_d || (weight > 0 && !pos_d) || weight < 0)
     return fail(CUOT_EINVAL, "bad argument");
   if (n == 0 || n % 64) return fail(CUOT_EINVAL, "n must be a positive multiple of 64");
   DeviceGuard g(ctx);
-  qc_sparse<<<1024, 256, 0, static_cast<cudaStream_t>(stream)>>>(a_d, pos_d, weight, n, out_d);
+  qc_sparse<<<1024, 256, 0, static_cast<cudaStream_t>(stream)>>>(a_d, pos_d, weight, n, out_d, 0);
+  return launch_status();
+}
+
+int cuot_qc_encode_sparse_r2(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *pos_d, int weight,
+                             uint64_t n, uint64_t *out_d, void *stream) {
+  if (!ctx || !a_d || !out_d || (weight > 0 && !pos_d) || weight < 0)
+    return fail(CUOT_EINVAL, "bad argument");
+  if (n == 0 || n % 64) return fail(CUOT_EINVAL, "n must be a positive multiple of 64");
+  DeviceGuard g(ctx);
+  qc_sparse<<<1024, 256, 0, static_cast<cudaStream_t>(stream)>>>(a_d, pos_d, weight, n, out_d, 1);
   return launch_status();
 }
 

@@ -1,4 +1,7 @@
-"""Splitting one Ferret extension over the GPUs of a node.
+"""Splitting one OT extension over the GPUs of a node.
+
+Ferret
+------
 
 One process per GPU (torch.distributed).  Trees are split as FerretCOT's
 gpu_task_division (ferret_cot.hpp:55-63: t / G trees each, the first t % G
@@ -10,6 +13,19 @@ LPN seed and of kk (k blocks, replicated on every GPU as the reference copies
 kk to every GPU, dev_layer.cu:174); there is no data-path exchange.
 The per-level sums and secret sums of each rank go to the host, as in the
 reference (dev_layer.cu:40-41,50).
+
+SOT
+---
+The GGM trees split the same way, but the quasi-cyclic encode works on whole
+bit planes (n bits each), so the one real exchange of the path sits between
+the two: every rank transposes its own rows into 128 partial planes, one
+all-to-all moves the planes to their owners (rank g owns planes
+[128g/G, 128(g+1)/G)), each owner encodes its planes over all n bits, and the
+reverse all-to-all returns every rank the encoded bits of its own rows.  Each
+rank sends (G-1)/G of its 16 n/G bytes each way.  The reference avoids the
+exchange by re-expanding every tree on every GPU (silent/sender.cu:113-115).
+The exchange functions are plain torch.distributed collectives on tensors
+of the process group's device (NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
@@ -67,3 +83,89 @@ def ferret_extend_rank(ctx, plan: ShardPlan, rank: int, roots, delta, choice, se
     ctx.lpn_primal_range(seed, kk_s, v, lo, hi, plan.n, stream=stream)
     ctx.lpn_primal_range(seed, kk_r, w, lo, hi, plan.n, stream=stream)
     return v, w
+
+
+# ---------------------------------------------------------------------------
+# SOT: plane ownership
+
+
+def plane_range(world: int, rank: int) -> tuple[int, int]:
+    """[lo, hi) of the 128 bit planes owned by `rank`."""
+    return 128 * rank // world, 128 * (rank + 1) // world
+
+
+def _check_rows(plan: ShardPlan):
+    for r in range(plan.world):
+        lo, hi = plan.rows(r)
+        if lo % 64 or hi % 64:
+            raise ValueError("SOT sharding needs every rank's row range on a 64-row boundary (depth >= 6)")
+
+
+def planes_to_owners(local, plan: ShardPlan, rank: int):
+    """local: uint8 (128, rows_r / 8), the 128 bit planes of this rank's rows
+    [plan.rows(rank)).  Returns uint8 (P, n / 8): the P planes this rank owns,
+    over all n rows, assembled from every rank's share (one all-to-all)."""
+    import torch
+    import torch.distributed as dist
+    _check_rows(plan)
+    world, n = plan.world, plan.n
+    lo_r, hi_r = plan.rows(rank)
+    nb = (hi_r - lo_r) // 8
+    if tuple(local.shape) != (128, nb):
+        raise ValueError(f"expected planes of shape (128, {nb}), got {tuple(local.shape)}")
+    p_lo, p_hi = plane_range(world, rank)
+    P = p_hi - p_lo
+    ins = [(plane_range(world, j)[1] - plane_range(world, j)[0]) * nb for j in range(world)]
+    outs = [P * (plan.rows(i)[1] - plan.rows(i)[0]) // 8 for i in range(world)]
+    recv = torch.empty(sum(outs), dtype=torch.uint8, device=local.device)
+    dist.all_to_all_single(recv, local.contiguous().view(-1), outs, ins)
+    mine = torch.empty((P, n // 8), dtype=torch.uint8, device=local.device)
+    off = 0
+    for i in range(world):
+        lo, hi = plan.rows(i)
+        mine[:, lo // 8:hi // 8] = recv[off:off + outs[i]].view(P, (hi - lo) // 8)
+        off += outs[i]
+    return mine
+
+
+def owners_to_rows(mine, plan: ShardPlan, rank: int):
+    """Inverse of planes_to_owners: mine is uint8 (P, n / 8), this rank's
+    (encoded) planes; returns uint8 (128, rows_r / 8), all planes of this
+    rank's rows (the reverse all-to-all)."""
+    import torch
+    import torch.distributed as dist
+    world = plan.world
+    p_lo, p_hi = plane_range(world, rank)
+    P = p_hi - p_lo
+    lo_r, hi_r = plan.rows(rank)
+    nb = (hi_r - lo_r) // 8
+    send = torch.cat([mine[:, plan.rows(i)[0] // 8:plan.rows(i)[1] // 8].reshape(-1) for i in range(world)])
+    ins = [P * (plan.rows(i)[1] - plan.rows(i)[0]) // 8 for i in range(world)]
+    outs = [(plane_range(world, j)[1] - plane_range(world, j)[0]) * nb for j in range(world)]
+    recv = torch.empty(sum(outs), dtype=torch.uint8, device=mine.device)
+    dist.all_to_all_single(recv, send, outs, ins)
+    return recv.view(128, nb)
+
+
+def sot_dual_lpn_rank(ctx, plan: ShardPlan, rank: int, a, rows, stream=None):
+    """Rate-1 dual LPN of one SOT instance split over the ranks: `rows` holds
+    this rank's noise blocks (rows_r x 16 bytes, the expansion of its own
+    trees); returns its rows of out = a * e mod (x^n - 1) per bit plane,
+    bit-identical to the unsplit cuot_sot_dual_lpn."""
+    import torch
+    lo, hi = plan.rows(rank)
+    nr = hi - lo
+    dev = rows.device
+    local = torch.empty((128, nr // 8), dtype=torch.uint8, device=dev)
+    ctx.bit_transpose(rows, nr, 16, 0, 128, local, stream=stream)
+    s = torch.cuda.current_stream() if stream is None else stream
+    s.synchronize()
+    mine = planes_to_owners(local, plan, rank)
+    p_lo, p_hi = plane_range(plan.world, rank)
+    if p_hi > p_lo:
+        ctx.qc_encode(a, mine.view(torch.int64), plan.n, p_hi - p_lo, stream=stream)
+        s.synchronize()
+    back = owners_to_rows(mine, plan, rank)
+    out = torch.empty((nr, 16), dtype=torch.uint8, device=dev)
+    ctx.bit_transpose(back, 128, nr // 8, 0, nr, out, stream=stream)
+    return out

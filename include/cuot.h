@@ -188,6 +188,20 @@ int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d,
                           uint64_t *out_d, void *stream);
 int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d,
                       uint64_t n, void *stream);
+/* Rate-1/2 dual LPN over 2n noise blocks e = (e0, e1):
+ *   out[i] = e0[i] ^ (a * e1 mod x^n - 1)[i]   per bit plane, i < n.
+ * in_d: 2n blocks (the expansion of 2t trees); out_d: n blocks (may equal
+ * in_d).  The reference SOT encodes only the rate-1 form
+ * (quasi_cyclic.cu:118-128); this is the 2n-leaf variant of the same code,
+ * built from the same exact product. */
+int cuot_sot_dual_lpn_r2(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *in_d,
+                         uint64_t n, cuot_block *out_d, void *stream);
+/* Receiver choice bits of the rate-1/2 form: out = e0 ^ a * e1 for the
+ * sparse 2n-bit noise e given by its nonzero positions pos_d[0..weight) in
+ * [0, 2n) (positions < n are e0, the rest e1; others are ignored). */
+int cuot_qc_encode_sparse_r2(cuot_ctx *ctx, const uint64_t *a_d,
+                             const uint64_t *pos_d, int weight, uint64_t n,
+                             uint64_t *out_d, void *stream);
 
 /* QC plan: the counterpart of the QuasiCyclic object (quasi_cyclic.h:8-26,
  * ctor quasi_cyclic.cu:51-106), which transforms `a` once and reuses it for
@@ -205,6 +219,8 @@ int cuot_qc_plan_set_batch(cuot_qc_plan *plan, int planes_per_batch);
 int cuot_qc_plan_encode(cuot_qc_plan *plan, uint64_t *planes_io_d,
                         int nplanes, void *stream);
 int cuot_qc_plan_dual_lpn(cuot_qc_plan *plan, cuot_block *io_d, void *stream);
+int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *plan, const cuot_block *in_d,
+                             cuot_block *out_d, void *stream);
 
 /* ---- batched engine ------------------------------------------------------
  * Many OT-extension instances of uneven n and depth, both roles each, run as

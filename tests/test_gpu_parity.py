@@ -289,6 +289,75 @@ def test_sot_end_to_end_cot_n20(ctx):
     assert 0.4 < cbits.mean() < 0.6
 
 
+# ---------------------------------------------------------------- SOT rate-1/2 form
+@pytest.mark.parametrize("e", [10, 13, 16])
+def test_sot_dual_lpn_r2_vs_oracle(ctx, e):
+    """out = e0 ^ a * e1 per bit plane over 2n noise blocks; one-shot, plan,
+    and in place (out aliasing the first n input blocks)."""
+    n = 1 << e
+    rng = np.random.default_rng(300 + e)
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+    a_np = to_host(a).view(np.uint64)
+    x = rng_blocks(rng, 2 * n)
+    exp = x[:n] ^ oracle.sot_dual_lpn(a_np, x[n:].copy(), n, threads=8)
+    d, out = to_dev(x), empty_blocks(n)
+    ctx.sot_dual_lpn_r2(a, d, n, out)
+    assert np.array_equal(to_host(out), exp)
+    assert np.array_equal(to_host(d), x)
+    plan = ctx.qc_plan(a, n)
+    plan.set_batch(3)
+    plan.dual_lpn_r2(d, d[:n])
+    assert np.array_equal(to_host(d)[:n], exp)
+    assert np.array_equal(to_host(d)[n:], x[n:])
+
+
+def test_qc_encode_sparse_r2(ctx):
+    n = 1 << 14
+    rng = np.random.default_rng(41)
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+    a_np = to_host(a).view(np.uint64)
+    pos = np.concatenate([rng.choice(2 * n, 37, replace=False), [0, n - 1, n, 2 * n - 1, 2 * n, 5 * n]])
+    out = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_encode_sparse_r2(a, to_dev(pos.astype(np.int64)), n, out)
+    e0 = np.zeros(n, np.uint8)
+    for p in pos[pos < n]:
+        e0[p] ^= 1
+    p1 = pos[(pos >= n) & (pos < 2 * n)] - n
+    exp = np.packbits(e0, bitorder="little").view(np.uint64) ^ oracle.qc_encode_sparse(a_np, p1, n)
+    assert np.array_equal(to_host(out).view(np.uint64), exp)
+
+
+def test_sot_end_to_end_cot_n20_r2(ctx):
+    """Rate-1/2 SOT with n = 2^20 outputs: 512 trees of depth 12 give 2n
+    noise blocks per role; after the rate-1/2 encode w_j = v_j ^ c_j * delta
+    with c = e0 ^ a * e1 from the punctured positions."""
+    t, h = 512, 12
+    n = (t << h) // 2
+    rng = np.random.default_rng(2121)
+    roots, delta, b0, b1, ch = sot_inputs(rng, t, h)
+    lv, m0, m1, rl, mc = run_sot(ctx, roots, h, delta, b0, b1, ch)
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+    v, w = to_dev(lv), to_dev(rl)
+    plan = ctx.qc_plan(a, n)
+    plan.dual_lpn_r2(v, v[:n])
+    plan.dual_lpn_r2(w, w[:n])
+    chm = ch.reshape(h, t)
+    pos = np.zeros(t, np.int64)
+    for d in range(h):
+        pos = pos * 2 + 1 - chm[d].astype(np.int64)
+    pos += np.arange(t) * (1 << h)
+    c = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_encode_sparse_r2(a, to_dev(pos), n, c)
+    cbits = np.unpackbits(to_host(c).view(np.uint8), bitorder="little").astype(bool)
+    diff = to_host(v)[:n] ^ to_host(w)[:n]
+    assert not diff[~cbits].any()
+    assert (diff[cbits] == delta).all()
+    assert 0.4 < cbits.mean() < 0.6
+
+
 # ---------------------------------------------------------------- row-range LPN / sharding
 @pytest.mark.parametrize("n,k,cuts", [(4096, 1000, [0, 1024, 2048, 4096]), (1003, 77, [0, 500, 1003]),
                                       (10, 5, [0, 4, 8, 10])])
@@ -325,6 +394,35 @@ def test_sharded_ferret_extend_equals_unsplit(ctx):
     rleaves = oracle.ferret_pprf_recver(mc, choice, ss, h, threads=4)
     assert np.array_equal(np.concatenate(vs), oracle.lpn_primal(seed, kk_s, leaves))
     assert np.array_equal(np.concatenate(ws), oracle.lpn_primal(seed, kk_r, rleaves))
+
+
+def test_sharded_sot_dual_lpn_one_rank_nccl(ctx):
+    """cuot_b200.shard's SOT path (transpose -> all-to-all to plane owners ->
+    encode -> reverse all-to-all -> transpose) through a one-rank NCCL group
+    on this GPU equals the unsplit dual LPN.  The multi-rank exchange itself
+    is covered by the gloo tests in test_shard.py."""
+    import datetime
+    import socket
+    import torch.distributed as dist
+    from cuot_b200.shard import ShardPlan, sot_dual_lpn_rank
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        t, h = 16, 10
+        n = t << h
+        rng = np.random.default_rng(4242)
+        rows = rng_blocks(rng, n)
+        a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+        ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
+        out = sot_dual_lpn_rank(ctx, ShardPlan(t, h, 1), 0, a, to_dev(rows))
+        exp = oracle.sot_dual_lpn(to_host(a).view(np.uint64), rows, n, threads=8)
+        assert np.array_equal(to_host(out), exp)
+    finally:
+        dist.destroy_process_group()
 
 
 def test_pprf_128_threads_per_tree_matches_oracle(ctx):
