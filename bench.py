@@ -235,6 +235,12 @@ NCU_TRAFFIC_PER_STEP = {
     "sot_n20:dual_lpn": 2892.64e6,
 }
 
+def ntt_butterflies(n: int) -> int:
+    """Radix-2 butterflies of one SOT dual LPN, both roles: 128 planes, a
+    forward and an inverse n-point transform each."""
+    return 2 * 128 * 2 * (n // 2) * (n.bit_length() - 1)
+
+
 AES_PEAK_MODEL = ("T-table AES: 160 shared-memory lookups per block (10 rounds x 16), one conflict-free "
                   "32-lane lookup wavefront per clock per SM; peak = SMs x 32 x median SM clock / 160")
 
@@ -525,6 +531,23 @@ def run_batch(args):
     dom = max(stages, key=lambda k: stages[k])
     peaks, peak_kind = measured_peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
+    # traffic: the batch is too large for a multi-metric ncu capture; the SOT
+    # encode runs the same NTT kernels as sot_n20, whose captured DRAM bytes
+    # per COT (both roles) scale it; other stages have no capture (null)
+    traffic = None
+    if dom == "sot_encode":
+        traffic = NCU_TRAFFIC_PER_STEP["sot_n20:dual_lpn"] / (1 << 20) * n_sot
+    props = torch.cuda.get_device_properties(local)
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    aes_peak = props.multi_processor_count * 32 * mhz * 1e6 / 160
+    aes_counts = {"pprf_send": sum(2 * i.t * ((1 << i.h) - 1) for i in insts),
+                  "pprf_recv": sum(2 * i.t * ((1 << i.h) - 1) for i in insts),
+                  "lpn": sum(2 * i.n * i.d // 4 for i in insts if i.kind == KIND_FERRET)}
+    aes = {"peak_aes_per_s": aes_peak, "model": AES_PEAK_MODEL}
+    for k, cnt in aes_counts.items():
+        a = cnt / (stages[k] / 1e3)
+        aes[k] = {"aes_per_step": cnt, "aes_per_s": a, "frac": a / aes_peak}
+    bfly = sum(ntt_butterflies(i.n) for i in insts if i.kind != KIND_FERRET)
     out = {
         "metric": metric_name(args.workload),
         "value": world * cots / (ms / 1e3), "unit": "COTs/s", "n_gpus": world, "steps": args.steps,
@@ -538,9 +561,13 @@ def run_batch(args):
         "autotuned": tuned,
         "stages_ms": stages,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "algorithmic_bytes_per_step": alg[dom]},
+                     "algorithmic_bytes_per_step": alg[dom],
+                     "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu capture "
+                              "by SOT COTs (2,759 DRAM bytes per COT, cold cache per kernel)"},
+        "aes_roofline": aes,
+        "ntt": {"butterflies_per_step": bfly, "butterflies_per_s": bfly / (stages["sot_encode"] / 1e3)},
         "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": launches * args.steps,
@@ -709,6 +736,9 @@ def run_ours(args):
         "clocks": clocks,
     }
     out["aes_roofline"] = aes_roofline(inst, stages, clocks, torch.cuda.get_device_properties(local))
+    if inst.spec["kind"] == "sot":
+        b = ntt_butterflies(inst.n)
+        out["ntt"] = {"butterflies_per_step": b, "butterflies_per_s": b / (lpn_ms / 1e3)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample(args.workload, threads)

@@ -11,6 +11,13 @@ quasi-cyclic encode -> transpose stages; nothing returns to the host between
 stages.  Latency = completion (outputs in device memory, observed by the
 loop) - arrival.
 
+Scheduling: requests are admitted in arrival order; optionally at most
+`max_big` requests with n >= `big_n` run at once (one such request already
+fills the GPU, two only time-slice it and both finish late) while smaller
+requests may pass a big one that waits for that reason.  The executor can
+launch small requests on a higher-priority stream so their blocks are
+scheduled ahead of a running big request's.
+
 Host-side failure handling: a request waiting in the queue longer than
 `max_queue_wait` seconds times out; a request can be cancelled while
 queued; a request whose footprint can never fit the budget is rejected.  No
@@ -97,12 +104,16 @@ class Server:
     the same interface for host-only tests)."""
 
     def __init__(self, executor, budget_bytes: float = 120e9, max_queue_wait: float | None = None,
-                 poll_s: float = 20e-6):
+                 poll_s: float = 20e-6, big_n: int | None = None, max_big: int = 1):
         self.ex = executor
         self.budget = float(budget_bytes) - float(executor.reserved_bytes())
         self.max_queue_wait = max_queue_wait
         self.poll_s = poll_s
+        self.big_n, self.max_big = big_n, max_big
         self.cancelled: set[int] = set()
+
+    def _is_big(self, r: Request) -> bool:
+        return self.big_n is not None and r.n >= self.big_n
 
     def cancel(self, rid: int):
         self.cancelled.add(rid)
@@ -145,9 +156,23 @@ class Server:
                     else:
                         keep.append(r)
                 queue = keep
-            # admission: FIFO, as slots and memory free up
-            while queue and free_slots and used + footprint(queue[0]) <= self.budget:
-                r = queue.popleft()
+            # admission in arrival order, as slots and memory free up; memory
+            # is head-of-line (no request passes one that does not fit), the
+            # big-request limit is not
+            while queue and free_slots:
+                nbig = sum(self._is_big(b) for b in busy.values())
+                pick = None
+                for j, r in enumerate(queue):
+                    if used + footprint(r) > self.budget:
+                        break
+                    if self._is_big(r) and nbig >= self.max_big:
+                        continue
+                    pick = j
+                    break
+                if pick is None:
+                    break
+                r = queue[pick]
+                del queue[pick]
                 s = free_slots.pop()
                 used += footprint(r)
                 r.t_admit = clock() - t0
@@ -178,15 +203,19 @@ class GpuExecutor:
     per slot at a time.  Inputs come from the request seed's PRNG stream on
     the device (block layout in `_inputs`)."""
 
-    def __init__(self, slots: int = 8, device: int = 0, max_log_n: int = 24, keep_outputs: bool = False):
+    def __init__(self, slots: int = 8, device: int = 0, max_log_n: int = 24, keep_outputs: bool = False,
+                 high_priority_below_n: int | None = None):
         import torch
         import cuot_b200
         self.torch, self.cb = torch, cuot_b200
         self.slots = slots
         self.keep_outputs = keep_outputs
+        self.high_below = high_priority_below_n
         torch.cuda.set_device(device)
         self.ctxs = [cuot_b200.Context(device) for _ in range(slots)]
         self.streams = [torch.cuda.Stream() for _ in range(slots)]
+        # requests with n < high_below run on a higher-priority stream of their slot
+        self.streams_hi = [torch.cuda.Stream(priority=-1) for _ in range(slots)] if self.high_below else None
         self.events = [None] * slots
         self.state = [None] * slots
         nmax = 1 << max_log_n
@@ -236,6 +265,8 @@ class GpuExecutor:
     def start(self, slot: int, r: Request):
         torch = self.torch
         ctx, st = self.ctxs[slot], self.streams[slot]
+        if self.streams_hi is not None and r.n < self.high_below:
+            st = self.streams_hi[slot]
         with torch.cuda.stream(st):
             inp = self._inputs(ctx, r, st)
             t, h, n = r.t, r.h, r.n

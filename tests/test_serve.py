@@ -74,3 +74,17 @@ def test_stream_shape():
     assert all(14 <= (r.n.bit_length() - 1) <= 24 and 10 <= r.h <= 14 for r in s)
     assert sorted(r.arrival for r in s) == [r.arrival for r in s]
     assert 0.3 < sum(r.kind for r in s) / len(s) < 0.7
+
+
+def test_big_request_limit_lets_small_ones_pass():
+    """At most one request with n >= big_n runs at a time; small requests
+    queued behind a waiting big one are admitted meanwhile."""
+    big = [Request(i, KIND_FERRET, 1 << 6, 10, bytes(16), 0.0, k=10) for i in range(2)]     # n = 2^16
+    small = [req(10 + i, 0.0) for i in range(3)]                                            # n = 2^14
+    ex = FakeExecutor(slots=4, service_s=0.03)
+    rep = Server(ex, budget_bytes=1e12, big_n=1 << 16, max_big=1).run(big + small)
+    assert rep["done"] == 5
+    order = [rid for ev, rid in ex.log if ev == "start"]
+    assert order[0] == 0 and order.index(1) > order.index(12)   # the second big waits for the first
+    assert big[1].t_admit >= big[0].t_done - 1e-3
+    assert all(s.t_admit < big[0].t_done for s in small)
