@@ -262,56 +262,56 @@ def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
     return res
 
 
-def e2e_step(inst: Instance, host, stream):
-    """Same step through the public API with HOST buffers: H2D of the step's
-    inputs from pinned memory, D2H of the results, inside the timed region.
-    Returns (h2d_bytes, d2h_bytes)."""
+def e2e_inputs(inst: Instance, host):
+    """(pinned host tensor, device tensor) pairs of one step's inputs."""
+    pairs = [(host["roots"], inst.d_roots), (host["choice"], inst.d_choice)]
+    if inst.spec["kind"] == "ferret":
+        pairs += [(host["kk_s"], inst.d_kk_s), (host["kk_r"], inst.d_kk_r)]
+    else:
+        pairs += [(host["b0"], inst.d_b0), (host["b1"], inst.d_b1), (host["mc"], inst.d_mc)]
+    return pairs
+
+
+def e2e_outputs(inst: Instance, host):
+    """(device result, pinned host tensor) pairs returned by every step."""
+    pairs = [(inst.leaves_s[:inst.n], host["v"]), (inst.leaves_r[:inst.n], host["w"])]
+    if inst.spec["kind"] != "ferret":
+        pairs.append((inst.cbits, host["c"]))
+    return pairs
+
+
+def e2e_compute(inst: Instance, host, stream) -> int:
+    """The step's device work through the public API on `stream`.  Ferret's
+    level sums and secret sums go to the host inside the step, as in
+    dev_layer.cu:40-41,50; returns those bytes."""
     torch = inst.torch
-    h2d = d2h = 0
+    d2h = 0
     with torch.cuda.stream(stream):
-        inst.d_roots.copy_(host["roots"], non_blocking=True)
-        inst.d_choice.copy_(host["choice"], non_blocking=True)
-        h2d += host["roots"].numel() + host["choice"].numel()
         if inst.spec["kind"] == "ferret":
-            inst.d_kk_s.copy_(host["kk_s"], non_blocking=True)
-            inst.d_kk_r.copy_(host["kk_r"], non_blocking=True)
-            h2d += host["kk_s"].numel() + host["kk_r"].numel()
             inst.sctx.ferret_pprf_sender(inst.d_roots, inst.h, inst.delta, inst.leaves_s, inst.lsum, inst.rsum,
                                          inst.ss, stream=stream)
-            # sums and secret sums go to the host (sent to the receiver by the OT), as in
-            # dev_layer.cu:40-41,50; the chosen messages come back to the receiver's GPU
-            host["lsum"].copy_(inst.lsum, non_blocking=True)
-            host["rsum"].copy_(inst.rsum, non_blocking=True)
-            host["ss"].copy_(inst.ss, non_blocking=True)
-            d2h += 3 * 0 + host["lsum"].numel() + host["rsum"].numel() + host["ss"].numel()
+            for k, d in (("lsum", inst.lsum), ("rsum", inst.rsum), ("ss", inst.ss)):
+                host[k].copy_(d, non_blocking=True)
+                d2h += host[k].numel()
             torch.where(inst.d_choice.view(-1, 1).bool(), inst.rsum, inst.lsum, out=inst.mc)
             inst.rctx.ferret_pprf_recver(inst.mc, inst.d_choice, inst.ss, inst.h, inst.leaves_r, stream=stream)
             inst.sctx.lpn_primal(inst.seed, inst.d_kk_s, inst.leaves_s, d=inst.d, stream=stream)
             inst.rctx.lpn_primal(inst.seed, inst.d_kk_r, inst.leaves_r, d=inst.d, stream=stream)
         else:
-            inst.d_b0.copy_(host["b0"], non_blocking=True)
-            inst.d_b1.copy_(host["b1"], non_blocking=True)
-            inst.d_mc.copy_(host["mc"], non_blocking=True)
-            h2d += host["b0"].numel() + host["b1"].numel() + host["mc"].numel()
             inst.sctx.sot_pprf_sender(inst.d_roots, inst.h, inst.delta, inst.d_b0, inst.d_b1, inst.leaves_s,
                                       inst.m0, inst.m1, stream=stream)
             inst.rctx.sot_pprf_recver(inst.m0, inst.m1, inst.d_mc, inst.d_choice, inst.t, inst.h, inst.leaves_r,
                                       stream=stream)
+            n = inst.n
             if inst.r2:
-                n = inst.n
                 inst.plan_s.dual_lpn_r2(inst.leaves_s, inst.leaves_s[:n], stream=stream)
                 inst.plan_r.dual_lpn_r2(inst.leaves_r, inst.leaves_r[:n], stream=stream)
                 inst.rctx.qc_encode_sparse_r2(inst.a, inst.d_pos, n, inst.cbits, stream=stream)
             else:
                 inst.plan_s.dual_lpn(inst.leaves_s, stream=stream)
                 inst.plan_r.dual_lpn(inst.leaves_r, stream=stream)
-                inst.rctx.qc_encode_sparse(inst.a, inst.d_pos, inst.n, inst.cbits, stream=stream)
-            host["c"].copy_(inst.cbits, non_blocking=True)
-            d2h += host["c"].numel() * 8
-        host["v"].copy_(inst.leaves_s[:inst.n], non_blocking=True)
-        host["w"].copy_(inst.leaves_r[:inst.n], non_blocking=True)
-        d2h += host["v"].numel() + host["w"].numel()
-    return h2d, d2h
+                inst.rctx.qc_encode_sparse(inst.a, inst.d_pos, n, inst.cbits, stream=stream)
+    return d2h
 
 
 def make_host(inst: Instance):
@@ -486,6 +486,29 @@ def run_batch(args):
             ms = tt.item()
         return ms
 
+    def timed_pipelined(fn, pipe):
+        """Like timed(), but one event pair around all steps, closed after
+        the last step's host copy (steps overlap, so per-step events would
+        not bracket a step's own work)."""
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn(stream)
+        pipe.join()
+        b.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = a.elapsed_time(b) / args.steps
+        if dist:
+            tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = tt.item()
+        return ms
+
     clk = ClockSampler(local)
     clk.start()
     time.sleep(0.3)
@@ -510,16 +533,21 @@ def run_batch(args):
     h2d = sum(hs.numel() * hs.element_size() for hs, _ in host_in)
     d2h = sum(hs.numel() * hs.element_size() for hs, _ in host_out)
 
-    def e2e(st):
+    # the host copy of step i overlaps step i+1's compute (HostPipeline)
+    from cuot_b200.pipeline import HostPipeline
+    pipe = HostPipeline([dv for _, dv in host_out], stream=stream)
+
+    def run_flushed(st):
         with torch.cuda.stream(st):
-            for hs, dv in host_in:
-                dv.copy_(hs, non_blocking=True)
+            flush.zero_()  # L2 flush between steps, as in the device-timed loop
         batch.run(st)
-        with torch.cuda.stream(st):
-            for hs, dv in host_out:
-                hs.copy_(dv, non_blocking=True)
+
+    def e2e(st):
+        pipe.step(host_in, run_flushed, [hs for hs, _ in host_out])
+
     e2e(stream)
-    e2e_ms = timed(e2e)
+    pipe.join()
+    e2e_ms = timed_pipelined(e2e, pipe)
 
     names = ["pprf_send", "pprf_recv", "lpn", "sot_encode"]
     stages = dict(zip(names, phases))
@@ -601,11 +629,15 @@ def run_served(args, device: int) -> dict:
     from cuot_b200.serve import GpuExecutor, Server, make_stream, sustained_rate
 
     lo, hi = 14, 24
-    cont = GpuExecutor(slots=args.serve_slots, device=device, max_log_n=hi)
+    # small requests (n < 2^20) on high-priority streams; at most one request
+    # with n >= 2^22 in flight (a sweep of these two knobs on this workload:
+    # this pair beat plain per-request execution on p50, p99 and mean)
+    big_n, prio_n = 1 << 22, 1 << 20
+    cont = GpuExecutor(slots=args.serve_slots, device=device, max_log_n=hi, high_priority_below_n=prio_n)
     probe = make_stream(min(100, args.serve_requests), rate=0.0, seed=5, lo=lo, hi=hi)
     rate = sustained_rate(cont, probe)
     reqs = make_stream(args.serve_requests, rate=rate, seed=6, lo=lo, hi=hi)
-    rep = Server(cont, budget_bytes=120e9).run(reqs)
+    rep = Server(cont, budget_bytes=120e9, big_n=big_n).run(reqs)
     del cont
     torch.cuda.synchronize()
     plain = GpuExecutor(slots=1, device=device, max_log_n=hi)
@@ -616,6 +648,7 @@ def run_served(args, device: int) -> dict:
     keys = ("done", "cots_per_s", "p50_ms", "p99_ms", "mean_ms", "wall_s")
     return {"requests": args.serve_requests, "slots": args.serve_slots, "budget_gb": 120,
             "log2_n": [lo, hi], "rate_rps": rate,
+            "policy": {"high_priority_below_n": prio_n, "max_in_flight_with_n_ge": [big_n, 1]},
             "continuous": {k: rep[k] for k in keys},
             "plain_per_request": {k: rep_plain[k] for k in keys},
             "note": "latency = arrival -> outputs in device memory; rate = 0.9 x saturation throughput "
@@ -677,18 +710,35 @@ def run_ours(args):
         ms, pprf_ms, lpn_ms = tt.tolist()
     value = world * n / (ms / 1e3)
 
-    # e2e through the public API with host buffers
+    # e2e through the public API with pinned host buffers: every step's inputs
+    # go host -> device and its outputs device -> host inside the timed
+    # region; the host copy of step i overlaps step i+1's compute
+    from cuot_b200.pipeline import HostPipeline
     host = make_host(inst)
     stream = torch.cuda.Stream()
+    outs = e2e_outputs(inst, host)
+    pipe = HostPipeline([d for d, _ in outs], stream=stream)
+
+    def compute(st, extra):
+        with torch.cuda.stream(st):
+            flush.zero_()  # L2 flush between steps, as in the device-timed loop
+        extra.append(e2e_compute(inst, host, st))
+
+    def e2e_one():
+        extra = []
+        h2d, d2h = pipe.step(e2e_inputs(inst, host), lambda st: compute(st, extra), [h for _, h in outs])
+        return h2d, d2h + extra[0]
     for _ in range(max(1, args.warmup)):
-        e2e_step(inst, host, stream)
+        e2e_one()
+    pipe.join()
     stream.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
         dist.barrier()
     e0.record(stream)
     for _ in range(args.steps):
-        h2d, d2h = e2e_step(inst, host, stream)
+        h2d, d2h = e2e_one()
+    pipe.join()
     e1.record(stream)
     stream.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -760,7 +810,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=300,
+    ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the served stream reported with mixed64 (0: skip; configs[4] uses 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")

@@ -222,8 +222,8 @@ int check_item(const cuot_batch_item &it, int i) {
     if (it.k < 1 || it.k > 0x7fffffffll || it.d < 1 || it.d > 32 || !it.kk_send_d || !it.kk_recv_d)
       return fail(CUOT_EINVAL, "item %d: bad LPN arguments", i);
   } else {
-    if (n < 1024 || n > (1ull << 26) || (n & (n - 1)))
-      return fail(CUOT_EINVAL, "item %d: SOT n=%llu must be a power of two in [2^10, 2^26]", i,
+    if (n < 1024 || n > (1ull << 25) || (n & (n - 1)))
+      return fail(CUOT_EINVAL, "item %d: SOT n=%llu must be a power of two in [2^10, 2^25]", i,
                   (unsigned long long)n);
     if (!it.base0_d || !it.base1_d || !it.mc_d || !it.a_d || !it.punct_d || !it.cbits_d)
       return fail(CUOT_EINVAL, "item %d: null SOT pointer", i);

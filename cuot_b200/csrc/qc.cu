@@ -31,7 +31,24 @@ namespace cuot {
 
 constexpr uint32_t kP = 469762049u;
 constexpr uint32_t kG = 3u;
-constexpr int kQcThreads = 256;
+// Launch shape of the NTT passes (compile-time knobs, swept on B200):
+// threads per CTA, CTAs per SM the register budget is sized for, the unroll
+// depth of the column passes' strided global loads, and the elements per
+// CTA of the row pass.
+#ifndef CUOT_QC_THREADS
+#define CUOT_QC_THREADS 256
+#endif
+#ifndef CUOT_QC_MIN_BLOCKS
+#define CUOT_QC_MIN_BLOCKS 4
+#endif
+#ifndef CUOT_QC_COL_UNROLL
+#define CUOT_QC_COL_UNROLL 4
+#endif
+#ifndef CUOT_QC_ROW_ELEMS
+#define CUOT_QC_ROW_ELEMS 4096
+#endif
+constexpr int kQcThreads = CUOT_QC_THREADS;
+constexpr int kQcColUnroll = CUOT_QC_COL_UNROLL;
 constexpr int kCW = 8;  // columns per CTA in the column passes
 
 __host__ __device__ __forceinline__ uint32_t mulmod(uint32_t a, uint32_t b) {
@@ -204,7 +221,7 @@ __device__ __forceinline__ void stage_tw(uint2 *dst, const uint2 *src, int cnt) 
 // Pass A.  bits: plane-major, plane_words 32-bit words per plane.
 // grid (N2 / kCW, nplanes_batch).  Y: [plane][N1][N2].
 template <int E1>
-__global__ void __launch_bounds__(kQcThreads, 4) qc_col_fwd(
+__global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_col_fwd(
     const uint32_t *__restrict__ bits, uint64_t plane_words, int e2,
     const uint2 *__restrict__ tw1f, const uint2 *__restrict__ fsf, uint32_t *__restrict__ Y) {
   extern __shared__ uint32_t xs[];
@@ -215,7 +232,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_fwd(
   const int c0 = blockIdx.x * kCW;
   const uint64_t plane = blockIdx.y;
   const uint32_t *pb = bits + plane * plane_words;
-#pragma unroll 4
+#pragma unroll kQcColUnroll
   for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
     const uint64_t bit = uint64_t(j1) * N2 + c0;
     const uint32_t w = __ldg(&pb[bit >> 5]) >> (bit & 31);
@@ -226,7 +243,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_fwd(
   ntt_smem<E1, true>(xs, kCW, ld, tws);
   // x w_n^(j2 * rev(r)) on the way out; fsf is [r][j2], read coalesced
   uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
-#pragma unroll 4
+#pragma unroll kQcColUnroll
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
@@ -239,7 +256,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_fwd(
 // build ahat).  Plane y of the launch uses ahat.p[(ahat.first + y) / ahat.per]
 // (planes of several encodes, each with its own `a`, can share a launch).
 template <int E2>
-__global__ void __launch_bounds__(kQcThreads, 4) qc_row(
+__global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_row(
     uint32_t *__restrict__ Y, int e1, int rows_per_cta,
     const uint2 *__restrict__ tw2f, const uint2 *__restrict__ tw2i,
     AhatTab ahat_tab, int mode) {
@@ -282,7 +299,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_row(
 // Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits, written
 // (accumulate == 0) or XORed into (accumulate == 1; the rate-1/2 form).
 template <int E1>
-__global__ void __launch_bounds__(kQcThreads, 4) qc_col_inv(
+__global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_col_inv(
     const uint32_t *__restrict__ Y, int e2, const uint2 *__restrict__ fsi,
     const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes, int accumulate) {
   extern __shared__ uint32_t xs[];
@@ -293,7 +310,7 @@ __global__ void __launch_bounds__(kQcThreads, 4) qc_col_inv(
   const int c0 = blockIdx.x * kCW;
   const uint64_t plane = blockIdx.y;
   const uint32_t *Yp = Y + plane * (uint64_t(N1) << e2);
-#pragma unroll 4
+#pragma unroll kQcColUnroll
   for (int idx = threadIdx.x; idx < kCW * N1; idx += blockDim.x) {
     const int r = idx / kCW, c = idx % kCW;
     const uint64_t o = uint64_t(r) * N2 + c0 + c;
@@ -471,7 +488,7 @@ static int col_smem(const QcTables *t) {
 }
 static int row_rows(const QcTables *t) {
   const int N2 = 1 << t->e2;
-  int r = 4096 / N2;
+  int r = CUOT_QC_ROW_ELEMS / N2;
   if (r < 1) r = 1;
   if (r > (1 << t->e1)) r = 1 << t->e1;
   return r;
@@ -585,8 +602,8 @@ static int dual_lpn_r2(const QcTables *t, const uint2 *ahat, const cuot_block *i
 }
 
 static int check_n(uint64_t n, int *e) {
-  if (n < 1024 || n > (1ull << 26) || (n & (n - 1)))
-    return fail(CUOT_EINVAL, "QC n=%llu must be a power of two in [2^10, 2^26]",
+  if (n < 1024 || n > (1ull << 25) || (n & (n - 1)))
+    return fail(CUOT_EINVAL, "QC n=%llu must be a power of two in [2^10, 2^25]",
                 (unsigned long long)n);
   *e = __builtin_ctzll(n);
   return CUOT_OK;

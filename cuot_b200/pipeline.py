@@ -1,0 +1,61 @@
+"""Host-facing pipelining of repeated OT-extension steps.
+
+A step takes inputs from pinned host memory, computes on the device and
+returns its outputs to pinned host memory.  Run back to back, the device
+would idle during each step's device-to-host copy (PCIe-bound: a ferret_b13
+step returns 336 MB in ~6.7 ms against ~2.8 ms of compute).  HostPipeline
+overlaps that copy with the next step's compute: the outputs are first copied
+device-to-device into a staging buffer on the compute stream (HBM speed), and
+a separate copy stream moves the staging buffer to the host while the compute
+stream runs the next step.  Ordering: the staging copy of step i+1 waits for
+the host copy of step i (an event), so at most one step's results are in
+flight; inputs are copied on the compute stream ahead of the step that reads
+them.
+"""
+from __future__ import annotations
+
+
+class HostPipeline:
+    def __init__(self, outputs, stream=None, copy_stream=None):
+        import torch
+        self.torch = torch
+        self.outputs = list(outputs)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        self.copy_stream = copy_stream if copy_stream is not None else torch.cuda.Stream()
+        self.staging = [torch.empty_like(o) for o in self.outputs]
+        self._d2h_done = None
+
+    def step(self, inputs, compute, host_outputs):
+        """inputs: [(host_tensor, device_tensor)] copied host->device first;
+        compute(stream) enqueues the step's device work; host_outputs: pinned
+        host tensors receiving this step's outputs (same shapes as `outputs`).
+        Returns (h2d_bytes, d2h_bytes).  Nothing here blocks the host."""
+        torch, st = self.torch, self.stream
+        h2d = d2h = 0
+        with torch.cuda.stream(st):
+            for h, d in inputs:
+                d.copy_(h, non_blocking=True)
+                h2d += h.numel() * h.element_size()
+        compute(st)
+        if self._d2h_done is not None:
+            st.wait_event(self._d2h_done)
+        with torch.cuda.stream(st):
+            for o, s in zip(self.outputs, self.staging):
+                s.copy_(o, non_blocking=True)
+        staged = torch.cuda.Event()
+        staged.record(st)
+        cs = self.copy_stream
+        cs.wait_event(staged)
+        with torch.cuda.stream(cs):
+            for s, h in zip(self.staging, host_outputs):
+                h.copy_(s, non_blocking=True)
+                d2h += h.numel() * h.element_size()
+        self._d2h_done = torch.cuda.Event()
+        self._d2h_done.record(cs)
+        return h2d, d2h
+
+    def join(self):
+        """Makes the compute stream wait for the last host copy (so an event
+        recorded on it after join() covers every step's results)."""
+        if self._d2h_done is not None:
+            self.stream.wait_event(self._d2h_done)

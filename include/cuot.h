@@ -173,7 +173,9 @@ int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
  * gpu/gpu_ops.cu:102-109).  encode: every plane r (n bits, planes
  * consecutive) becomes a * plane_r mod (x^n - 1) over GF(2), exactly
  * (replaces the float cuFFT path of QuasiCyclic::encode_dense,
- * quasi_cyclic.cu:118-128).  n a power of two in [2^10, 2^26].
+ * quasi_cyclic.cu:118-128).  n a power of two in [2^10, 2^25] (the
+ * row pass keeps 2^ceil(log n / 2) twiddle pairs of both directions in
+ * shared memory).
  * encode_sparse: out = a * e mod (x^n - 1), e = indicator of pos_d[0..w)
  * (QuasiCyclic::encode_sparse, quasi_cyclic.cu:130-161).
  * dual_lpn: io_d holds n blocks; block j becomes XOR_{i: a_i = 1}
@@ -253,7 +255,7 @@ typedef struct {
   uint8_t lpn_seed[16];
   const cuot_block *kk_send_d;    /* [k] */
   const cuot_block *kk_recv_d;    /* [k] */
-  /* SOT (n a power of two in [2^10, 2^26]) */
+  /* SOT (n a power of two in [2^10, 2^25]) */
   const cuot_block *base0_d;      /* [h][t] sender base-OT messages */
   const cuot_block *base1_d;      /* [h][t] */
   const cuot_block *mc_d;         /* [h][t] receiver's chosen messages */
