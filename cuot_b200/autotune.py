@@ -117,9 +117,9 @@ def tune_single(ctx, inst, table: TuningTable | None = None, reps: int = 3):
                                                                stream=st), stream, reps)
         hit = {"pprf_threads": min(res, key=res.get), "pprf_ms": res}
         if inst.kind == 1:
-            base = max(1, (64 << 20) // (4 * inst.n))
+            base = max(1, (512 << 20) // (4 * inst.n))  # the library's default batch
             qres = {}
-            for planes in sorted({max(1, base // 2), min(128, base), min(128, base * 2)}):
+            for planes in sorted({max(1, base // 4), max(1, min(128, base // 2)), min(128, base)}):
                 ctx.set_tuning(ctx.TUNE_QC_PLANES, planes)
                 qres[planes] = _time(lambda st: ctx.sot_dual_lpn(inst.a, inst.v, inst.n, stream=st), stream, reps)
             hit["qc_planes_per_pass"] = min(qres, key=qres.get)

@@ -220,8 +220,9 @@ class GpuExecutor:
         self.state = [None] * slots
         nmax = 1 << max_log_n
         # per-slot scratch: PPRF levels (16n) or dual LPN (8n ahat + 16n planes
-        # + the NTT batch, >= 4n), plus the QC twiddle tables of every size
-        self.scratch_per_slot = 28 * nmax + (64 << 20)
+        # + the NTT batch: up to 512 MiB, at least 4n), plus the QC twiddle
+        # tables of every size
+        self.scratch_per_slot = 24 * nmax + max(4 * nmax, 512 << 20) + (64 << 20)
         self.tables_per_slot = sum(16 * (1 << e) + 32 * (1 << (e // 2 + 1)) for e in range(10, max_log_n + 1))
         for c in self.ctxs:
             c.reserve(self.scratch_per_slot)
