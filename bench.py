@@ -5,13 +5,15 @@ receiver) of one OT-extension instance, seeded synthetic inputs of the named
 shape.
 
 Workloads (--workload):
-  mixed64     batched mix: 64 instances, half SOT and
+  mixed64     batched mix (the headline line): 64 instances, half SOT and
               half Ferret-style, log2 n uniform in [16, 22], depth 10-14; run
               as one CUDA-graph device program (value) and one instance at a
               time through the plain entry points (plain.value).
+  mixed64_small  the same mix with log2 n in [12, 16]: launch-bound
+              instances, where one device program pays off most.
   sot_n20     plain SOT, n = 2^20: 256 GGM trees of depth 12 (both roles),
-              exact quasi-cyclic encode of the 128 bit planes of the 2n-bit
-              noise vector, transposes both ways, plus the
+              exact quasi-cyclic encode of the 128 bit planes of the n noise
+              blocks, transposes both ways, plus the
               receiver's choice-bit encode.
   sot_n20_r2  SOT rate-1/2 form with n = 2^20 outputs: 512 trees of depth
               12 give 2n noise blocks e = (e0, e1) per role, encoded as
@@ -47,6 +49,7 @@ import numpy as np
 
 WORKLOADS = {
     "mixed64": dict(kind="batch", count=64, lo=16, hi=22),
+    "mixed64_small": dict(kind="batch", count=64, lo=12, hi=16),
     "sot_n20": dict(kind="sot", t=256, h=12),
     "sot_n20_r2": dict(kind="sot", t=512, h=12, r2=True),
     "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
@@ -55,6 +58,8 @@ WORKLOADS = {
 CONFIG_TEXT = {
     "mixed64": "batched mix: 64 instances (32 SOT, 32 Ferret-style), log2 n uniform in [16,22], depth 10-14, "
                "both roles, one CUDA-graph program vs the plain one-instance-at-a-time path",
+    "mixed64_small": "batched mix of small instances: 64 instances (32 SOT, 32 Ferret-style), log2 n uniform in "
+                     "[12,16], depth 10-14, both roles, one CUDA-graph program vs the plain one-instance-at-a-time path",
     "sot_n20": "plain SOT n=2^20: 256 GGM trees depth 12, exact QC encode of 128 planes, transposes (both roles)",
     "sot_n20_r2": "plain SOT rate-1/2, n=2^20 outputs: 512 GGM trees depth 12 (2n noise blocks), "
                   "out = e0 ^ a*e1 exact on 128 planes, transposes (both roles)",
@@ -232,7 +237,7 @@ class Instance:
 # intermediate that steady state keeps in L2 is counted).
 NCU_TRAFFIC_PER_STEP = {
     "ferret_b13:lpn": 570.44e6,
-    "sot_n20:dual_lpn": 2892.64e6,
+    "sot_n20:dual_lpn": 3990.2e6,
 }
 
 def ntt_butterflies(n: int) -> int:
@@ -431,7 +436,7 @@ def run_reference(args):
 
 
 def run_batch(args):
-    """the mixed batch, batched (graph) vs plain."""
+    """The mixed batch of instances, batched (graph) vs plain."""
     import torch
     import cuot_b200
     from cuot_b200.batch import KIND_FERRET, Batch, mixed_workload
@@ -452,10 +457,8 @@ def run_batch(args):
     stream = torch.cuda.Stream()
     tuned = {}
     if not args.no_autotune:
-        from cuot_b200.autotune import DEFAULT_TABLE, TuningTable, tune_batch
-        out_dir = os.path.join(ROOT, "gpurun_out")
-        path = os.path.join(out_dir, "tuning.json") if os.path.isdir(out_dir) else DEFAULT_TABLE
-        tuned, _ = tune_batch(ctx, insts, table=TuningTable(path))
+        from cuot_b200.autotune import TuningTable, tune_batch
+        tuned, _ = tune_batch(ctx, insts, table=TuningTable())  # CUOT_TUNING_TABLE sets its path
     batch = Batch(ctx, insts, use_graph=True, **tuned)
     for _ in range(args.warmup):
         batch.run(stream)
@@ -593,7 +596,7 @@ def run_batch(args):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": alg[dom],
                      "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu capture "
-                              "by SOT COTs (2,759 DRAM bytes per COT, cold cache per kernel)"},
+                              "by SOT COTs (3,805 DRAM bytes per COT, cold cache per kernel)"},
         "aes_roofline": aes,
         "ntt": {"butterflies_per_step": bfly, "butterflies_per_s": bfly / (stages["sot_encode"] / 1e3)},
         "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
@@ -621,7 +624,7 @@ def run_batch(args):
 
 
 def run_served(args, device: int) -> dict:
-    """served request stream.  Saturation throughput of the
+    """The served request stream.  Saturation throughput of the
     continuous-batching server sets the sustained rate (90 % of it); the
     same Poisson stream is then served by the continuous-batching server and
     by plain per-request execution (one request at a time)."""
@@ -811,7 +814,7 @@ def main():
     ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=1000,
-                    help="requests of the served stream reported with mixed64 (0: skip; configs[4] uses 10000)")
+                    help="requests of the served stream reported with mixed64 (0: skip; the full served configuration is 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()

@@ -122,7 +122,7 @@ class Batch:
 
 
 def mixed_workload(ctx, count: int = 64, seed: int = 2024, lo: int = 16, hi: int = 22):
-    """BASELINE configs[3]-shaped mix: `count` instances, half SOT and half
+    """The mixed batch: `count` instances, half SOT and half
     Ferret-style, log2(n) uniform over [lo, hi], depth in [10, 14] with t =
     n / 2^h; Ferret k = ceil(n * 452000 / 10485760) (ferret_b13's ratio)."""
     rng = np.random.default_rng(seed)

@@ -84,8 +84,8 @@ def build_oracle() -> str:
     subprocess.check_call(["make", "-s", "-C", odir])
     ref_script = os.path.join(odir, "build_ref.sh")
     ref_lib = os.path.join(odir, "_ref", "libctref.so")
-    if os.path.isdir("/root/reference") and _stale(ref_lib, [os.path.join(odir, "ref_driver.cpp"), ref_script]):
-        subprocess.check_call(["sh", ref_script])
+    if _stale(ref_lib, [os.path.join(odir, "ref_driver.cpp"), ref_script]):
+        subprocess.check_call(["sh", ref_script])  # skips itself without the reference tree
     return os.path.join(odir, "liboracle.so")
 
 

@@ -379,34 +379,53 @@ __global__ void prg_make_counters(Blk *b, uint64_t nb, uint64_t off) {
   }
 }
 
-// Sparse encode: out = XOR_i rot(a, pos_i), one thread per output word.
+// Sparse encode: out = XOR_i rot(a, pos_i).  Grid: x over output words (256
+// consecutive words per CTA, so the reads of `a` coalesce), y over chunks of
+// kSparseChunk positions staged in shared memory; each thread XORs its
+// chunk's partial into out (zeroed by the caller) with one 64-bit atomic.
 // r2 (rate-1/2 noise of 2n positions): positions p < n contribute x^p
 // itself, positions p in [n, 2n) contribute rot(a, p - n).
-__global__ void qc_sparse(const uint64_t *__restrict__ a, const uint64_t *__restrict__ pos,
-                          int weight, uint64_t n, uint64_t *__restrict__ out, int r2) {
+constexpr int kSparseChunk = 256;
+__global__ void __launch_bounds__(256) qc_sparse(const uint64_t *__restrict__ a, const uint64_t *__restrict__ pos,
+                                                 int weight, uint64_t n, uint64_t *__restrict__ out, int r2) {
+  __shared__ uint64_t sp[kSparseChunk];
   const uint64_t nw = n / 64;
-  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nw;
-       w += uint64_t(gridDim.x) * blockDim.x) {
-    uint64_t acc = 0;
-    for (int i = 0; i < weight; i++) {
-      uint64_t p = __ldg(&pos[i]);
-      if (r2) {
-        if (p < n) {
-          if ((p >> 6) == w) acc ^= 1ull << (p & 63);
-          continue;
-        }
-        p -= n;
+  const int i0 = blockIdx.y * kSparseChunk;
+  const int cnt = min(kSparseChunk, weight - i0);
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) sp[i] = __ldg(&pos[i0 + i]);
+  __syncthreads();
+  const uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (w >= nw) return;
+  uint64_t acc = 0;
+#pragma unroll 4
+  for (int i = 0; i < cnt; i++) {
+    uint64_t p = sp[i];
+    if (r2) {
+      if (p < n) {
+        if ((p >> 6) == w) acc ^= 1ull << (p & 63);
+        continue;
       }
-      if (p >= n) continue;
-      const uint64_t ws = p >> 6, bs = p & 63;
-      // bit (64w + b) of rot(a, p) = bit (64w + b - p) mod n of a
-      const uint64_t src = (w + nw - ws) % nw;
-      uint64_t v = __ldg(&a[src]) << bs;
-      if (bs) v |= __ldg(&a[(src + nw - 1) % nw]) >> (64 - bs);
-      acc ^= v;
+      p -= n;
     }
-    out[w] = acc;
+    if (p >= n) continue;
+    const uint64_t ws = p >> 6, bs = p & 63;
+    // bit (64w + b) of rot(a, p) = bit (64w + b - p) mod n of a
+    const uint64_t src = w >= ws ? w - ws : w + nw - ws;
+    uint64_t v = __ldg(&a[src]) << bs;
+    if (bs) v |= __ldg(&a[src ? src - 1 : nw - 1]) >> (64 - bs);
+    acc ^= v;
   }
+  if (acc) atomicXor(reinterpret_cast<unsigned long long *>(out + w), (unsigned long long)acc);
+}
+
+static int launch_sparse(const uint64_t *a_d, const uint64_t *pos_d, int weight, uint64_t n, uint64_t *out_d,
+                         int r2, cudaStream_t st) {
+  if (cudaMemsetAsync(out_d, 0, n / 8, st) != cudaSuccess) return launch_status(0);
+  if (weight == 0) return launch_status(0);
+  const uint64_t nw = n / 64;
+  const dim3 grid(unsigned((nw + 255) / 256), unsigned((weight + kSparseChunk - 1) / kSparseChunk));
+  qc_sparse<<<grid, 256, 0, st>>>(a_d, pos_d, weight, n, out_d, r2);
+  return launch_status();
 }
 
 // ---------------------------------------------------------------------------
@@ -853,9 +872,9 @@ int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *po
   if (!ctx || !a_d || !out_d || (weight > 0 && !pos_d) || weight < 0)
     return fail(CUOT_EINVAL, "bad argument");
   if (n == 0 || n % 64) return fail(CUOT_EINVAL, "n must be a positive multiple of 64");
+  if (weight > (1 << 24)) return fail(CUOT_EINVAL, "weight %d above 2^24", weight);
   DeviceGuard g(ctx);
-  qc_sparse<<<1024, 256, 0, static_cast<cudaStream_t>(stream)>>>(a_d, pos_d, weight, n, out_d, 0);
-  return launch_status();
+  return launch_sparse(a_d, pos_d, weight, n, out_d, 0, static_cast<cudaStream_t>(stream));
 }
 
 int cuot_qc_encode_sparse_r2(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *pos_d, int weight,
@@ -863,9 +882,9 @@ int cuot_qc_encode_sparse_r2(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t 
   if (!ctx || !a_d || !out_d || (weight > 0 && !pos_d) || weight < 0)
     return fail(CUOT_EINVAL, "bad argument");
   if (n == 0 || n % 64) return fail(CUOT_EINVAL, "n must be a positive multiple of 64");
+  if (weight > (1 << 24)) return fail(CUOT_EINVAL, "weight %d above 2^24", weight);
   DeviceGuard g(ctx);
-  qc_sparse<<<1024, 256, 0, static_cast<cudaStream_t>(stream)>>>(a_d, pos_d, weight, n, out_d, 1);
-  return launch_status();
+  return launch_sparse(a_d, pos_d, weight, n, out_d, 1, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

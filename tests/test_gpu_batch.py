@@ -56,7 +56,7 @@ def test_mixed_batch_equals_plain_and_oracle(ctx):
 
 
 def test_configs3_shaped_mix_is_a_cot_everywhere(ctx):
-    """A smaller configs[3]-shaped mix (log2 n in [12, 16]); every instance's
+    """A smaller mix shaped like the 64-instance batch (log2 n in [12, 16]); every instance's
     outputs satisfy the COT correlation against its own delta."""
     insts = mixed_workload(ctx, count=10, seed=7, lo=12, hi=16)
     stream = torch.cuda.Stream()
