@@ -22,6 +22,9 @@ Workloads (--workload):
               t = 1280 trees of depth 13, k = 452,000, d = 10 (both roles:
               MPCOT + primal LPN).
   ferret_c1   plain Ferret small: t = 64, h = 10, k = 8192.
+  ferret_rcot FerretCOT's extension loop at ferret_b13 parameters (cuot_b200.ferret):
+              one extension per step, pre-COTs carried over on the device,
+              usable COTs (ot_limit per extension) per second.
 
 Multi-GPU: one process per GPU (torchrun), each rank runs its own instance
 (the path shards by independent instances; no data-path collective):
@@ -54,6 +57,7 @@ WORKLOADS = {
     "sot_n20_r2": dict(kind="sot", t=512, h=12, r2=True),
     "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
     "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
+    "ferret_rcot": dict(kind="session", t=1280, h=13, k=452000, d=10),
 }
 CONFIG_TEXT = {
     "mixed64": "batched mix: 64 instances (32 SOT, 32 Ferret-style), log2 n uniform in [16,22], depth 10-14, "
@@ -65,6 +69,9 @@ CONFIG_TEXT = {
                   "out = e0 ^ a*e1 exact on 128 planes, transposes (both roles)",
     "ferret_b13": "plain Ferret ferret_b13: n=10485760, t=1280, h=13, k=452000, d=10 (both roles)",
     "ferret_c1": "plain Ferret small: n=65536, t=64, h=10, k=8192, d=10 (both roles)",
+    "ferret_rcot": "Ferret rcot session at ferret_b13 parameters: one extension per step (both roles), its M = "
+                   "k + t*h + 128 pre-COTs carried over on the device; value counts the ot_limit = 10,016,992 "
+                   "usable COTs per extension",
 }
 
 
@@ -416,6 +423,11 @@ def run_reference(args):
             v2, s2 = cpu_sample("ferret_b13", threads, budget_s=2.0)
             v = (n_sot + n_fer) / (n_sot / v1 + n_fer / v2)
             sample = f"SOT: {s1}; Ferret: {s2}; weighted by the mix's COTs"
+        elif spec["kind"] == "session":
+            v, sample = cpu_sample("ferret_b13", threads, budget_s=5.0)
+            v *= (spec["t"] << spec["h"]) - (spec["k"] + spec["t"] * spec["h"] + 128)
+            v /= spec["t"] << spec["h"]
+            sample += "; usable COTs (ot_limit / n of the outputs)"
         else:
             v, sample = cpu_sample(name, threads, budget_s=5.0)
         if i >= args.warmup:
@@ -658,12 +670,114 @@ def run_served(args, device: int) -> dict:
                     "of the continuous-batching server"}
 
 
+def run_session(args):
+    """Ferret extension loop (FerretSession.extend_f2k) at ferret_b13
+    parameters; one replica per rank."""
+    import torch
+    import cuot_b200
+    from cuot_b200.ferret import FERRET_B13, FerretSession
+    from cuot_b200.pipeline import HostPipeline
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    p = FERRET_B13
+    st = torch.cuda.Stream()
+    ctx = cuot_b200.Context(local)
+    sess = FerretSession(ctx, ctx, p, seed=b"bench-session-%d" % rank, stream=st)
+    for _ in range(args.warmup):
+        sess.extend_f2k()
+    st.synchronize()
+    before = cuot_b200.launch_count()
+    sess.extend_f2k()
+    st.synchronize()
+    launches = cuot_b200.launch_count() - before
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clk = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    time.sleep(0.3)
+    for i in range(args.steps):
+        with torch.cuda.stream(st):
+            flush.zero_()
+        evs[i][0].record(st)
+        sess.extend_f2k()
+        evs[i][1].record(st)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    # e2e: every extension's usable COTs of both roles returned to pinned host
+    # memory, overlapped with the next extension (the extension's inputs are
+    # the previous extension's outputs, resident on the device)
+    hv = torch.empty((p.ot_limit, 16), dtype=torch.uint8).pin_memory()
+    hw = torch.empty((p.ot_limit, 16), dtype=torch.uint8).pin_memory()
+    pipe = HostPipeline([sess.ot_s[:p.ot_limit], sess.ot_r[:p.ot_limit]], stream=st)
+    pipe.step([], lambda s: sess.extend_f2k(), [hv, hw])
+    pipe.join()
+    st.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(args.steps):
+        h2d, d2h = pipe.step([], lambda s: sess.extend_f2k(), [hv, hw])
+    pipe.join()
+    b.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / args.steps
+    if dist:
+        tt = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = tt.tolist()
+    peaks, peak_kind = measured_peaks()
+    alg = 2 * (32 * p.n + 16 * p.k) + 2 * (16 * p.n + 32 * p.t * p.h)  # LPN + PPRF, both roles
+    achieved = alg / (ms / 1e3) / 1e9
+    out = {
+        "metric": metric_name(args.workload), "value": world * p.ot_limit / (ms / 1e3), "unit": "COTs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "usable_cots_per_step_per_gpu":
+                   p.ot_limit, "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed steps (L2 flush)"},
+        "roofline": {"bound": "hbm", "kernel": "extension (PPRF + LPN, both roles)", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": None, "algorithmic_bytes_per_step": alg,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "e2e": {"value": world * p.ot_limit / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sample = cpu_sample("ferret_b13", threads)
+        out["cpu_baseline"] = {"value": v * p.ot_limit / p.n, "unit": "COTs/s", "cores": threads, "kind": "port",
+                               "sample": sample + "; scaled by ot_limit / n"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del sess
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
     import cuot_b200
 
     if WORKLOADS[args.workload]["kind"] == "batch":
         return run_batch(args)
+    if WORKLOADS[args.workload]["kind"] == "session":
+        return run_session(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

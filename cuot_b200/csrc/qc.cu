@@ -139,6 +139,24 @@ __device__ __forceinline__ void bf_dit_lazy(uint32_t &u, uint32_t &v, uint2 w) {
 // `rows` rows, everything but the row count known at compile time.
 // ah (optional, the last DIF pass only): after its stages, element `pos` of
 // row `row` is multiplied by ah[row * 2^LG + pos] (the pointwise product).
+// Group order within a row for a pass with S_LO < 5: a warp then spans
+// 2^(5 - S_LO) values t of the group bits above S_LO, whose bases differ by
+// multiples of 2^(S_LO + K) and (through the padding) by 3 * 2^(S_LO+K-5)
+// words per step of t.  Consecutive t would put two lanes on one bank; taking
+// t in steps of 2^(5 - K) (a rotation of its low bits, a bijection) spreads
+// the lanes over all 32 banks.  Conflict-free for every pass of LG >= 10.
+template <int LG, int K, int S_LO>
+__device__ __forceinline__ int group_hi(int t) {
+  constexpr int H = LG - K - S_LO, A = 5 - S_LO, SB = 5 - K;
+  if constexpr (S_LO < 5 && S_LO + K >= 5 && SB > 0 && A > 0 && A + SB <= H) {
+    constexpr int LB = A + SB, M = (1 << LB) - 1;
+    const int low = t & M;
+    return (t & ~M) | (((low << SB) | (low >> A)) & M);
+  } else {
+    return t;
+  }
+}
+
 template <int LG, int K, int S_LO, bool DIF>
 __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const uint2 *tw,
                                          const uint2 *__restrict__ ah = nullptr) {
@@ -148,7 +166,7 @@ __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const ui
   for (int w = threadIdx.x; w < (rows << NGR_LG); w += blockDim.x) {
     const int row = w >> NGR_LG, g = w & ((1 << NGR_LG) - 1);
     const int glo = g & LOWMASK;
-    const int base = glo | ((g >> S_LO) << (S_LO + K));
+    const int base = glo | (group_hi<LG, K, S_LO>(g >> S_LO) << (S_LO + K));
     uint32_t *xr = x + row * ld + swz(base);
     const uint2 *twg = tw + glo;
     uint32_t v[R];
