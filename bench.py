@@ -21,6 +21,8 @@ Workloads (--workload):
   ferret_b13  plain Ferret at full size (ferret_b13): n = 10,485,760,
               t = 1280 trees of depth 13, k = 452,000, d = 10 (both roles:
               MPCOT + primal LPN).
+  ferret_b13_mal  ferret_b13 plus the per-tree GF(2^128) check values of the
+              malicious consistency check on both roles (stage "chi").
   ferret_c1   plain Ferret small: t = 64, h = 10, k = 8192.
   ferret_rcot FerretCOT's extension loop at ferret_b13 parameters (cuot_b200.ferret):
               one extension per step, pre-COTs carried over on the device,
@@ -56,6 +58,7 @@ WORKLOADS = {
     "sot_n20": dict(kind="sot", t=256, h=12),
     "sot_n20_r2": dict(kind="sot", t=512, h=12, r2=True),
     "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
+    "ferret_b13_mal": dict(kind="ferret", t=1280, h=13, k=452000, d=10, mal=True),
     "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
     "ferret_rcot": dict(kind="session", t=1280, h=13, k=452000, d=10),
 }
@@ -68,6 +71,8 @@ CONFIG_TEXT = {
     "sot_n20_r2": "plain SOT rate-1/2, n=2^20 outputs: 512 GGM trees depth 12 (2n noise blocks), "
                   "out = e0 ^ a*e1 exact on 128 planes, transposes (both roles)",
     "ferret_b13": "plain Ferret ferret_b13: n=10485760, t=1280, h=13, k=452000, d=10 (both roles)",
+    "ferret_b13_mal": "ferret_b13 plus the malicious consistency check's per-tree GF(2^128) sums of both roles "
+                      "(seeds given; their SHA-256 derivation is host protocol)",
     "ferret_c1": "plain Ferret small: n=65536, t=64, h=10, k=8192, d=10 (both roles)",
     "ferret_rcot": "Ferret rcot session at ferret_b13 parameters: one extension per step (both roles), its M = "
                    "k + t*h + 128 pre-COTs carried over on the device; value counts the ot_limit = 10,016,992 "
@@ -172,6 +177,7 @@ class Instance:
         self.d_roots = dev(self.roots)
         self.d_choice = dev(self.choice)
         self.leaves_s, self.leaves_r = emp(self.nleaves), emp(self.nleaves)
+        self.mal = False
         if s["kind"] == "ferret":
             k = s["k"]
             self.k, self.d = k, s["d"]
@@ -181,6 +187,10 @@ class Instance:
             self.lsum, self.rsum, self.ss = emp(t * h), emp(t * h), emp(t)
             self.mc = emp(t * h)
             self.seed = blk(1)[0]
+            self.mal = bool(s.get("mal"))
+            if self.mal:
+                self.d_chiseed = dev(blk(t))
+                self.chi_v, self.chi_w = emp(t), emp(t)
         else:
             self.base0, self.base1 = blk(h * t), blk(h * t)
             self.d_b0, self.d_b1 = dev(self.base0), dev(self.base1)
@@ -211,6 +221,10 @@ class Instance:
             torch.where(self.d_choice.view(-1, 1).bool(), self.rsum, self.lsum, out=self.mc)
             self.rctx.ferret_pprf_recver(self.mc, self.d_choice, self.ss, h, self.leaves_r)
             mark("pprf1")
+            if self.mal:
+                self.sctx.ferret_chi_sum(self.leaves_s, h, self.d_chiseed, self.chi_v)
+                self.rctx.ferret_chi_sum(self.leaves_r, h, self.d_chiseed, self.chi_w)
+            mark("chi1")
             self.sctx.lpn_primal(self.seed, self.d_kk_s, self.leaves_s, d=self.d)
             self.rctx.lpn_primal(self.seed, self.d_kk_r, self.leaves_r, d=self.d)
             mark("lpn1")
@@ -221,6 +235,7 @@ class Instance:
                                       self.m0, self.m1)
             self.rctx.sot_pprf_recver(self.m0, self.m1, self.d_mc, self.d_choice, t, h, self.leaves_r)
             mark("pprf1")
+            mark("chi1")
             if self.r2:
                 self.plan_s.dual_lpn_r2(self.leaves_s, self.leaves_s[:n])
                 self.plan_r.dual_lpn_r2(self.leaves_r, self.leaves_r[:n])
@@ -307,6 +322,9 @@ def e2e_compute(inst: Instance, host, stream) -> int:
                 d2h += host[k].numel()
             torch.where(inst.d_choice.view(-1, 1).bool(), inst.rsum, inst.lsum, out=inst.mc)
             inst.rctx.ferret_pprf_recver(inst.mc, inst.d_choice, inst.ss, inst.h, inst.leaves_r, stream=stream)
+            if inst.mal:
+                inst.sctx.ferret_chi_sum(inst.leaves_s, inst.h, inst.d_chiseed, inst.chi_v, stream=stream)
+                inst.rctx.ferret_chi_sum(inst.leaves_r, inst.h, inst.d_chiseed, inst.chi_w, stream=stream)
             inst.sctx.lpn_primal(inst.seed, inst.d_kk_s, inst.leaves_s, d=inst.d, stream=stream)
             inst.rctx.lpn_primal(inst.seed, inst.d_kk_r, inst.leaves_r, d=inst.d, stream=stream)
         else:
@@ -799,7 +817,7 @@ def run_ours(args):
 
     # L2 flush buffer (larger than the 126 MB L2), written between steps
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    names = ["pprf0", "pprf1", "lpn1"]
+    names = ["pprf0", "pprf1", "chi1", "lpn1"]
     step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     stage_ev = [{k: torch.cuda.Event(enable_timing=True) for k in names} for _ in range(args.steps)]
     clk = ClockSampler(local)
@@ -820,11 +838,12 @@ def run_ours(args):
     ms_steps = [a.elapsed_time(b) for a, b in step_ev]
     ms = sum(ms_steps) / len(ms_steps)
     pprf_ms = statistics.mean(e["pprf0"].elapsed_time(e["pprf1"]) for e in stage_ev)
-    lpn_ms = statistics.mean(e["pprf1"].elapsed_time(e["lpn1"]) for e in stage_ev)
+    chi_ms = statistics.mean(e["pprf1"].elapsed_time(e["chi1"]) for e in stage_ev)
+    lpn_ms = statistics.mean(e["chi1"].elapsed_time(e["lpn1"]) for e in stage_ev)
     if dist:
-        tt = torch.tensor([ms, pprf_ms, lpn_ms], device="cuda", dtype=torch.float64)
+        tt = torch.tensor([ms, pprf_ms, chi_ms, lpn_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, pprf_ms, lpn_ms = tt.tolist()
+        ms, pprf_ms, chi_ms, lpn_ms = tt.tolist()
     value = world * n / (ms / 1e3)
 
     # e2e through the public API with pinned host buffers: every step's inputs
@@ -872,6 +891,8 @@ def run_ours(args):
         lpn_bytes = 2 * (32 * n + 16 * k)
         pprf_bytes = 2 * (16 * n + 32 * inst.t * inst.h)
         stages = {"pprf": (pprf_ms, pprf_bytes), "lpn": (lpn_ms, lpn_bytes)}
+        if inst.mal:
+            stages["chi"] = (chi_ms, 2 * 16 * n)  # both roles read their n leaves
     else:
         # dual LPN per role: two transposes (32 B per block each way) + encode
         # planes in/out (32n); rate-1/2: 2n blocks in (64n), e0 XOR (48n), n out (32n)

@@ -138,6 +138,12 @@ class Context:
         return out
 
     # ---- Ferret ------------------------------------------------------------
+    def ferret_chi_sum(self, leaves, h: int, seeds, out, stream=None):
+        """Per-tree GF(2^128) check values sum_i seed^(i+1) * leaf_i."""
+        t = _nblocks(seeds)
+        _check(self.lib.cuot_ferret_chi_sum(self.h, _ptr(leaves), C.c_uint64(t), C.c_int(h), _ptr(seeds),
+                                            _ptr(out), _stream(stream)), "cuot_ferret_chi_sum")
+
     def ferret_pprf_sender(self, roots, h: int, delta, leaves, lsum, rsum, secret_sum, stream=None):
         t = _nblocks(roots)
         _check(self.lib.cuot_ferret_pprf_sender(self.h, _ptr(roots), C.c_uint64(t), C.c_int(h),

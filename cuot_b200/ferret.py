@@ -87,6 +87,14 @@ def session_delta(seed: bytes) -> bytes:
     return bytes(d)
 
 
+def chi_seeds(secret_sums) -> bytes:
+    """Seeds of the per-tree consistency check: the first 16 bytes of
+    SHA-256 over each tree's 16-byte secret sum (Hash::hash_once in
+    spcot_sender.h:91-94), concatenated."""
+    raw = bytes(secret_sums)
+    return b"".join(hashlib.sha256(raw[i:i + 16]).digest()[:16] for i in range(0, len(raw), 16))
+
+
 class FerretSession:
     """Both roles of a Ferret random-COT generator on one GPU.
 

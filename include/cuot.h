@@ -168,6 +168,19 @@ int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
                        uint64_t row_bytes, uint64_t col_lo, uint64_t col_hi,
                        void *out_d, void *stream);
 
+/* ---- Ferret malicious consistency check ------------------------------------
+ * out_d[j] = sum_{i < 2^h} seed_j^(i+1) * leaves[j*2^h + i] over GF(2^128)
+ * (natural bit order, mod x^128 + x^7 + x^2 + x + 1), for every tree j < t:
+ * the per-tree check values of SPCOT_Sender/SPCOT_Recver::
+ * consistency_check_msg_gen (spcot_sender.h:88-98, spcot_recver.h:97-107),
+ * all trees in one launch.  seeds_d[j] = the first 16 bytes of
+ * Hash(secret_sum_j) (host side, as the reference derives it).  The sender
+ * passes its leaves (V_j), the receiver its leaves (W_j); then
+ * V_j ^ W_j = seed_j^(alpha_j + 1) * Delta for the punctured leaf alpha_j. */
+int cuot_ferret_chi_sum(cuot_ctx *ctx, const cuot_block *leaves_d, uint64_t t,
+                        int h, const cuot_block *seeds_d, cuot_block *out_d,
+                        void *stream);
+
 /* ---- SOT quasi-cyclic dual LPN ------------------------------------------------
  * a = n bits of AES_key(make_block counters) (silent/quasi_cyclic.cu:57-66,
  * gpu/gpu_ops.cu:102-109).  encode: every plane r (n bits, planes

@@ -197,3 +197,23 @@ def ref_prng(seed, nblocks: int):
     out = np.empty((nblocks, 16), np.uint8)
     r.ref_prng(_p(_u8(seed)), _p(out), C.c_ulonglong(nblocks))
     return out
+
+
+def gf128_mul(a, b) -> np.ndarray:
+    """GF(2^128) product of 16-byte blocks (natural bit order, mod x^128 +
+    x^7 + x^2 + x + 1)."""
+    a = np.ascontiguousarray(a, np.uint8).reshape(16)
+    b = np.ascontiguousarray(b, np.uint8).reshape(16)
+    out = np.empty(16, np.uint8)
+    lib().or_gf128_mul(_p(a), _p(b), _p(out))
+    return out
+
+
+def ferret_chi_sum(leaves, h: int, seeds, threads: int = 1) -> np.ndarray:
+    """Per-tree sum_i seed^(i+1) * leaf_i over GF(2^128)."""
+    seeds = np.ascontiguousarray(seeds, np.uint8).reshape(-1, 16)
+    t = seeds.shape[0]
+    leaves = np.ascontiguousarray(leaves, np.uint8).reshape(t << h, 16)
+    out = np.empty((t, 16), np.uint8)
+    lib().or_ferret_chi_sum(_p(leaves), I64(t), INT(h), _p(seeds), _p(out), INT(threads))
+    return out

@@ -684,3 +684,59 @@ void or_sot_pprf_recver(const or_block *m0, const or_block *m1,
   srecv_ctx c = {m0, m1, mc, choice, t, h, leaves};
   parallel_for(t, threads, 1, srecv_range, &c);
 }
+
+/* ======================================================================== */
+/* GF(2^128) (emp-tool gfmul semantics: natural bit order, reduction        */
+/* polynomial x^128 + x^7 + x^2 + x + 1) and the per-tree chi sums of the   */
+/* malicious consistency check (spcot_sender.h:88-98, spcot_recver.h:97-107).*/
+/* ======================================================================== */
+void or_gf128_mul(const or_block *a, const or_block *b, or_block *out) {
+  uint64_t r[4] = {0, 0, 0, 0}, lo, hi;
+  clmul64(a->lo, b->lo, &lo, &hi); r[0] ^= lo; r[1] ^= hi;
+  clmul64(a->lo, b->hi, &lo, &hi); r[1] ^= lo; r[2] ^= hi;
+  clmul64(a->hi, b->lo, &lo, &hi); r[1] ^= lo; r[2] ^= hi;
+  clmul64(a->hi, b->hi, &lo, &hi); r[2] ^= lo; r[3] ^= hi;
+  /* fold x^128 * (r2 + r3 x^64) with x^128 = x^7 + x^2 + x + 1, twice */
+  for (int pass = 0; pass < 2; pass++) {
+    uint64_t h0 = r[2], h1 = r[3];
+    r[2] = r[3] = 0;
+    /* (h0 + h1 x^64) * (1 + x + x^2 + x^7) */
+    const int sh[4] = {0, 1, 2, 7};
+    for (int k = 0; k < 4; k++) {
+      int s = sh[k];
+      r[0] ^= h0 << s;
+      r[1] ^= (h1 << s) | (s ? h0 >> (64 - s) : 0);
+      r[2] ^= s ? h1 >> (64 - s) : 0;
+    }
+  }
+  out->lo = r[0];
+  out->hi = r[1];
+}
+
+typedef struct {
+  const or_block *leaves;
+  const or_block *seeds;
+  or_block *out;
+  int h;
+} chi_ctx;
+
+static void chi_range(void *p, int64_t lo, int64_t hi) {
+  chi_ctx *c = (chi_ctx *)p;
+  const int64_t L = (int64_t)1 << c->h;
+  for (int64_t j = lo; j < hi; j++) {
+    or_block chi = c->seeds[j], acc = {0, 0}, prod;
+    for (int64_t i = 0; i < L; i++) {
+      or_gf128_mul(&chi, &c->leaves[j * L + i], &prod);
+      acc.lo ^= prod.lo;
+      acc.hi ^= prod.hi;
+      or_gf128_mul(&chi, &c->seeds[j], &chi);
+    }
+    c->out[j] = acc;
+  }
+}
+
+void or_ferret_chi_sum(const or_block *leaves, int64_t t, int h,
+                       const or_block *seeds, or_block *out, int threads) {
+  chi_ctx c = {leaves, seeds, out, h};
+  parallel_for(t, threads, 1, chi_range, &c);
+}

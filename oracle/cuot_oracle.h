@@ -75,6 +75,18 @@ void or_sot_pprf_recver(const or_block *m0, const or_block *m1,
                         const or_block *mc, const uint8_t *choice, int64_t t,
                         int h, or_block *leaves, int threads);
 
+/* ---- Ferret malicious consistency check: per-tree chi sums -------------- */
+/* GF(2^128) with the natural bit order (bit i of the little-endian block is
+ * the coefficient of x^i), reduced mod x^128 + x^7 + x^2 + x + 1: emp-tool's
+ * gfmul (emp-tool/utils/f2k.h @ 44b1dde, not vendored). */
+void or_gf128_mul(const or_block *a, const or_block *b, or_block *out);
+/* out[j] = sum_{i < 2^h} seed_j^(i+1) * leaves[j*2^h + i]: emp-tool's
+ * uni_hash_coeff_gen (chi_i = seed^(i+1)) followed by
+ * vector_inn_prdt_sum_red, as spcot_sender.h:88-98 / spcot_recver.h:97-107
+ * use them on one tree (seed = the first half of Hash(secret_sum)). */
+void or_ferret_chi_sum(const or_block *leaves, int64_t t, int h,
+                       const or_block *seeds, or_block *out, int threads);
+
 #ifdef __cplusplus
 }
 #endif
