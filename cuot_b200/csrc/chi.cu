@@ -17,7 +17,8 @@
 // Multiplication by the fixed u uses byte tables in shared memory: T[k][b] =
 // u * (b x^(8k)), so u * x = XOR_k T[k][byte k of x] -- 16 conflict-light
 // 128-bit lookups per leaf instead of a 128 x 128 carry-less product.  The
-// few general products (tree levels, squarings) are bit-serial.
+// squarings s^(2^l) spread bits (squaring is linear in characteristic 2);
+// the few general products (tree levels) are bit-serial.
 #include "ctx.cuh"
 
 namespace cuot {
@@ -42,17 +43,45 @@ __device__ __forceinline__ U128 mulx(U128 a) {
   const uint64_t c = a.hi >> 63;
   return U128{(a.lo << 1) ^ (c * 0x87ull), (a.hi << 1) | (a.lo >> 63)};
 }
-// general product, bit-serial from the top bit of a (Horner in x)
+// general product: r = XOR_i a_i (b x^i), with b x^i advanced by one mulx per
+// bit, so the dependency chain is the short mulx and the accumulation
+// pipelines behind it
 __device__ U128 gmul(U128 a, U128 b) {
-  U128 r{0, 0};
-  for (int i = 127; i >= 0; i--) {
-    r = mulx(r);
-    const uint64_t bit = (i >= 64 ? a.hi >> (i - 64) : a.lo >> i) & 1;
-    const uint64_t m = 0 - bit;
-    r.lo ^= b.lo & m;
-    r.hi ^= b.hi & m;
+  U128 r{0, 0}, bx = b;
+#pragma unroll 8
+  for (int i = 0; i < 128; i++) {
+    const uint64_t m = 0 - ((i < 64 ? a.lo >> i : a.hi >> (i - 64)) & 1);
+    r.lo ^= bx.lo & m;
+    r.hi ^= bx.hi & m;
+    bx = mulx(bx);
   }
   return r;
+}
+// bits i -> 2i of a 32-bit word
+__device__ __forceinline__ uint64_t spread32(uint32_t x) {
+  uint64_t v = x;
+  v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+  v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+  v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  v = (v | (v << 2)) & 0x3333333333333333ull;
+  v = (v | (v << 1)) & 0x5555555555555555ull;
+  return v;
+}
+// a^2: squaring is GF(2)-linear (bit i -> bit 2i), then the high 128 bits
+// are folded with x^128 = x^7 + x^2 + x + 1 (twice: the first fold spills
+// at most 7 bits)
+__device__ U128 gsqr(U128 a) {
+  uint64_t r0 = spread32(uint32_t(a.lo)), r1 = spread32(uint32_t(a.lo >> 32));
+  uint64_t r2 = spread32(uint32_t(a.hi)), r3 = spread32(uint32_t(a.hi >> 32));
+#pragma unroll
+  for (int pass = 0; pass < 2; pass++) {
+    const uint64_t h0 = r2, h1 = r3;
+    r2 = r3 = 0;
+    r0 ^= h0 ^ (h0 << 1) ^ (h0 << 2) ^ (h0 << 7);
+    r1 ^= h1 ^ (h1 << 1) ^ (h1 << 2) ^ (h1 << 7) ^ (h0 >> 63) ^ (h0 >> 62) ^ (h0 >> 57);
+    r2 ^= (h1 >> 63) ^ (h1 >> 62) ^ (h1 >> 57);
+  }
+  return U128{r0, r1};
 }
 
 // u * x with the byte tables T (16 x 256 entries)
@@ -80,7 +109,7 @@ __global__ void __launch_bounds__(kChiThreads) chi_sum_kernel(const uint4 *__res
     U128 c = s;
     spow[0] = to_u4(c);
     for (int l = 1; l <= 8; l++) {
-      c = gmul(c, c);
+      c = gsqr(c);
       spow[l] = to_u4(c);
     }
     U128 b = c;  // u * x^0

@@ -47,7 +47,25 @@ constexpr uint32_t kG = 3u;
 #ifndef CUOT_QC_ROW_ELEMS
 #define CUOT_QC_ROW_ELEMS 8192
 #endif
+#ifndef CUOT_QC_THREADS_L11
+#define CUOT_QC_THREADS_L11 256
+#endif
+#ifndef CUOT_QC_THREADS_L12
+#define CUOT_QC_THREADS_L12 512
+#endif
 constexpr int kQcThreads = CUOT_QC_THREADS;
+// Threads per CTA of a pass over 2^LG-point transforms: the 2048- and
+// 4096-point passes hold 2-4x the shared memory per CTA, so fewer CTAs fit
+// an SM; bigger CTAs keep the same threads per SM.  Registers stay at
+// 64 per thread (threads x CTAs per SM = 1024).
+template <int LG>
+constexpr int qc_threads() {
+  return LG >= 12 ? CUOT_QC_THREADS_L12 : LG >= 11 ? CUOT_QC_THREADS_L11 : kQcThreads;
+}
+template <int LG>
+constexpr int qc_min_blocks() {
+  return (kQcThreads * CUOT_QC_MIN_BLOCKS) / qc_threads<LG>() > 0 ? (kQcThreads * CUOT_QC_MIN_BLOCKS) / qc_threads<LG>() : 1;
+}
 constexpr int kQcColUnroll = CUOT_QC_COL_UNROLL;
 constexpr int kCW = 8;  // columns per CTA in the column passes
 
@@ -239,7 +257,7 @@ __device__ __forceinline__ void stage_tw(uint2 *dst, const uint2 *src, int cnt) 
 // Pass A.  bits: plane-major, plane_words 32-bit words per plane.
 // grid (N2 / kCW, nplanes_batch).  Y: [plane][N1][N2].
 template <int E1>
-__global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_col_fwd(
+__global__ void __launch_bounds__(qc_threads<E1>(), qc_min_blocks<E1>()) qc_col_fwd(
     const uint32_t *__restrict__ bits, uint64_t plane_words, int e2,
     const uint2 *__restrict__ tw1f, const uint2 *__restrict__ fsf, uint32_t *__restrict__ Y) {
   extern __shared__ uint32_t xs[];
@@ -274,7 +292,7 @@ __global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_col_fwd(
 // build ahat).  Plane y of the launch uses ahat.p[(ahat.first + y) / ahat.per]
 // (planes of several encodes, each with its own `a`, can share a launch).
 template <int E2>
-__global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_row(
+__global__ void __launch_bounds__(qc_threads<E2>(), qc_min_blocks<E2>()) qc_row(
     uint32_t *__restrict__ Y, int e1, int rows_per_cta,
     const uint2 *__restrict__ tw2f, const uint2 *__restrict__ tw2i,
     AhatTab ahat_tab, int mode) {
@@ -317,7 +335,7 @@ __global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_row(
 // Pass C.  grid (N2 / kCW, nplanes_batch).  out: plane-major bits, written
 // (accumulate == 0) or XORed into (accumulate == 1; the rate-1/2 form).
 template <int E1>
-__global__ void __launch_bounds__(kQcThreads, CUOT_QC_MIN_BLOCKS) qc_col_inv(
+__global__ void __launch_bounds__(qc_threads<E1>(), qc_min_blocks<E1>()) qc_col_inv(
     const uint32_t *__restrict__ Y, int e2, const uint2 *__restrict__ fsi,
     const uint2 *__restrict__ tw1i, uint8_t *__restrict__ out, uint64_t plane_bytes, int accumulate) {
   extern __shared__ uint32_t xs[];
@@ -523,9 +541,12 @@ static int col_smem(const QcTables *t) {
   const int ld = padded_len(1 << t->e1);
   return (kCW * ld + 1) * 4 + (1 << t->e1) * 8;
 }
+static int qc_threads_rt(int lg) {
+  return lg >= 12 ? CUOT_QC_THREADS_L12 : lg >= 11 ? CUOT_QC_THREADS_L11 : kQcThreads;
+}
 static int row_rows(const QcTables *t) {
   const int N2 = 1 << t->e2;
-  int r = CUOT_QC_ROW_ELEMS / N2;
+  int r = int(int64_t(CUOT_QC_ROW_ELEMS) * qc_threads_rt(t->e2) / kQcThreads / N2);
   if (r < 1) r = 1;
   if (r > (1 << t->e1)) r = 1 << t->e1;
   return r;
@@ -566,14 +587,14 @@ static int set_attrs(const QcTables *t) {
 static void launch_col_fwd(const QcTables *t, dim3 grid, cudaStream_t st, const uint32_t *bits,
                            uint64_t plane_words, uint32_t *Y) {
   switch (t->e1) {
-#define L1(E) case E: qc_col_fwd<E><<<grid, kQcThreads, col_smem(t), st>>>(bits, plane_words, t->e2, t->tw1f, t->fsf, Y); break;
+#define L1(E) case E: qc_col_fwd<E><<<grid, qc_threads<E>(), col_smem(t), st>>>(bits, plane_words, t->e2, t->tw1f, t->fsf, Y); break;
     CUOT_E1_CASES(L1)
 #undef L1
   }
 }
 static void launch_row(const QcTables *t, dim3 grid, cudaStream_t st, uint32_t *Y, const AhatTab &ahat, int mode) {
   switch (t->e2) {
-#define L2(E) case E: qc_row<E><<<grid, kQcThreads, row_smem(t), st>>>(Y, t->e1, row_rows(t), t->tw2f, t->tw2i, ahat, mode); break;
+#define L2(E) case E: qc_row<E><<<grid, qc_threads<E>(), row_smem(t), st>>>(Y, t->e1, row_rows(t), t->tw2f, t->tw2i, ahat, mode); break;
     CUOT_E2_CASES(L2)
 #undef L2
   }
@@ -581,7 +602,7 @@ static void launch_row(const QcTables *t, dim3 grid, cudaStream_t st, uint32_t *
 static void launch_col_inv(const QcTables *t, dim3 grid, cudaStream_t st, const uint32_t *Y, uint8_t *out,
                            uint64_t plane_bytes, int accumulate = 0) {
   switch (t->e1) {
-#define L3(E) case E: qc_col_inv<E><<<grid, kQcThreads, col_smem(t), st>>>(Y, t->e2, t->fsi, t->tw1i, out, plane_bytes, accumulate); break;
+#define L3(E) case E: qc_col_inv<E><<<grid, qc_threads<E>(), col_smem(t), st>>>(Y, t->e2, t->fsi, t->tw1i, out, plane_bytes, accumulate); break;
     CUOT_E1_CASES(L3)
 #undef L3
   }
