@@ -147,6 +147,23 @@ def test_transpose_vs_oracle(ctx, rows, rb, lo, hi):
     assert np.array_equal(to_host(out), exp)
 
 
+def test_transpose_past_2p23_rows(ctx):
+    """Rows beyond 2^23 (the reference's transposer indexes wrongly there):
+    2^23 + 64 blocks to planes and back, against the oracle's transpose and
+    round-tripped."""
+    rows = (1 << 23) + 64
+    rng = np.random.default_rng(24)
+    m = rng.integers(0, 256, (rows, 16), dtype=np.uint8)
+    planes = torch.empty(128 * rows // 8, dtype=torch.uint8, device="cuda")
+    dm = to_dev(m)
+    ctx.bit_transpose(dm, rows, 16, 0, 128, planes)
+    exp = oracle.bit_transpose(m, rows, 16, 0, 128)
+    assert np.array_equal(to_host(planes), exp.reshape(-1))
+    back = torch.empty((rows, 16), dtype=torch.uint8, device="cuda")
+    ctx.bit_transpose(planes, 128, rows // 8, 0, rows, back)
+    assert torch.equal(back, dm)
+
+
 # ---------------------------------------------------------------- QC
 def test_qc_golden(ctx, golden):
     for c in golden["qc"]:
@@ -184,6 +201,22 @@ def test_qc_encode_vs_oracle(ctx, e, nplanes):
     d = to_dev(planes.view(np.int64))
     ctx.qc_encode(a, d, n, nplanes)
     exp = oracle.qc_encode(a_np, planes, n, threads=8)
+    assert np.array_equal(to_host(d).view(np.uint64), exp)
+
+
+@pytest.mark.parametrize("e", [21, 22, 24, 25])
+def test_qc_encode_large_sizes(ctx, e):
+    """The 2048/4096/8192-point pass kernels (n = 2^21 .. 2^25, the largest
+    size the row pass fits) against the oracle on two planes."""
+    n = 1 << e
+    rng = np.random.default_rng(e + 1000)
+    key = rng_blocks(rng, 1)[0]
+    a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
+    ctx.qc_gen_a(key, n, a)
+    planes = rng.integers(0, 2**63, (2, n // 64), dtype=np.uint64)
+    d = to_dev(planes.view(np.int64))
+    ctx.qc_encode(a, d, n, 2)
+    exp = oracle.qc_encode(to_host(a).view(np.uint64), planes, n, threads=16)
     assert np.array_equal(to_host(d).view(np.uint64), exp)
 
 
