@@ -47,6 +47,9 @@ constexpr uint32_t kG = 3u;
 #ifndef CUOT_QC_ROW_ELEMS
 #define CUOT_QC_ROW_ELEMS 8192
 #endif
+#ifndef CUOT_QC_ROWS_K3
+#define CUOT_QC_ROWS_K3 4
+#endif
 #ifndef CUOT_QC_PAIR_ROWS
 #define CUOT_QC_PAIR_ROWS 1
 #endif
@@ -273,7 +276,9 @@ __device__ __forceinline__ void ntt_pass_rows(uint32_t *x, int rows, int ld, con
 template <int LG, int K, int S_LO, bool DIF>
 __device__ __forceinline__ void ntt_pass(uint32_t *x, int rows, int ld, const uint2 *tw,
                                          const uint2 *__restrict__ ah = nullptr) {
-  if (CUOT_QC_PAIR_ROWS && LG >= 10 && (rows & 1) == 0)
+  if (CUOT_QC_PAIR_ROWS && LG >= 10 && K <= 3 && (rows & 3) == 0)
+    ntt_pass_rows<LG, K, S_LO, DIF, CUOT_QC_ROWS_K3>(x, rows, ld, tw, ah);
+  else if (CUOT_QC_PAIR_ROWS && LG >= 10 && (rows & 1) == 0)
     ntt_pass_rows<LG, K, S_LO, DIF, 2>(x, rows, ld, tw, ah);
   else
     ntt_pass_rows<LG, K, S_LO, DIF, 1>(x, rows, ld, tw, ah);
