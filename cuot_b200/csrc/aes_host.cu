@@ -65,4 +65,27 @@ void host_aes_key_expand(const uint8_t key[16], AesKey *out) {
   std::memcpy(out->rk, rk, 176);  // little-endian words
   for (int i = 0; i < 44; i++) out->rkr[i] = (out->rk[i] >> 8) | (out->rk[i] << 24);
 }
+
+// One block, FIPS-197 rounds over the T-table (column j of a round =
+// T0[row-0 byte of column j] ^ rotl8/16/24 of T0 of the row-1/2/3 bytes of
+// columns j+1, j+2, j+3 (ShiftRows) ^ round key); little-endian columns.
+void host_aes_encrypt(const AesKey &k, const uint8_t in[16], uint8_t out[16]) {
+  const uint32_t *t0 = tables().t0;
+  const uint8_t *sb = tables().sbox;
+  auto rotl = [](uint32_t x, int s) { return (x << s) | (x >> (32 - s)); };
+  uint32_t s[4], n[4];
+  std::memcpy(s, in, 16);
+  for (int j = 0; j < 4; j++) s[j] ^= k.rk[j];
+  for (int r = 1; r < 10; r++) {
+    for (int j = 0; j < 4; j++)
+      n[j] = t0[s[j] & 255] ^ rotl(t0[(s[(j + 1) & 3] >> 8) & 255], 8) ^
+             rotl(t0[(s[(j + 2) & 3] >> 16) & 255], 16) ^ rotl(t0[s[(j + 3) & 3] >> 24], 24) ^ k.rk[4 * r + j];
+    std::memcpy(s, n, 16);
+  }
+  for (int j = 0; j < 4; j++)
+    n[j] = (uint32_t(sb[s[j] & 255]) | (uint32_t(sb[(s[(j + 1) & 3] >> 8) & 255]) << 8) |
+            (uint32_t(sb[(s[(j + 2) & 3] >> 16) & 255]) << 16) | (uint32_t(sb[s[(j + 3) & 3] >> 24]) << 24)) ^
+           k.rk[40 + j];
+  std::memcpy(out, n, 16);
+}
 }  // namespace cuot

@@ -361,7 +361,7 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
     s.roots = reinterpret_cast<const Blk *>(it.roots_d);
     s.leaves = reinterpret_cast<Blk *>(it.v_d);
     r.leaves = reinterpret_cast<Blk *>(it.w_d);
-    s.delta = *reinterpret_cast<const Blk *>(&it.delta);
+    s.delta = host_load_blk(&it.delta);
     if (it.kind == CUOT_KIND_FERRET) {
       if ((st = balloc(b, &b->lsum[i], t * h * 16)) || (st = balloc(b, &b->rsum[i], t * h * 16)) ||
           (st = balloc(b, &b->ss[i], t * 16)) || (st = balloc(b, &b->mc[i], t * h * 16)))

@@ -7,6 +7,7 @@
 // encrypted without any byte swapping (cuOT's kernel swaps every word,
 // gpu/aes_op.cu:117-171).
 #pragma once
+#include <cstring>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/cuot.h"
@@ -14,6 +15,14 @@
 namespace cuot {
 
 struct __align__(16) Blk { uint32_t w[4]; };
+// A block from a host pointer with no alignment guarantee (a cuot_block is
+// 4-byte aligned; dereferencing it as the 16-byte-aligned Blk would let the
+// compiler use an aligned vector load).
+__host__ inline Blk host_load_blk(const void *p) {
+  Blk b;
+  std::memcpy(b.w, p, 16);
+  return b;
+}
 
 __host__ __device__ __forceinline__ Blk blk_xor(Blk a, Blk b) {
   Blk r;
@@ -49,6 +58,7 @@ struct AesKey { uint32_t rk[44]; uint32_t rkr[44]; };
 // S[x], little-endian).
 void host_aes_key_expand(const uint8_t key[16], AesKey *out);
 const uint32_t *host_t0_table();
+void host_aes_encrypt(const AesKey &k, const uint8_t in[16], uint8_t out[16]);
 
 // ---------------------------------------------------------------------------
 // Shared-memory T-table.  Row x (256 bytes) holds T0[x] replicated in words

@@ -97,7 +97,7 @@ extern "C" int cuot_ferret_pprf_sender_noalloc(const cuot_block *roots_d, uint64
   a.roots = reinterpret_cast<const Blk *>(roots_d);
   a.leaves = reinterpret_cast<Blk *>(leaves_d);
   a.scratch = s->scratch;
-  a.delta = *reinterpret_cast<const Blk *>(delta);
+  a.delta = host_load_blk(delta);
   a.lsum = reinterpret_cast<Blk *>(lsum_d);
   a.rsum = reinterpret_cast<Blk *>(rsum_d);
   a.ss_out = reinterpret_cast<Blk *>(secret_sum_d);

@@ -73,7 +73,7 @@ int cuot_ferret_pprf_sender(cuot_ctx *ctx, const cuot_block *roots_d, uint64_t t
   a.t = t; a.h = h;
   a.roots = reinterpret_cast<const Blk *>(roots_d);
   a.leaves = reinterpret_cast<Blk *>(leaves_d);
-  a.delta = *reinterpret_cast<const Blk *>(delta);
+  a.delta = host_load_blk(delta);
   a.lsum = reinterpret_cast<Blk *>(lsum_d);
   a.rsum = reinterpret_cast<Blk *>(rsum_d);
   a.ss_out = reinterpret_cast<Blk *>(secret_sum_d);
@@ -108,7 +108,7 @@ int cuot_sot_pprf_sender(cuot_ctx *ctx, const cuot_block *roots_d, uint64_t t, i
   a.t = t; a.h = h;
   a.roots = reinterpret_cast<const Blk *>(roots_d);
   a.leaves = reinterpret_cast<Blk *>(leaves_d);
-  a.delta = *reinterpret_cast<const Blk *>(delta);
+  a.delta = host_load_blk(delta);
   a.base0 = reinterpret_cast<const Blk *>(base0_d);
   a.base1 = reinterpret_cast<const Blk *>(base1_d);
   a.m0 = reinterpret_cast<Blk *>(m0_d);

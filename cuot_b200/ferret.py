@@ -1,6 +1,7 @@
 """Ferret random-COT session with device-resident state: the bootstrap
-instance and the rcot buffer loop of FerretCOT (ferret_cot.hpp) over the
-engine's MPCOT and primal-LPN kernels.
+instance and the rcot buffer loop of FerretCOT (ferret_cot.hpp), run by the
+C session of the library (cuot_ferret_session_*, ferret_session.cu); this
+module is its Python binding plus the parameter sets.
 
 Both parties live on one GPU and the transport between them is ideal: the
 sender's per-level sums reach the receiver as the OT would deliver them (the
@@ -26,12 +27,15 @@ LSB(v) = 0 (ferret_cot.hpp:27-31; spcot_sender.h clears the leaves' LSB), so
 the receiver's choice bit of every COT is LSB(w).
 
 Base COTs come from an ideal dealer seeded by the session (the reference
-produces them with IKNP, which is host protocol).  Host scalars (Delta, the
-per-extension LPN seed) are derived from the session seed with SHA-256;
-tree roots are drawn on the device with the AES-CTR PRG.
+produces them with IKNP, which is host protocol).  Every random choice comes
+from the AES-CTR stream (the cryptoTools PRNG) keyed by SHA-256 of the
+caller's seed: block 0 = Delta (LSB set), blocks 1 and 2 seed the dealer's
+COT values and choice bits, blocks 16 + 2e and 17 + 2e are the LPN seed and
+the roots seed of extension e (e = 0 is the set-up).
 """
 from __future__ import annotations
 
+import ctypes
 import hashlib
 from dataclasses import dataclass
 
@@ -75,16 +79,9 @@ FERRET_B12 = PrimalLPNParameter(10268672, 2507, 238000, 12, 268800, 1050, 17384,
 FERRET_B11 = PrimalLPNParameter(10180608, 4971, 124000, 11, 178944, 699, 17384, 8)
 
 
-def session_scalar(seed: bytes, label: str, index: int = 0) -> bytes:
-    """16 bytes derived from the session seed (SHA-256 of seed, label, index)."""
-    return hashlib.sha256(bytes(seed) + label.encode() + index.to_bytes(8, "little")).digest()[:16]
-
-
-def session_delta(seed: bytes) -> bytes:
-    """Delta with its LSB set (ferret_cot.hpp:27-31)."""
-    d = bytearray(session_scalar(seed, "delta"))
-    d[0] |= 1
-    return bytes(d)
+def session_key(seed: bytes) -> bytes:
+    """The 16-byte AES key of a session: SHA-256 of the caller's seed."""
+    return hashlib.sha256(bytes(seed)).digest()[:16]
 
 
 def chi_seeds(secret_sums) -> bytes:
@@ -95,123 +92,86 @@ def chi_seeds(secret_sums) -> bytes:
     return b"".join(hashlib.sha256(raw[i:i + 16]).digest()[:16] for i in range(0, len(raw), 16))
 
 
-class FerretSession:
-    """Both roles of a Ferret random-COT generator on one GPU.
+class _Param(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int64) for f in ("n", "t", "k", "log_bin_sz", "n_pre", "t_pre", "k_pre",
+                                              "log_bin_sz_pre")]
 
-    ctx_s / ctx_r: the sender's and the receiver's contexts (they may be the
-    same object).  `seed`: 16+ bytes from which every random choice of the
-    session is derived (reproducible).  After construction (set-up done),
-    rcot(num) returns (v, w): num COTs of each role as (num, 16) uint8 device
-    tensors."""
+
+class _State(ctypes.Structure):
+    _fields_ = [("M", ctypes.c_int64), ("ot_limit", ctypes.c_int64), ("ot_used", ctypes.c_int64),
+                ("extensions", ctypes.c_int64), ("delta", ctypes.c_uint32 * 4)]
+
+
+class FerretSession:
+    """Both roles of a Ferret random-COT generator on one GPU, over the C
+    session (cuot_ferret_session_*, ferret_session.cu).
+
+    ctx_s / ctx_r: the roles' contexts; both roles run on ctx_s's context and
+    `stream` (the C session orders them).  `seed`: bytes from which every
+    random choice of the session is derived (reproducible).  After
+    construction (set-up done), rcot(num) returns (v, w): num COTs of each
+    role as (num, 16) uint8 device tensors; ot_s / ot_r are the session's
+    output buffers (n blocks each)."""
 
     def __init__(self, ctx_s, ctx_r, param: PrimalLPNParameter, seed: bytes, d: int = 10, stream=None):
         import torch
-        self.torch = torch
-        self.ctx_s, self.ctx_r = ctx_s, ctx_r
+        from . import _check, _ptr, _stream
+        self.torch, self._check, self._ptr = torch, _check, _ptr
+        self.ctx = ctx_s
         self.p, self.seed, self.d = param, bytes(seed), d
         self.stream = stream
-        self.delta = session_delta(self.seed)
-        self.extensions = 0  # extensions run, the bootstrap included
-        dev = torch.device("cuda", torch.cuda.current_device())
-        self.dev = dev
-        emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device=dev)
-        p = param
-        # current output buffer of each role (n blocks) and the pre-COTs (M)
-        self.ot_s, self.ot_r = emp(p.n), emp(p.n)
-        self.pre_s, self.pre_r = emp(p.M), emp(p.M)
-        tmax = max(p.t, p.t_pre)
-        thmax = max(p.t * p.h, p.t_pre * p.h_pre)
-        self._roots = emp(tmax)
-        self._lsum, self._rsum, self._mc = emp(thmax), emp(thmax), emp(thmax)
-        self._ss = emp(tmax)
-        self._setup()
-        self.ot_used = p.ot_limit
-
-    # -- one extension (ferret_cot.hpp:83-97) ------------------------------
-    def _extend(self, n, t, h, k, mp_s, mp_r, kk_s, kk_r, out_s, out_r):
-        torch = self.torch
-        st = self.stream
-        idx = self.extensions
-        roots = self._roots[:t]
-        self.ctx_s.prg_fill(session_scalar(self.seed, "roots", idx), roots, stream=st)
-        lsum, rsum, ss, mc = self._lsum[:t * h], self._rsum[:t * h], self._ss[:t], self._mc[:t * h]
-        self.ctx_s.ferret_pprf_sender(roots, h, self.delta, out_s, lsum, rsum, ss, stream=st)
-        # OTs over the pre-COTs: choice bit i = LSB(mp_r[i]); the receiver gets
-        # the sum its bit selects (preot.h:58-82)
-        with torch.cuda.stream(st) if st is not None else _null():
-            choice = (mp_r[:, 0] & 1).contiguous()
-            torch.where(choice.view(-1, 1).bool(), rsum, lsum, out=mc)
-        self.ctx_r.ferret_pprf_recver(mc, choice, ss, h, out_r, stream=st)
-        lpn_seed = session_scalar(self.seed, "lpn", idx)
-        self.ctx_s.lpn_primal(lpn_seed, kk_s, out_s, d=self.d, stream=st)
-        self.ctx_r.lpn_primal(lpn_seed, kk_r, out_r, d=self.d, stream=st)
-        self.extensions += 1
-
-    def _setup(self):
-        """Bootstrap (ferret_cot.hpp:150-170) on dealer base COTs."""
-        torch, p = self.torch, self.p
-        nb_mp, nb_data = p.t_pre * p.h_pre, p.k_pre + CONSIST_CHECK_COT_NUM
-        base_s, base_r = self.base_cots(nb_mp + nb_data)
+        self.dev = torch.device("cuda", torch.cuda.current_device())
         emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device=self.dev)
-        out_s, out_r = emp(p.n_pre), emp(p.n_pre)
-        data_s, data_r = base_s[nb_mp:], base_r[nb_mp:]
-        c = CONSIST_CHECK_COT_NUM
-        self._extend(p.n_pre, p.t_pre, p.h_pre, p.k_pre, base_s[:nb_mp], base_r[:nb_mp],
-                     data_s[c:c + p.k_pre], data_r[c:c + p.k_pre], out_s, out_r)
-        self.pre_s.copy_(out_s[:p.M])
-        self.pre_r.copy_(out_r[:p.M])
+        self.ot_s, self.ot_r = emp(param.n), emp(param.n)
+        pr = _Param(param.n, param.t, param.k, param.h, param.n_pre, param.t_pre, param.k_pre, param.h_pre)
+        key = (ctypes.c_uint8 * 16).from_buffer_copy(session_key(self.seed))
+        h = ctypes.c_void_p()
+        self.lib = ctx_s.lib
+        _check(self.lib.cuot_ferret_session_create(ctx_s.h, ctypes.byref(pr), key, ctypes.c_int(d), _ptr(self.ot_s),
+                                                   _ptr(self.ot_r), _stream(stream), ctypes.byref(h)),
+               "cuot_ferret_session_create")
+        self.h = h
 
-    def base_cots(self, count: int):
-        """Ideal dealer: count COTs (v, w = v ^ x * Delta) with LSB(v) = 0."""
-        torch = self.torch
-        emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device=self.dev)
-        v, x = emp(count), emp(count)
-        self.ctx_s.prg_fill(session_scalar(self.seed, "base-v"), v, stream=self.stream)
-        self.ctx_s.prg_fill(session_scalar(self.seed, "base-x"), x, stream=self.stream)
-        with torch.cuda.stream(self.stream) if self.stream is not None else _null():
-            v[:, 0] &= 0xFE
-            dl = torch.frombuffer(bytearray(self.delta), dtype=torch.uint8).to(self.dev)
-            w = torch.where((x[:, :1] & 1).bool(), v ^ dl, v)
-        return v, w
+    def _state(self) -> _State:
+        st = _State()
+        self._check(self.lib.cuot_ferret_session_info(self.h, ctypes.byref(st)), "cuot_ferret_session_info")
+        return st
+
+    @property
+    def extensions(self) -> int:
+        return int(self._state().extensions)
+
+    @property
+    def ot_used(self) -> int:
+        return int(self._state().ot_used)
+
+    @property
+    def delta(self) -> bytes:
+        return bytes(bytearray(self._state().delta))
 
     def extend_f2k(self):
-        """One extension into the session buffer; its last M outputs become
-        the next pre-COTs (ferret_cot.hpp:99-106)."""
-        p = self.p
-        c = CONSIST_CHECK_COT_NUM
-        th = p.t * p.h
-        self._extend(p.n, p.t, p.h, p.k, self.pre_s[:th], self.pre_r[:th],
-                     self.pre_s[c:c + p.k], self.pre_r[c:c + p.k], self.ot_s, self.ot_r)
-        with self.torch.cuda.stream(self.stream) if self.stream is not None else _null():
-            self.pre_s.copy_(self.ot_s[p.ot_limit:])
-            self.pre_r.copy_(self.ot_r[p.ot_limit:])
-        self.ot_used = 0
+        """One extension into ot_s / ot_r (ferret_cot.hpp:99-106)."""
+        self._check(self.lib.cuot_ferret_session_extend(self.h), "cuot_ferret_session_extend")
 
     def silent_ot_left(self) -> int:
-        return self.p.ot_limit - self.ot_used
+        st = self._state()
+        return int(st.ot_limit - st.ot_used)
 
     def rcot(self, num: int):
         """num random COTs of each role (ferret_cot.hpp:178-210)."""
-        torch = self.torch
-        emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device=self.dev)
+        emp = lambda m: self.torch.empty((m, 16), dtype=self.torch.uint8, device=self.dev)
         v, w = emp(num), emp(num)
-        done = 0
-        while done < num:
-            if self.silent_ot_left() == 0:
-                self.extend_f2k()
-            take = min(num - done, self.silent_ot_left())
-            a = self.ot_used
-            with torch.cuda.stream(self.stream) if self.stream is not None else _null():
-                v[done:done + take].copy_(self.ot_s[a:a + take])
-                w[done:done + take].copy_(self.ot_r[a:a + take])
-            self.ot_used += take
-            done += take
+        self._check(self.lib.cuot_ferret_session_rcot(self.h, ctypes.c_int64(num), self._ptr(v), self._ptr(w)),
+                    "cuot_ferret_session_rcot")
         return v, w
 
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cuot_ferret_session_destroy(self.h)
+            self.h = None
 
-class _null:
-    def __enter__(self):
-        return None
-
-    def __exit__(self, *a):
-        return False
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -168,6 +168,38 @@ int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
                        uint64_t row_bytes, uint64_t col_lo, uint64_t col_hi,
                        void *out_d, void *stream);
 
+/* ---- Ferret session: set-up + rcot buffer loop -------------------------------
+ * FerretCOT's data flow (ferret_cot.hpp:99-210) with both parties on one GPU
+ * and an ideal transport between them (the receiver's MPCOT OT messages are
+ * selected by the LSB of its pre-COTs, as OTPre over the pre-COTs would
+ * deliver them; secret sums and the LPN seed are handed over directly).
+ * Parameters as PrimalLPNParameter (constants.h:9-25).  create() runs the
+ * set-up extension on dealer base COTs; every extension consumes M = k + t*h
+ * + 128 pre-COTs of each role, writes n COTs of each role into ot_s_d /
+ * ot_r_d (caller-owned, n blocks each; w = v ^ x * delta, x = LSB(w)) and
+ * keeps the last M as the next pre-COTs on the device.  rcot() returns num
+ * COTs of each role (device), extending whenever the buffer runs dry.  All
+ * randomness comes from `seed` (AES-CTR blocks, as cuot_prg_fill).  Calls are
+ * stream-ordered on `stream`; create() synchronises once. */
+typedef struct {
+  int64_t n, t, k, log_bin_sz, n_pre, t_pre, k_pre, log_bin_sz_pre;
+} cuot_ferret_param;
+typedef struct {
+  int64_t M, ot_limit, ot_used, extensions;
+  cuot_block delta;
+} cuot_ferret_session_state;
+typedef struct cuot_ferret_session cuot_ferret_session;
+int cuot_ferret_session_create(cuot_ctx *ctx, const cuot_ferret_param *param,
+                               const uint8_t seed[16], int d, cuot_block *ot_s_d,
+                               cuot_block *ot_r_d, void *stream,
+                               cuot_ferret_session **out);
+int cuot_ferret_session_extend(cuot_ferret_session *s);
+int cuot_ferret_session_rcot(cuot_ferret_session *s, int64_t num,
+                             cuot_block *v_d, cuot_block *w_d);
+int cuot_ferret_session_info(const cuot_ferret_session *s,
+                             cuot_ferret_session_state *out);
+int cuot_ferret_session_destroy(cuot_ferret_session *s);
+
 /* ---- Ferret malicious consistency check ------------------------------------
  * out_d[j] = sum_{i < 2^h} seed_j^(i+1) * leaves[j*2^h + i] over GF(2^128)
  * (natural bit order, mod x^128 + x^7 + x^2 + x + 1), for every tree j < t:

@@ -2,8 +2,8 @@
 import numpy as np
 import pytest
 
-from cuot_b200.ferret import FERRET_B11, FERRET_B12, FERRET_B13, PrimalLPNParameter, session_delta
-from tests.ferret_replay import SMALL, check_cot, oracle_session
+from cuot_b200.ferret import FERRET_B11, FERRET_B12, FERRET_B13, PrimalLPNParameter
+from tests.ferret_replay import SMALL, check_cot, oracle_session, session_delta
 
 
 def test_b13_limits():
@@ -24,5 +24,5 @@ def test_parameter_check():
 def test_oracle_replay_keeps_cot_correlation():
     seed = b"ferret-session-cpu"
     v, w = oracle_session(SMALL, seed, 3)
-    x = check_cot(v, w, np.frombuffer(session_delta(seed), np.uint8))
+    x = check_cot(v, w, session_delta(seed))
     assert 0.45 < x.mean() < 0.55

@@ -45,3 +45,26 @@ def test_argument_errors_leave_context_usable(ctx):
     d = to_dev(pt)
     ctx.aes128_ecb(key, d)
     assert np.array_equal(to_host(d), oracle.aes_ecb(key, pt))
+
+
+def test_host_block_arguments_need_no_alignment(ctx):
+    """A host cuot_block (delta) is only 4-byte aligned in C; the entry points
+    must not assume 16 (a misaligned vector load would crash the caller)."""
+    import ctypes
+    from cuot_b200 import _check, _ptr, _stream
+    from tests.util import delta_ferret
+    rng = np.random.default_rng(4)
+    t, h = 3, 5
+    roots, delta = rng_blocks(rng, t), delta_ferret(rng)
+    buf = (ctypes.c_uint8 * 64)()
+    base = ctypes.addressof(buf)
+    addr = base + (4 if base % 16 != 4 else 8)   # 4-byte aligned, not 16
+    assert addr % 16 != 0
+    ctypes.memmove(addr, delta.tobytes(), 16)
+    e = lambda m: torch.empty((m, 16), dtype=torch.uint8, device="cuda")
+    lv, ls, rs, ss = e(t << h), e(t * h), e(t * h), e(t)
+    _check(ctx.lib.cuot_ferret_pprf_sender(ctx.h, _ptr(to_dev(roots)), ctypes.c_uint64(t), ctypes.c_int(h),
+                                           ctypes.c_void_p(addr), _ptr(lv), _ptr(ls), _ptr(rs), _ptr(ss),
+                                           _stream(None)), "cuot_ferret_pprf_sender")
+    exp = oracle.ferret_pprf_sender(roots, h, delta)
+    assert np.array_equal(to_host(lv), exp[0]) and np.array_equal(to_host(ss), exp[3])

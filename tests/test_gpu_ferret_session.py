@@ -5,13 +5,13 @@ ferret_b13 size."""
 import numpy as np
 import pytest
 
-from tests.ferret_replay import SMALL, check_cot, oracle_session
+from tests.ferret_replay import SMALL, check_cot, oracle_session, session_delta
 from tests.util import to_host
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-from cuot_b200.ferret import FERRET_B13, FerretSession, session_delta  # noqa: E402
+from cuot_b200.ferret import FERRET_B13, FerretSession  # noqa: E402
 
 
 def test_session_matches_oracle_replay(ctx):
@@ -23,7 +23,7 @@ def test_session_matches_oracle_replay(ctx):
     exp_v, exp_w = oracle_session(SMALL, seed, 5)
     assert np.array_equal(to_host(s.ot_s), exp_v)
     assert np.array_equal(to_host(s.ot_r), exp_w)
-    delta = np.frombuffer(session_delta(seed), np.uint8)
+    delta = session_delta(seed)
     x = check_cot(np.concatenate([to_host(v1), to_host(v2)]), np.concatenate([to_host(w1), to_host(w2)]), delta)
     assert 0.45 < x.mean() < 0.55
     # the last 123 served COTs are the first outputs of the last extension
@@ -39,5 +39,5 @@ def test_session_b13_correlation(ctx):
     assert FERRET_B13.ot_limit == 10016992
     v, w = s.rcot(FERRET_B13.ot_limit + 1000)
     assert s.extensions == 3
-    x = check_cot(to_host(v), to_host(w), np.frombuffer(session_delta(seed), np.uint8))
+    x = check_cot(to_host(v), to_host(w), session_delta(seed))
     assert 0.49 < x.mean() < 0.51
