@@ -658,26 +658,24 @@ def run_served(args, device: int) -> dict:
     continuous-batching server sets the sustained rate (90 % of it); the
     same Poisson stream is then served by the continuous-batching server and
     by plain per-request execution (one request at a time)."""
-    import torch
-    from cuot_b200.serve import GpuExecutor, Server, make_stream, sustained_rate
+    from cuot_b200.serve import Server, make_stream, sustained_rate
 
     lo, hi = 14, 24
     # small requests (n < 2^20) on high-priority streams; at most one request
     # with n >= 2^22 in flight (a sweep of these two knobs on this workload:
     # this pair beat plain per-request execution on p50, p99 and mean)
     big_n, prio_n = 1 << 22, 1 << 20
-    cont = GpuExecutor(slots=args.serve_slots, device=device, max_log_n=hi, high_priority_below_n=prio_n)
+    cont = Server(slots=args.serve_slots, device=device, max_log_n=hi, budget_bytes=1e15,
+                  high_priority_below_n=prio_n)
     probe = make_stream(min(100, args.serve_requests), rate=0.0, seed=5, lo=lo, hi=hi)
     rate = sustained_rate(cont, probe)
     reqs = make_stream(args.serve_requests, rate=rate, seed=6, lo=lo, hi=hi)
-    rep = Server(cont, budget_bytes=120e9, big_n=big_n).run(reqs)
-    del cont
-    torch.cuda.synchronize()
-    plain = GpuExecutor(slots=1, device=device, max_log_n=hi)
-    for r in reqs:
-        r.status, r.result = "pending", None
-    rep_plain = Server(plain, budget_bytes=120e9).run(reqs)
-    del plain
+    cont.configure(budget_bytes=120e9, big_n=big_n, high_priority_below_n=prio_n)
+    rep = cont.run(reqs)
+    cont.close()
+    plain = Server(slots=1, device=device, max_log_n=hi, budget_bytes=120e9)
+    rep_plain = plain.run(reqs)
+    plain.close()
     keys = ("done", "cots_per_s", "p50_ms", "p99_ms", "mean_ms", "wall_s")
     return {"requests": args.serve_requests, "slots": args.serve_slots, "budget_gb": 120,
             "log2_n": [lo, hi], "rate_rps": rate,

@@ -336,6 +336,87 @@ int cuot_batch_kernels_per_run(const cuot_batch *b);
  * receiver PPRF, LPN, SOT encodes. */
 int cuot_batch_run_phases(cuot_batch *b, void *stream, float *phase_ms);
 
+/* ---- Serving: continuous batching of OT-extension requests ------------------
+ * No counterpart in the reference, which runs one instance per call.  Each
+ * request is one extension with both roles (Ferret: MPCOT + primal LPN with
+ * d = 10 and k inputs; SOT: PPRF + exact QC dual LPN + the receiver's choice
+ * bits a*e), its inputs derived on the device from `seed`: AES-CTR blocks
+ * [0, t) are the roots, the next ceil(t*h/16) blocks' byte LSBs the choice
+ * bits (Ferret [t][h], SOT [h][t]), then kk_send, kk_recv (k blocks each) or
+ * base0, base1 ([h][t] each).  Its scalars are blocks 2^40 + {0, 1, 2}
+ * (cuot_request_scalars).  The server keeps `slots` contexts busy, admitting
+ * queued requests in arrival order while a slot is free and the request's
+ * footprint fits budget_bytes minus the slots' reserved scratch; at most
+ * max_big (>= 1) requests with n >= big_n (0: no limit) run at once, and
+ * smaller ones may pass a big one waiting for that reason.  Requests with
+ * n < high_priority_below_n run on a high-priority stream.  A request waiting
+ * longer than max_queue_wait seconds (0: forever) times out; one that can
+ * never run (bad shape, n > 2^max_log_n, footprint above the budget) is
+ * rejected.  Results: v_h / w_h (n blocks) and c_h (SOT, n bits) when non-null
+ * (pinned host memory keeps the copies asynchronous); t_admit and t_done are
+ * seconds from the start of run().  With dry_run_service_s > 0 no device work
+ * is done: every request takes that long (host-only scheduling tests). */
+#define CUOT_REQ_PENDING 0
+#define CUOT_REQ_QUEUED 1
+#define CUOT_REQ_RUNNING 2
+#define CUOT_REQ_DONE 3
+#define CUOT_REQ_TIMEOUT 4
+#define CUOT_REQ_CANCELLED 5
+#define CUOT_REQ_REJECTED 6
+#define CUOT_REQ_FAILED 7
+typedef struct {
+  int kind;           /* CUOT_KIND_* */
+  int h;              /* tree depth */
+  uint64_t t;         /* trees; n = t << h */
+  int64_t k;          /* Ferret LPN inputs */
+  uint8_t seed[16];
+  double arrival;     /* seconds from the start of run() */
+  cuot_block *v_h;    /* [n] out (optional) */
+  cuot_block *w_h;    /* [n] out (optional) */
+  uint64_t *c_h;      /* [n/64] out (optional, SOT) */
+  int status;         /* out: CUOT_REQ_* */
+  double t_admit;     /* out: -1 if never admitted */
+  double t_done;      /* out: -1 if not done */
+} cuot_request;
+typedef struct {
+  int slots;                       /* concurrent requests (contexts), 1..256 */
+  int max_log_n;                   /* largest request, 10..25 (0: 24) */
+  double budget_bytes;             /* device bytes for slots' scratch + requests */
+  double max_queue_wait;           /* seconds; 0: no timeout */
+  uint64_t big_n;                  /* 0: no big-request limit */
+  int max_big;
+  uint64_t high_priority_below_n;  /* 0: one stream priority */
+  double dry_run_service_s;        /* > 0: host-only mode */
+} cuot_server_config;
+typedef struct {
+  double wall_s;          /* run() duration */
+  double max_used_bytes;  /* peak footprint of admitted requests */
+} cuot_server_stats;
+typedef struct cuot_server cuot_server;
+/* Creates the slots' contexts and streams, reserves their scratch and builds
+ * the QC tables of every size up to 2^max_log_n (synchronises). */
+int cuot_server_create(int device, const cuot_server_config *cfg,
+                       cuot_server **out);
+/* Device bytes reserved by the slots (taken from the budget). */
+int cuot_server_reserved_bytes(const cuot_server *s, uint64_t *out);
+/* Replaces the scheduling policy (budget_bytes, max_queue_wait, big_n,
+ * max_big, high_priority_below_n) for later run() calls; the other fields
+ * are fixed at creation. */
+int cuot_server_configure(cuot_server *s, const cuot_server_config *cfg);
+/* Cancels reqs[index] of the current (or next) run() if it is still queued;
+ * callable from another thread while run() is in progress. */
+int cuot_server_cancel(cuot_server *s, int index);
+/* Serves `count` requests until each is done, timed out, cancelled or
+ * rejected (blocks).  Returns CUOT_ECUDA if a request's device work failed
+ * (that and the running requests end as CUOT_REQ_FAILED). */
+int cuot_server_run(cuot_server *s, cuot_request *reqs, int count,
+                    cuot_server_stats *stats);
+int cuot_server_destroy(cuot_server *s);
+/* Delta (LSB set), LPN seed and QC key of a request with this seed. */
+int cuot_request_scalars(const uint8_t seed[16], cuot_block out[3]);
+/* Device bytes a request holds while admitted. */
+int cuot_request_footprint(const cuot_request *r, uint64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,3 +55,15 @@ def test_null_arguments_are_rejected_without_a_device():
     assert lib.cuot_ferret_pprf_sender(None, None, ctypes.c_uint64(1), 3, None, None, None, None, None, None) == 1
     assert lib.cuot_lpn_primal(None, None, None, ctypes.c_int64(1), 10, None, ctypes.c_int64(1), None) == 1
     assert lib.cuot_ctx_destroy(None) == 0
+
+
+def test_server_arguments_are_checked_without_a_device():
+    lib = cuot_b200.load()
+    from cuot_b200.serve import _Config
+    h = ctypes.c_void_p()
+    assert lib.cuot_server_create(0, None, ctypes.byref(h)) == 1
+    bad = _Config(slots=2, max_log_n=30, dry_run_service_s=0.01)
+    assert lib.cuot_server_create(0, ctypes.byref(bad), ctypes.byref(h)) == 1
+    assert b"max_log_n" in lib.cuot_last_error()
+    assert lib.cuot_server_run(None, None, 0, None) == 1
+    assert lib.cuot_server_destroy(None) == 0

@@ -9,7 +9,7 @@ import oracle
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-from cuot_b200.serve import KIND_FERRET, GpuExecutor, Server, make_stream, request_scalars  # noqa: E402
+from cuot_b200.serve import KIND_FERRET, Server, make_stream, request_scalars  # noqa: E402
 
 
 def oracle_result(r):
@@ -47,20 +47,38 @@ def oracle_result(r):
 
 def test_results_same_alone_and_in_the_mix():
     reqs = make_stream(14, rate=0.0, seed=11, lo=11, hi=15)
-    mix = GpuExecutor(slots=4, max_log_n=15, keep_outputs=True)
-    rep = Server(mix, budget_bytes=8e9).run(reqs)
+    mix = Server(slots=4, max_log_n=15, keep_outputs=True, budget_bytes=8e9, high_priority_below_n=1 << 13)
+    rep = mix.run(reqs)
+    mix.close()
     assert rep["done"] == len(reqs)
     in_mix = [r.result for r in reqs]
-    alone_ex = GpuExecutor(slots=1, max_log_n=15, keep_outputs=True)
-    for r in reqs:
-        r.status, r.result = "pending", None
-    Server(alone_ex, budget_bytes=8e9).run(reqs)
+    alone = Server(slots=1, max_log_n=15, keep_outputs=True, budget_bytes=8e9)
+    alone.run(reqs)
+    alone.close()
     for r, m in zip(reqs, in_mix):
         a = r.result
         assert np.array_equal(a[0], m[0]) and np.array_equal(a[1], m[1])
         if a[2] is not None:
             assert np.array_equal(a[2], m[2])
     for r in (reqs[0], reqs[1], reqs[-1]):
+        ev, ew, ec = oracle_result(r)
+        assert np.array_equal(r.result[0], ev) and np.array_equal(r.result[1], ew)
+        if ec is not None:
+            assert np.array_equal(r.result[2].view(np.uint64), ec)
+
+
+def test_both_kinds_checked_and_big_limit_on_device():
+    """One Ferret and one SOT request against the oracle, served with the
+    big-request limit on and arrivals spread out."""
+    reqs = make_stream(12, rate=400.0, seed=21, lo=11, hi=14)
+    kinds = {r.kind for r in reqs}
+    assert kinds == {0, 1}
+    srv = Server(slots=3, max_log_n=14, keep_outputs=True, budget_bytes=8e9, big_n=1 << 13, max_big=1)
+    rep = srv.run(reqs)
+    srv.close()
+    assert rep["done"] == len(reqs)
+    for kind in (0, 1):
+        r = next(x for x in reqs if x.kind == kind)
         ev, ew, ec = oracle_result(r)
         assert np.array_equal(r.result[0], ev) and np.array_equal(r.result[1], ew)
         if ec is not None:
