@@ -149,7 +149,7 @@ struct SotClass {
   int batch = 1;                  // planes per NTT pass for this size (Y holds batch * 4n bytes)
   std::vector<int> items;         // item indices of this size
   uint8_t *planes = nullptr;      // 2 * items * 16n bytes (jobs: item x role)
-  std::vector<const uint2 *> ahats;  // per job
+  std::vector<const void *> ahats;  // per job
 };
 
 }  // namespace
@@ -176,8 +176,8 @@ struct cuot_batch {
   unsigned int *counters = nullptr;  // [3]
   // SOT
   std::vector<SotClass> classes;
-  uint32_t *Y = nullptr;  // NTT intermediate, max over classes of batch * 4n bytes
-  std::vector<uint2 *> item_ahat;     // per item (SOT), nullptr otherwise
+  void *Y = nullptr;  // QC intermediate, max over classes of qc_y_bytes(batch)
+  std::vector<void *> item_ahat;      // per item (SOT), nullptr otherwise
   std::vector<cuot_qc_plan *> plans;  // plain path, per item (SOT)
   // Ferret per-item sums (batch-owned)
   std::vector<Blk *> lsum, rsum, ss, mc, m0, m1;
@@ -454,14 +454,14 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
                                            : qc_default_batch(n, int(256 * c.items.size()));
     pb = std::min(pb, int(256 * c.items.size()));
     c.batch = pb;  // this class's passes use exactly the Y size reserved for them
-    ybytes = std::max(ybytes, uint64_t(pb) * n * 4);
+    ybytes = std::max(ybytes, qc_y_bytes(ctx, c.e, pb));
   }
   if (!b->classes.empty()) {
     if ((st = balloc(b, &b->Y, ybytes))) return cleanup(st);
     for (auto &c : b->classes) {
       for (int i : c.items) {
         const uint64_t n = 1ull << c.e;
-        if ((st = balloc(b, &b->item_ahat[i], n * 8))) return cleanup(st);
+        if ((st = balloc(b, &b->item_ahat[i], qc_ahat_bytes(ctx, c.e)))) return cleanup(st);
         if ((st = qc_build_ahat(ctx, c.e, items[i].a_d, b->Y, b->item_ahat[i], nullptr))) return cleanup(st);
         c.ahats.push_back(b->item_ahat[i]);  // sender job
         c.ahats.push_back(b->item_ahat[i]);  // receiver job

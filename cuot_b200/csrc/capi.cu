@@ -142,6 +142,10 @@ int cuot_ctx_set_tuning(cuot_ctx *c, int key, int64_t value) {
       if (value < 0 || value > 4096) return fail(CUOT_EINVAL, "planes per pass out of range");
       c->qc_planes_per_pass = int(value);
       return CUOT_OK;
+    case CUOT_TUNE_QC_BACKEND:
+      if (value < 0 || value > 2) return fail(CUOT_EINVAL, "QC backend must be 0 (automatic), 1 (NTT) or 2 (FFT)");
+      c->qc_backend = int(value);
+      return CUOT_OK;
     default:
       return fail(CUOT_EINVAL, "unknown tuning key %d", key);
   }

@@ -8,8 +8,10 @@ struct cuot_ctx {
   void *scratch;           // grow-only scratch arena
   uint64_t scratch_bytes;
   void *qc_tables[32];     // NTT twiddle tables per log2(n) (qc.cu)
+  void *qcf_tables[32];    // FFT twiddle tables per log2(n) (qc_fft.cu)
   int pprf_threads;        // threads per tree CTA (128 or 256)
   int qc_planes_per_pass;  // 0: automatic
+  int qc_backend;          // CUOT_TUNE_QC_BACKEND value: 0 automatic, 1 NTT, 2 FFT
 };
 
 namespace cuot {
@@ -35,12 +37,34 @@ int scratch(cuot_ctx *ctx, uint64_t bytes, void **out);
 int pprf_init_device();
 // Frees the context's cached QC tables (qc.cu).
 void qc_free_ctx_tables(cuot_ctx *ctx);
-// QC helpers used by the batched engine (qc.cu).
+// QC helpers used by the batched engine (qc.cu).  The backend (NTT or FFT)
+// of an n = 2^e encode follows the context's CUOT_TUNE_QC_BACKEND; A_hat
+// and intermediate sizes depend on it.
 int qc_prepare(cuot_ctx *ctx, int e);
-int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, uint32_t *Y, uint2 *ahat, cudaStream_t st);
-int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const uint2 *const *ahats,
-                   uint32_t *Y, int batch, cudaStream_t st);
+uint64_t qc_ahat_bytes(const cuot_ctx *ctx, int e);
+uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch);
+int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st);
+int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void *const *ahats,
+                   void *Y, int batch, cudaStream_t st);
 int qc_default_batch(uint64_t n, int nplanes);
+// FP64 FFT backend of the QC encode (qc_fft.cu): n = 2^e, 10 <= e <= kQcfMaxE.
+constexpr int kQcfMaxE = 20;
+// A_hat of each transform y of a launch: p[(first + y) / per] (4 planes per transform).
+struct QcfAhatTab {
+  const void *p[16];
+  int first;
+  int per;
+};
+struct QcfTables;
+bool qcf_supported(int e);
+int qcf_get_tables(cuot_ctx *ctx, int e, QcfTables **out);
+void qcf_free_ctx_tables(cuot_ctx *ctx);
+// A_hat (n complex doubles) of `a`; Y holds 16n bytes.
+int qcf_build_ahat(const QcfTables *t, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st);
+// Planes p < nplanes: in + p * stride -> out + p * stride (64-bit words),
+// written or XORed (accumulate); Y holds round4(batch) * 4n bytes.
+int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
+               int accumulate, int nplanes, void *Y, int batch, cudaStream_t st);
 int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
                      uint64_t col_hi, void *out, cudaStream_t st);
 }  // namespace cuot

@@ -528,6 +528,7 @@ static int split_e(int e, int *e1, int *e2) {
 }
 
 static int dev_alloc(void **p, size_t bytes) {
+  *p = nullptr;
   if (cudaMalloc(p, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(CUOT_ENOMEM, "QC table allocation of %zu bytes failed", bytes);
@@ -584,6 +585,7 @@ void qc_free_ctx_tables(cuot_ctx *ctx) {
     free_tables(static_cast<QcTables *>(ctx->qc_tables[e]));
     ctx->qc_tables[e] = nullptr;
   }
+  qcf_free_ctx_tables(ctx);
 }
 
 static int col_smem(const QcTables *t) {
@@ -690,24 +692,6 @@ static int encode_planes_strided(const QcTables *t, const uint2 *ahat, const uin
   return launch_status(3 * ((nplanes + batch - 1) / batch));
 }
 
-// Encodes `nplanes` planes (n bits each, consecutive) in place.
-static int encode_planes(const QcTables *t, const uint2 *ahat, uint64_t *planes, int nplanes,
-                         uint32_t *Y, int batch, cudaStream_t st) {
-  const uint64_t n = 1ull << t->e;
-  return encode_planes_strided(t, ahat, planes, planes, n / 64, 0, nplanes, Y, batch, st);
-}
-
-// Rate-1/2 dual LPN: out[i] = in[i] ^ (a * in[n..2n))[i] blockwise, i < n.
-// planes: 128 planes of 2n bits (stride n/32 words); Y: batch planes.
-static int dual_lpn_r2(const QcTables *t, const uint2 *ahat, const cuot_block *in_d, cuot_block *out_d,
-                       uint8_t *planes, uint32_t *Y, int batch, cudaStream_t st) {
-  const uint64_t n = 1ull << t->e;
-  uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
-  CUOT_TRY(transpose_launch(in_d, 2 * n, 16, 0, 128, planes, st));
-  CUOT_TRY(encode_planes_strided(t, ahat, pl + n / 64, pl, n / 32, 1, 128, Y, batch, st));
-  return transpose_launch(planes, 128, n / 4, 0, n, out_d, st);
-}
-
 static int check_n(uint64_t n, int *e) {
   if (n < 1024 || n > (1ull << 25) || (n & (n - 1)))
     return fail(CUOT_EINVAL, "QC n=%llu must be a power of two in [2^10, 2^25]",
@@ -716,10 +700,10 @@ static int check_n(uint64_t n, int *e) {
   return CUOT_OK;
 }
 
-// Planes per batch: up to 512 MiB of 4-byte intermediate.  Measured on B200
-// (n = 2^20 / 2^22, one role): 64 MiB batches 2.02 / 9.19 ms, 512 MiB
-// batches 1.83 / 7.96 ms -- more CTAs per launch outweigh the intermediate
-// spilling out of L2.
+// Planes per batch: up to 512 MiB of 4-byte-per-plane intermediate.
+// Measured on B200 with the NTT (n = 2^20 / 2^22, one role): 64 MiB batches
+// 2.02 / 9.19 ms, 512 MiB batches 1.83 / 7.96 ms -- more CTAs per launch
+// outweigh the intermediate spilling out of L2.
 static int default_batch(uint64_t n, int nplanes) {
   uint64_t b = (512ull << 20) / (4 * n);
   if (b < 1) b = 1;
@@ -727,41 +711,124 @@ static int default_batch(uint64_t n, int nplanes) {
   return int(b);
 }
 
-// ---- helpers for the batched engine (batch.cu) ----------------------------
-int qc_prepare(cuot_ctx *ctx, int e) {
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  return set_attrs(t);
+// ---- backend selection -------------------------------------------------------
+// The fp64 FFT (qc_fft.cu) for n <= 2^20 unless the context asks for the NTT.
+static bool use_fft(const cuot_ctx *ctx, int e) { return ctx->qc_backend != 1 && qcf_supported(e); }
+
+// Intermediate bytes of a pass over `batch` planes: 4 bytes per plane and
+// coefficient for both backends (the FFT packs 4 planes in 16 bytes, in
+// whole transforms, and builds A_hat in one 16n-byte transform).
+static uint64_t y_bytes(bool fft, int e, int batch) {
+  if (!fft) return uint64_t(batch) << (e + 2);
+  uint64_t b = (uint64_t(batch) + 3) & ~3ull;
+  return (b < 4 ? 4 : b) << (e + 2);
 }
 
-int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, uint32_t *Y, uint2 *ahat, cudaStream_t st) {
+struct QcEngine {
+  bool fft;
   QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  return build_ahat(t, a_d, Y, ahat, st);
+  QcfTables *f;
+};
+
+static int engine(cuot_ctx *ctx, int e, bool fft, QcEngine *g) {
+  g->fft = fft;
+  g->t = nullptr;
+  g->f = nullptr;
+  if (fft) return qcf_get_tables(ctx, e, &g->f);
+  CUOT_TRY(get_tables(ctx, e, &g->t));
+  return set_attrs(g->t);
+}
+
+// A_hat of `a` (NTT: n Shoup pairs; FFT: n complex doubles) using Y as scratch.
+static int eng_ahat(const QcEngine &g, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
+  if (g.fft) return qcf_build_ahat(g.f, a_d, Y, ahat, st);
+  return build_ahat(g.t, a_d, static_cast<uint32_t *>(Y), static_cast<uint2 *>(ahat), st);
+}
+
+// Planes p < nplanes: in + p * stride -> out + p * stride (64-bit words),
+// written or XORed into (accumulate).
+static int eng_encode(const QcEngine &g, const void *ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
+                      int accumulate, int nplanes, void *Y, int batch, cudaStream_t st) {
+  if (g.fft) {
+    QcfAhatTab tab{};
+    tab.p[0] = ahat;
+    tab.per = 1 << 30;
+    return qcf_encode(g.f, tab, in, out, stride, accumulate, nplanes, Y, batch, st);
+  }
+  return encode_planes_strided(g.t, static_cast<const uint2 *>(ahat), in, out, stride, accumulate, nplanes,
+                               static_cast<uint32_t *>(Y), batch, st);
+}
+
+// Dual LPN of n blocks in place: transpose to 128 planes, encode, transpose back.
+static int eng_dual_lpn(const QcEngine &g, int e, const void *ahat, cuot_block *io_d, uint8_t *planes, void *Y,
+                        int batch, cudaStream_t st) {
+  const uint64_t n = 1ull << e;
+  uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
+  CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
+  CUOT_TRY(eng_encode(g, ahat, pl, pl, n / 64, 0, 128, Y, batch, st));
+  return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
+}
+
+// Rate-1/2 dual LPN: out[i] = in[i] ^ (a * in[n..2n))[i] blockwise, i < n.
+// planes: 128 planes of 2n bits (stride n/32 words).
+static int eng_dual_lpn_r2(const QcEngine &g, int e, const void *ahat, const cuot_block *in_d, cuot_block *out_d,
+                           uint8_t *planes, void *Y, int batch, cudaStream_t st) {
+  const uint64_t n = 1ull << e;
+  uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
+  CUOT_TRY(transpose_launch(in_d, 2 * n, 16, 0, 128, planes, st));
+  CUOT_TRY(eng_encode(g, ahat, pl + n / 64, pl, n / 32, 1, 128, Y, batch, st));
+  return transpose_launch(planes, 128, n / 4, 0, n, out_d, st);
+}
+
+// ---- helpers for the batched engine (batch.cu) ----------------------------
+int qc_prepare(cuot_ctx *ctx, int e) {
+  QcEngine g;
+  return engine(ctx, e, use_fft(ctx, e), &g);
+}
+
+uint64_t qc_ahat_bytes(const cuot_ctx *ctx, int e) { return (use_fft(ctx, e) ? 16ull : 8ull) << e; }
+
+uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch) { return y_bytes(use_fft(ctx, e), e, batch); }
+
+int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
+  QcEngine g;
+  CUOT_TRY(engine(ctx, e, use_fft(ctx, e), &g));
+  return eng_ahat(g, a_d, Y, ahat, st);
 }
 
 // Encodes `njobs` consecutive groups of 128 planes in place; group j uses
-// ahats[j] (host array of device pointers).  Y holds `batch` planes.
-int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const uint2 *const *ahats,
-                   uint32_t *Y, int batch, cudaStream_t st) {
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  const int N1 = 1 << t->e1, N2 = 1 << t->e2;
+// ahats[j] (host array of device pointers).  Y holds qc_y_bytes(batch).
+int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void *const *ahats, void *Y,
+                   int batch, cudaStream_t st) {
+  QcEngine g;
+  CUOT_TRY(engine(ctx, e, use_fft(ctx, e), &g));
   const uint64_t n = 1ull << e;
   const int nplanes = 128 * njobs;
   // a launch may span at most kAhatTab jobs
   if (batch > 128 * (kAhatTab - 1)) batch = 128 * (kAhatTab - 1);
+  if (g.fft) batch = (batch + 3) & ~3;
   int launches = 0;
   for (int p0 = 0; p0 < nplanes; p0 += batch) {
     const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
     uint64_t *pl = planes + uint64_t(p0) * (n / 64);
+    if (g.fft) {
+      QcfAhatTab tab{};
+      tab.per = 32;
+      tab.first = (p0 % 128) / 4;
+      for (int j = 0; j < 16 && p0 / 128 + j < njobs; j++) tab.p[j] = ahats[p0 / 128 + j];
+      CUOT_TRY(qcf_encode(g.f, tab, pl, pl, n / 64, 0, nb, Y, nb, st));
+      continue;
+    }
+    const int N1 = 1 << g.t->e1, N2 = 1 << g.t->e2;
     AhatTab tab{};
     tab.per = 128;
     tab.first = p0 % 128;
-    for (int j = 0; j < kAhatTab && p0 / 128 + j < njobs; j++) tab.p[j] = ahats[p0 / 128 + j];
-    launch_col_fwd(t, dim3(N2 / kCW, nb), st, reinterpret_cast<const uint32_t *>(pl), n / 32, Y);
-    launch_row(t, dim3(N1 / row_rows(t), nb), st, Y, tab, 0);
-    launch_col_inv(t, dim3(N2 / kCW, nb), st, Y, reinterpret_cast<uint8_t *>(pl), n / 8);
+    for (int j = 0; j < kAhatTab && p0 / 128 + j < njobs; j++) tab.p[j] = static_cast<const uint2 *>(ahats[p0 / 128 + j]);
+    launch_col_fwd(g.t, dim3(N2 / kCW, nb), st, reinterpret_cast<const uint32_t *>(pl), n / 32,
+                   static_cast<uint32_t *>(Y));
+    launch_row(g.t, dim3(N1 / row_rows(g.t), nb), st, static_cast<uint32_t *>(Y), tab, 0);
+    launch_col_inv(g.t, dim3(N2 / kCW, nb), st, static_cast<const uint32_t *>(Y), reinterpret_cast<uint8_t *>(pl),
+                   n / 8);
     launches += 3;
   }
   return launch_status(launches);
@@ -777,7 +844,8 @@ struct cuot_qc_plan {
   cuot_ctx *ctx;
   int e;
   uint64_t n;
-  uint2 *ahat;
+  bool fft;
+  void *ahat;
   int batch;
 };
 
@@ -810,19 +878,16 @@ int cuot_qc_plan_create(cuot_ctx *ctx, const uint64_t *a_d, uint64_t n, void *st
   *out = nullptr;
   int e;
   CUOT_TRY(check_n(n, &e));
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  CUOT_TRY(set_attrs(t));
-  cuot_qc_plan *pl = new cuot_qc_plan{ctx, e, n, nullptr, 0};
-  int st = dev_alloc((void **)&pl->ahat, n * 8);
-  if (st != CUOT_OK) { delete pl; return st; }
-  void *scr;
-  st = scratch(ctx, n * 4, &scr);
-  if (st == CUOT_OK)
-    st = build_ahat(t, a_d, static_cast<uint32_t *>(scr), pl->ahat, static_cast<cudaStream_t>(stream));
+  DeviceGuard dg(ctx);
+  cuot_qc_plan *pl = new cuot_qc_plan{ctx, e, n, use_fft(ctx, e), nullptr, 0};
+  QcEngine g;
+  int st = engine(ctx, e, pl->fft, &g);
+  if (st == CUOT_OK) st = dev_alloc(&pl->ahat, (pl->fft ? 16 : 8) * n);
+  void *scr = nullptr;
+  if (st == CUOT_OK) st = scratch(ctx, y_bytes(pl->fft, e, 1), &scr);
+  if (st == CUOT_OK) st = eng_ahat(g, a_d, scr, pl->ahat, static_cast<cudaStream_t>(stream));
   if (st != CUOT_OK) {
-    cudaFree(pl->ahat);
+    if (pl->ahat) cudaFree(pl->ahat);
     delete pl;
     return st;
   }
@@ -848,47 +913,43 @@ int cuot_qc_plan_set_batch(cuot_qc_plan *pl, int planes_per_batch) {
 int cuot_qc_plan_encode(cuot_qc_plan *pl, uint64_t *planes_io_d, int nplanes, void *stream) {
   if (!pl || !planes_io_d || nplanes < 1) return fail(CUOT_EINVAL, "bad argument");
   cuot_ctx *ctx = pl->ctx;
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, pl->e, &t));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  CUOT_TRY(engine(ctx, pl->e, pl->fft, &g));
   const int batch = pl->batch < nplanes ? pl->batch : nplanes;
   void *scr;
-  CUOT_TRY(scratch(ctx, uint64_t(batch) * pl->n * 4, &scr));
-  return encode_planes(t, pl->ahat, planes_io_d, nplanes, static_cast<uint32_t *>(scr), batch,
-                       static_cast<cudaStream_t>(stream));
+  CUOT_TRY(scratch(ctx, y_bytes(pl->fft, pl->e, batch), &scr));
+  return eng_encode(g, pl->ahat, planes_io_d, planes_io_d, pl->n / 64, 0, nplanes, scr, batch,
+                    static_cast<cudaStream_t>(stream));
 }
 
 int cuot_qc_plan_dual_lpn(cuot_qc_plan *pl, cuot_block *io_d, void *stream) {
   if (!pl || !io_d) return fail(CUOT_EINVAL, "bad argument");
   cuot_ctx *ctx = pl->ctx;
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, pl->e, &t));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  CUOT_TRY(engine(ctx, pl->e, pl->fft, &g));
   const uint64_t n = pl->n;
   const int batch = pl->batch < 128 ? pl->batch : 128;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 16 + uint64_t(batch) * n * 4, &scr));
+  CUOT_TRY(scratch(ctx, n * 16 + y_bytes(pl->fft, pl->e, batch), &scr));
   uint8_t *planes = static_cast<uint8_t *>(scr);
-  uint32_t *Y = reinterpret_cast<uint32_t *>(planes + n * 16);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
-  CUOT_TRY(encode_planes(t, pl->ahat, reinterpret_cast<uint64_t *>(planes), 128, Y, batch, st));
-  return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
+  return eng_dual_lpn(g, pl->e, pl->ahat, io_d, planes, planes + n * 16, batch, static_cast<cudaStream_t>(stream));
 }
 
 int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *pl, const cuot_block *in_d, cuot_block *out_d, void *stream) {
   if (!pl || !in_d || !out_d) return fail(CUOT_EINVAL, "bad argument");
   cuot_ctx *ctx = pl->ctx;
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, pl->e, &t));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  CUOT_TRY(engine(ctx, pl->e, pl->fft, &g));
   const uint64_t n = pl->n;
   const int batch = pl->batch < 128 ? pl->batch : 128;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 32 + uint64_t(batch) * n * 4, &scr));
+  CUOT_TRY(scratch(ctx, n * 32 + y_bytes(pl->fft, pl->e, batch), &scr));
   uint8_t *planes = static_cast<uint8_t *>(scr);
-  return dual_lpn_r2(t, pl->ahat, in_d, out_d, planes, reinterpret_cast<uint32_t *>(planes + n * 32), batch,
-                     static_cast<cudaStream_t>(stream));
+  return eng_dual_lpn_r2(g, pl->e, pl->ahat, in_d, out_d, planes, planes + n * 32, batch,
+                         static_cast<cudaStream_t>(stream));
 }
 
 int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, uint64_t n,
@@ -896,19 +957,19 @@ int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, ui
   if (!ctx || !a_d || !planes_io_d || nplanes < 1) return fail(CUOT_EINVAL, "bad argument");
   int e;
   CUOT_TRY(check_n(n, &e));
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  CUOT_TRY(set_attrs(t));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  const bool fft = use_fft(ctx, e);
+  CUOT_TRY(engine(ctx, e, fft, &g));
   int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, nplanes);
   if (batch > nplanes) batch = nplanes;
+  const uint64_t ab = (fft ? 16 : 8) * n;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 8 + uint64_t(batch) * n * 4, &scr));
-  uint2 *ahat = static_cast<uint2 *>(scr);
-  uint32_t *Y = reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(scr) + n * 8);
+  CUOT_TRY(scratch(ctx, ab + y_bytes(fft, e, batch), &scr));
+  void *Y = static_cast<uint8_t *>(scr) + ab;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(build_ahat(t, a_d, Y, ahat, st));
-  return encode_planes(t, ahat, planes_io_d, nplanes, Y, batch, st);
+  CUOT_TRY(eng_ahat(g, a_d, Y, scr, st));
+  return eng_encode(g, scr, planes_io_d, planes_io_d, n / 64, 0, nplanes, Y, batch, st);
 }
 
 int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d, uint64_t n,
@@ -916,22 +977,19 @@ int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d, uint
   if (!ctx || !a_d || !io_d) return fail(CUOT_EINVAL, "bad argument");
   int e;
   CUOT_TRY(check_n(n, &e));
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  CUOT_TRY(set_attrs(t));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  const bool fft = use_fft(ctx, e);
+  CUOT_TRY(engine(ctx, e, fft, &g));
   int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
   if (batch > 128) batch = 128;
+  const uint64_t ab = (fft ? 16 : 8) * n;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 8 + n * 16 + uint64_t(batch) * n * 4, &scr));
-  uint2 *ahat = static_cast<uint2 *>(scr);
-  uint8_t *planes = static_cast<uint8_t *>(scr) + n * 8;
-  uint32_t *Y = reinterpret_cast<uint32_t *>(planes + n * 16);
+  CUOT_TRY(scratch(ctx, ab + n * 16 + y_bytes(fft, e, batch), &scr));
+  uint8_t *planes = static_cast<uint8_t *>(scr) + ab;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(build_ahat(t, a_d, Y, ahat, st));
-  CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
-  CUOT_TRY(encode_planes(t, ahat, reinterpret_cast<uint64_t *>(planes), 128, Y, batch, st));
-  return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
+  CUOT_TRY(eng_ahat(g, a_d, planes + n * 16, scr, st));
+  return eng_dual_lpn(g, e, scr, io_d, planes, planes + n * 16, batch, st);
 }
 
 int cuot_sot_dual_lpn_r2(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *in_d, uint64_t n,
@@ -939,20 +997,19 @@ int cuot_sot_dual_lpn_r2(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *i
   if (!ctx || !a_d || !in_d || !out_d) return fail(CUOT_EINVAL, "bad argument");
   int e;
   CUOT_TRY(check_n(n, &e));
-  DeviceGuard g(ctx);
-  QcTables *t;
-  CUOT_TRY(get_tables(ctx, e, &t));
-  CUOT_TRY(set_attrs(t));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  const bool fft = use_fft(ctx, e);
+  CUOT_TRY(engine(ctx, e, fft, &g));
   int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
   if (batch > 128) batch = 128;
+  const uint64_t ab = (fft ? 16 : 8) * n;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 8 + n * 32 + uint64_t(batch) * n * 4, &scr));
-  uint2 *ahat = static_cast<uint2 *>(scr);
-  uint8_t *planes = static_cast<uint8_t *>(scr) + n * 8;
-  uint32_t *Y = reinterpret_cast<uint32_t *>(planes + n * 32);
+  CUOT_TRY(scratch(ctx, ab + n * 32 + y_bytes(fft, e, batch), &scr));
+  uint8_t *planes = static_cast<uint8_t *>(scr) + ab;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(build_ahat(t, a_d, Y, ahat, st));
-  return dual_lpn_r2(t, ahat, in_d, out_d, planes, Y, batch, st);
+  CUOT_TRY(eng_ahat(g, a_d, planes + n * 32, scr, st));
+  return eng_dual_lpn_r2(g, e, scr, in_d, out_d, planes, planes + n * 32, batch, st);
 }
 
 int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *pos_d, int weight,

@@ -1,0 +1,612 @@
+// qc_fft.cu -- exact quasi-cyclic encode through a double-precision complex
+// FFT (the default backend for n = 2^e, 10 <= e <= 20).
+//
+// out_r = a * e_r mod (x^n - 1) over GF(2) is the parity of the integer
+// cyclic convolution, whose coefficients lie in [0, n] (n <= 2^20 < 2^21).
+// Four planes share one complex transform:
+//   x_j = (e0_j + 2^21 e1_j) + i (e2_j + 2^21 e3_j),
+// and since `a` is real, IFFT(FFT(x) . FFT(a)) = (a*e0 + 2^21 a*e1) + i (a*e2
+// + 2^21 a*e3): every product coefficient is an integer below 2^42 whose
+// bits 0 and 21 are the coefficients of two planes.  The computed values
+// differ from those integers by less than 1/2, so rounding recovers them
+// exactly: by the error bound for FFT-based convolution (Percival,
+// "Rapid multiplication modulo the sum and difference of highly composite
+// numbers", Math. Comp. 72 (2003), Thm. 5.1) the error is at most
+// ||x||_2 ||a||_2 ((1+eps)^{3m} (1+eps sqrt5)^{3m+1} (1+beta)^{3m} - 1) with
+// m = log2 n = 20, eps = 2^-53 and twiddle error beta <= 4 eps, i.e. below
+// 2^41.5 * 436 * 2^-53 < 0.16 for n = 2^20 (smaller n: smaller bound).
+//
+// Work per plane and radix-2 stage is one fp64 operation (a complex
+// butterfly shared by four planes), against several integer instructions
+// per plane in the number-theoretic transform of qc.cu.
+//
+// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= N2 = 2^e2 <= 1024), input
+// index j = N2*j1 + j2, frequency k = k1 + N1*k2:
+//   A (columns): 8 columns j2 of one transform per CTA: load the plane bits,
+//     N1-point DIF FFT over j1 (frequencies land in bit-reversed row order r),
+//     multiply by w_n^(j2 * rev(r)), store Y[r][j2].
+//   B (rows): 8 rows per CTA: N2-point DIF FFT, multiply by A_hat (the
+//     transform of `a` in the same layout, scaled by 1/n), N2-point DIT
+//     inverse, store.
+//   C (columns): multiply by w_n^-(j2 * rev(r)), N1-point DIT inverse over r,
+//     round, extract the four planes' bits, store (or XOR) 8 columns per byte.
+// An N-point transform runs in shared memory as 2-3 passes of 2^K-point
+// butterflies in registers (K <= 4, constant internal twiddles), each pass
+// followed by one multiplication with w_S^(base * q) from a table.  The 8
+// transforms of a CTA sit in rows of N + 1 complex values and the 8 lanes of
+// each quarter-warp work on the same item of the 8 transforms, so every
+// shared-memory access is conflict-free.
+#include "ctx.cuh"
+
+namespace cuot {
+
+constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
+
+// Radix plan of an N = 2^L point transform, 5 <= L <= 10: K bits per pass.
+__host__ __device__ constexpr int qcf_npass(int L) { return L <= 8 ? 2 : 3; }
+__host__ __device__ constexpr int qcf_k(int L, int p) {
+  return L == 5 ? (p == 0 ? 3 : 2)
+       : L == 6 ? 3
+       : L == 7 ? (p == 0 ? 4 : 3)
+       : L == 8 ? 4
+       : L == 9 ? 3
+       : (p == 0 ? 4 : 3);
+}
+// log2 of the sub-transform size at the start of pass p
+__host__ __device__ constexpr int qcf_ls(int L, int p) { return p == 0 ? L : qcf_ls(L, p - 1) - qcf_k(L, p - 1); }
+__host__ __device__ constexpr int qcf_threads(int L) { return L >= 10 ? 512 : L == 9 ? 256 : L == 8 ? 128 : 64; }
+// four-step factor tables per column: 2^lo + 2^(e1 - lo) entries (global
+// row stride), staged with an odd row stride so the 8 columns of a
+// quarter-warp hit distinct banks
+__host__ __device__ constexpr int qcf_fs_lo(int e1) { return (e1 + 1) / 2; }
+__host__ __device__ constexpr int qcf_fs_width(int e1) { return (1 << qcf_fs_lo(e1)) + (1 << (e1 - qcf_fs_lo(e1))); }
+__host__ __device__ constexpr int qcf_fs_ld(int e1) { return qcf_fs_width(e1) + 1; }
+constexpr int kCols = 8;  // transforms (columns or rows) per CTA
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// a * w
+__device__ __forceinline__ double2 cmul(double2 a, double2 w) {
+  return make_double2(fma(a.x, w.x, -(a.y * w.y)), fma(a.x, w.y, a.y * w.x));
+}
+// a * conj(w)
+__device__ __forceinline__ double2 cmulc(double2 a, double2 w) {
+  return make_double2(fma(a.x, w.x, a.y * w.y), fma(a.y, w.x, -(a.x * w.y)));
+}
+
+// cos(2 pi J / 16) and sin(2 pi J / 16) for J in [0, 8)
+__device__ __forceinline__ constexpr double c16(int J) {
+  return J == 0 ? 1.0
+       : J == 1 ? 0.92387953251128675613
+       : J == 2 ? 0.70710678118654752440
+       : J == 3 ? 0.38268343236508977173
+       : J == 4 ? 0.0
+       : J == 5 ? -0.38268343236508977173
+       : J == 6 ? -0.70710678118654752440
+                : -0.92387953251128675613;
+}
+__device__ __forceinline__ constexpr double s16(int J) { return c16(J >= 4 ? J - 4 : 4 - J); }
+
+// v * w16^J (forward, w16 = exp(-2 pi i / 16)) or v * conj(w16^J) (INV),
+// J in [0, 8); J is a compile-time constant after unrolling.
+template <bool INV>
+__device__ __forceinline__ double2 wmul16(double2 v, int J) {
+  constexpr double r = 0.70710678118654752440;
+  if (J == 0) return v;
+  if (J == 4) return INV ? make_double2(-v.y, v.x) : make_double2(v.y, -v.x);
+  if (J == 2) return INV ? make_double2((v.x - v.y) * r, (v.x + v.y) * r) : make_double2((v.x + v.y) * r, (v.y - v.x) * r);
+  if (J == 6) return INV ? make_double2(-(v.x + v.y) * r, (v.x - v.y) * r) : make_double2((v.y - v.x) * r, -(v.x + v.y) * r);
+  const double c = c16(J), s = s16(J);
+  return INV ? make_double2(fma(v.x, c, -(v.y * s)), fma(v.y, c, v.x * s))
+             : make_double2(fma(v.x, c, v.y * s), fma(v.y, c, -(v.x * s)));
+}
+
+// 2^K-point DFT in registers, natural order in, bit-reversed order out.
+template <int K>
+__device__ __forceinline__ void dif_regs(double2 (&x)[1 << K]) {
+  constexpr int R = 1 << K;
+#pragma unroll
+  for (int t = 0; t < K; t++) {
+    const int h = R >> (t + 1);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      if (m & h) continue;
+      const double2 u = x[m], v = x[m + h];
+      x[m] = cadd(u, v);
+      x[m + h] = wmul16<false>(csub(u, v), (m & (h - 1)) * (8 / h));
+    }
+  }
+}
+// Its inverse (times 2^K): bit-reversed order in, natural order out.
+template <int K>
+__device__ __forceinline__ void dit_regs(double2 (&x)[1 << K]) {
+  constexpr int R = 1 << K;
+#pragma unroll
+  for (int t = K - 1; t >= 0; t--) {
+    const int h = R >> (t + 1);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      if (m & h) continue;
+      const double2 u = x[m], v = wmul16<true>(x[m + h], (m & (h - 1)) * (8 / h));
+      x[m] = cadd(u, v);
+      x[m + h] = csub(u, v);
+    }
+  }
+}
+
+// Item w of pass P over an N = 2^L point transform: 2^K elements
+// blk*S + base + M*m (S = 2^LS, M = S / 2^K).
+template <int L, int P>
+struct Pass {
+  static constexpr int K = qcf_k(L, P), R = 1 << K, LS = qcf_ls(L, P), M = (1 << LS) >> K;
+  static constexpr int items = (1 << L) >> K;
+  __device__ static int first(int w) { return ((w / M) << LS) + (w % M); }
+  __device__ static int base(int w) { return w % M; }
+};
+
+// Twiddles of a DIF pass after its butterflies: x[m] holds frequency
+// q = rev_K(m) of its sub-transform; multiply by w_S^(base q) = T[base q 2^(L-LS)].
+template <int L, int P, bool INV>
+__device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int base, const double2 *T) {
+  using Q = Pass<L, P>;
+  if (Q::M == 1) return;
+#pragma unroll
+  for (int m = 1; m < Q::R; m++) {
+    const int q = __brev(m) >> (32 - Q::K);
+    const double2 w = T[(base * q) << (L - Q::LS)];
+    x[m] = INV ? cmulc(x[m], w) : cmul(x[m], w);
+  }
+}
+
+// One pass entirely in shared memory (xs rows of ld complex values).
+template <int L, int P, bool INV>
+__device__ __forceinline__ void smem_pass(double2 *xs, int ld, const double2 *T) {
+  using Q = Pass<L, P>;
+  for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+    const int c = it & (kCols - 1), w = it / kCols;
+    double2 *row = xs + c * ld + Q::first(w);
+    double2 x[Q::R];
+#pragma unroll
+    for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
+    if (!INV) {
+      dif_regs<Q::K>(x);
+      pass_twiddle<L, P, false>(x, Q::base(w), T);
+    } else {
+      pass_twiddle<L, P, true>(x, Q::base(w), T);
+      dit_regs<Q::K>(x);
+    }
+#pragma unroll
+    for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
+  }
+}
+
+// Middle passes [1, npass - 1) forward, or in reverse order inverse.
+template <int L, bool INV>
+__device__ __forceinline__ void middle_passes(double2 *xs, int ld, const double2 *T) {
+  if constexpr (qcf_npass(L) == 3) {
+    __syncthreads();
+    smem_pass<L, 1, INV>(xs, ld, T);
+  }
+  __syncthreads();
+}
+
+// w_n^(j2 * k1) for the CTA's column c and k1 = rev_e1(r), from the column's
+// two factor tables in shared memory.
+template <int E1>
+__device__ __forceinline__ double2 fourstep_w(const double2 *fs, int c, int r) {
+  constexpr int lo = qcf_fs_lo(E1), W = qcf_fs_ld(E1);
+  const int k1 = __brev(r) >> (32 - E1);
+  return cmul(fs[c * W + (k1 & ((1 << lo) - 1))], fs[c * W + (1 << lo) + (k1 >> lo)]);
+}
+
+__device__ __forceinline__ void stage(double2 *dst, const double2 *src, int cnt) {
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = __ldg(&src[i]);
+}
+// The 8 columns' four-step factor rows (global stride W) into rows of W + 1.
+template <int E1>
+__device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0) {
+  constexpr int W = qcf_fs_width(E1);
+  const double2 *src = fs + uint64_t(c0) * W;
+  for (int i = threadIdx.x; i < kCols * W; i += blockDim.x) dst[(i / W) * (W + 1) + i % W] = __ldg(&src[i]);
+}
+
+// Pass A.  grid (N2 / 8, transforms).  in: plane p at in + p * stride_bytes;
+// transform y holds planes 4y .. 4y+3 (< nplanes); one_plane: `a` (real
+// part only).
+template <int E1>
+__global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
+    const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2,
+    const double2 *__restrict__ T1, const double2 *__restrict__ fs, double2 *__restrict__ Y) {
+  constexpr int N1 = 1 << E1, ld = N1 + 1, W = qcf_fs_ld(E1);
+  constexpr int NP = qcf_npass(E1);
+  extern __shared__ double2 sm[];
+  double2 *xs = sm, *Ts = xs + kCols * ld, *fss = Ts + N1;
+  uint32_t *bits = reinterpret_cast<uint32_t *>(fss + kCols * W);
+  const int c0 = blockIdx.x * kCols;
+  const int p0 = 4 * blockIdx.y;
+  stage(Ts, T1, N1);
+  stage_fs<E1>(fss, fs, c0);
+  for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
+    const uint64_t byte = ((uint64_t(j1) << e2) | uint64_t(c0)) >> 3;
+    uint32_t word = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (p0 + q < nplanes) word |= uint32_t(__ldg(in + uint64_t(p0 + q) * stride_bytes + byte)) << (8 * q);
+    bits[j1] = word;
+  }
+  __syncthreads();
+  {  // pass 0 from the bits
+    using Q = Pass<E1, 0>;
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) {
+        const uint32_t b = bits[i0 + Q::M * m] >> c;
+        if (one_plane) {
+          x[m] = make_double2(double(b & 1u), 0.0);
+        } else {
+          x[m] = make_double2(double((b & 1u) | ((b >> 8) & 1u) << 21), double(((b >> 16) & 1u) | ((b >> 24) & 1u) << 21));
+        }
+      }
+      dif_regs<Q::K>(x);
+      pass_twiddle<E1, 0, false>(x, Q::base(w), Ts);
+      double2 *row = xs + c * ld + i0;
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
+    }
+  }
+  middle_passes<E1, false>(xs, ld, Ts);
+  {  // last pass (M = 1), then the four-step twiddle, to global
+    using Q = Pass<E1, NP - 1>;
+    static_assert(Q::M == 1, "last pass");
+    double2 *Yp = Y + (uint64_t(blockIdx.y) << (E1 + e2));
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + i0 + m];
+      dif_regs<Q::K>(x);
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) {
+        const int r = i0 + m;
+        Yp[(uint64_t(r) << e2) + c0 + c] = cmul(x[m], fourstep_w<E1>(fss, c, r));
+      }
+    }
+  }
+}
+
+// Pass B.  grid (N1 / 8, transforms).  mode 0: forward, pointwise by the
+// transform's A_hat (ahat.p[(ahat.first + y) / ahat.per]), inverse, in place.
+// mode 1: forward only, times `scale`, written to `out` (builds A_hat).
+template <int E2>
+__global__ void __launch_bounds__(qcf_threads(E2), 1) qcf_row(
+    double2 *__restrict__ Y, int e1, const double2 *__restrict__ T2, QcfAhatTab ahat, int mode,
+    double2 *__restrict__ out, double scale) {
+  constexpr int N2 = 1 << E2, ld = N2 + 1;
+  constexpr int NP = qcf_npass(E2);
+  extern __shared__ double2 sm[];
+  double2 *xs = sm, *Ts = xs + kCols * ld;
+  const int r0 = blockIdx.x * kCols;
+  stage(Ts, T2, N2);
+  double2 *Yp = Y + (uint64_t(blockIdx.y) << (e1 + E2)) + (uint64_t(r0) << E2);
+  __syncthreads();
+  {  // pass 0 from global
+    using Q = Pass<E2, 0>;
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      const double2 *src = Yp + (uint64_t(c) << E2) + i0;
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = src[Q::M * m];
+      dif_regs<Q::K>(x);
+      pass_twiddle<E2, 0, false>(x, Q::base(w), Ts);
+      double2 *row = xs + c * ld + i0;
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
+    }
+  }
+  middle_passes<E2, false>(xs, ld, Ts);
+  {  // last forward pass; pointwise product; first inverse pass
+    using Q = Pass<E2, NP - 1>;
+    const double2 *ah = mode == 0 ? static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
+                                        (uint64_t(r0) << E2)
+                                  : nullptr;
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + i0 + m];
+      dif_regs<Q::K>(x);
+      if (mode == 1) {
+        double2 *o = out + (uint64_t(r0 + c) << E2) + i0;
+#pragma unroll
+        for (int m = 0; m < Q::R; m++) o[m] = make_double2(x[m].x * scale, x[m].y * scale);
+        continue;
+      }
+      const double2 *a = ah + (uint64_t(c) << E2) + i0;
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m]));
+      dit_regs<Q::K>(x);
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
+    }
+  }
+  if (mode == 1) return;
+  middle_passes<E2, true>(xs, ld, Ts);
+  {  // inverse of pass 0, to global
+    using Q = Pass<E2, 0>;
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      const double2 *row = xs + c * ld + i0;
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
+      pass_twiddle<E2, 0, true>(x, Q::base(w), Ts);
+      dit_regs<Q::K>(x);
+      double2 *dst = Yp + (uint64_t(c) << E2) + i0;
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) dst[Q::M * m] = x[m];
+    }
+  }
+}
+
+// Pass C.  grid (N2 / 8, transforms).  out: plane p at out + p * stride_bytes,
+// written (accumulate == 0) or XORed into (accumulate == 1).
+template <int E1>
+__global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_inv(
+    const double2 *__restrict__ Y, int e2, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
+    uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate) {
+  constexpr int N1 = 1 << E1, ld = N1 + 1;
+  constexpr int NP = qcf_npass(E1);
+  extern __shared__ double2 sm[];
+  double2 *xs = sm, *Ts = xs + kCols * ld, *fss = Ts + N1;
+  const int c0 = blockIdx.x * kCols;
+  const int p0 = 4 * blockIdx.y;
+  stage(Ts, T1, N1);
+  stage_fs<E1>(fss, fs, c0);
+  __syncthreads();
+  {  // inverse of the last pass, from global
+    using Q = Pass<E1, NP - 1>;
+    const double2 *Yp = Y + (uint64_t(blockIdx.y) << (E1 + e2));
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) {
+        const int r = i0 + m;
+        x[m] = cmulc(Yp[(uint64_t(r) << e2) + c0 + c], fourstep_w<E1>(fss, c, r));
+      }
+      dit_regs<Q::K>(x);
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
+    }
+  }
+  middle_passes<E1, true>(xs, ld, Ts);
+  {  // inverse of pass 0; round; the 8 columns' bits of each plane form a byte
+    using Q = Pass<E1, 0>;
+    const int lane = threadIdx.x & 31;
+    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
+      const int c = it & (kCols - 1), w = it / kCols;
+      const int i0 = Q::first(w);
+      const double2 *row = xs + c * ld + i0;
+      double2 x[Q::R];
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
+      pass_twiddle<E1, 0, true>(x, Q::base(w), Ts);
+      dit_regs<Q::K>(x);
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) {
+        // round(v) mod 2^32 is the low word of v + 1.5 * 2^52
+        const uint32_t re = uint32_t(__double2loint(x[m].x + kRoundMagic));
+        const uint32_t im = uint32_t(__double2loint(x[m].y + kRoundMagic));
+        const uint32_t pl[4] = {re & 1u, (re >> 21) & 1u, im & 1u, (im >> 21) & 1u};
+        const uint64_t byte = ((uint64_t(i0 + Q::M * m) << e2) | uint64_t(c0)) >> 3;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint32_t mask = __ballot_sync(0xffffffffu, pl[q]);
+          if (c == 0 && p0 + q < nplanes) {
+            const uint8_t v = uint8_t(mask >> (lane & ~7));
+            uint8_t *o = out + uint64_t(p0 + q) * stride_bytes + byte;
+            *o = accumulate ? uint8_t(*o ^ v) : v;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Table generation (one-time per n).  T[k] = w_N^k, k < N.
+__global__ void qcf_gen_roots(int L, double2 *T) {
+  const int N = 1 << L;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * double(k) / double(N), &s, &c);
+    T[k] = make_double2(c, -s);
+  }
+}
+// fs[j2][u] = w_n^(j2 u) (u < 2^lo), fs[j2][2^lo + v] = w_n^(j2 v 2^lo).
+__global__ void qcf_gen_fourstep(int e1, int e2, double2 *fs) {
+  const int lo = qcf_fs_lo(e1), W = qcf_fs_width(e1);
+  const uint64_t n = 1ull << (e1 + e2), N2 = 1ull << e2;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N2 * W;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t j2 = i / W, u = i % W;
+    const uint64_t k = u < (1u << lo) ? u : (u - (1u << lo)) << lo;
+    const uint64_t m = (j2 * k) & (n - 1);
+    double s, c;
+    sincospi(2.0 * double(m) / double(n), &s, &c);
+    fs[i] = make_double2(c, -s);
+  }
+}
+
+struct QcfTables {
+  int e, e1, e2;
+  double2 *T1, *T2, *fs;
+};
+
+namespace {
+
+int qcf_alloc(void **p, size_t bytes) {
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(CUOT_ENOMEM, "QC FFT table allocation of %zu bytes failed", bytes);
+  }
+  return CUOT_OK;
+}
+
+void qcf_free(QcfTables *t) {
+  if (!t) return;
+  cudaFree(t->T1);
+  cudaFree(t->T2);
+  cudaFree(t->fs);
+  delete t;
+}
+
+int col_smem(int e1) {
+  const int N1 = 1 << e1;
+  return (kCols * (N1 + 1) + N1 + kCols * qcf_fs_ld(e1)) * 16 + N1 * 4;
+}
+int row_smem(int e2) {
+  const int N2 = 1 << e2;
+  return (kCols * (N2 + 1) + N2) * 16;
+}
+
+#define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10)
+
+int set_attrs() {
+  static bool done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && done[dev]) return CUOT_OK;
+  bool ok = true;
+#define QCF_SET(E)                                                                                     \
+  ok &= cudaFuncSetAttribute(qcf_col_fwd<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E)) == \
+        cudaSuccess;                                                                                   \
+  ok &= cudaFuncSetAttribute(qcf_col_inv<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E)) == \
+        cudaSuccess;                                                                                   \
+  ok &= cudaFuncSetAttribute(qcf_row<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem(E)) == cudaSuccess;
+  QCF_CASES(QCF_SET)
+#undef QCF_SET
+  if (!ok) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "QC FFT shared-memory attribute failed");
+  }
+  if (dev < 64) done[dev] = true;
+  return CUOT_OK;
+}
+
+void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t *in, uint64_t stride_bytes,
+                    int nplanes, int one_plane, double2 *Y) {
+  const dim3 grid((1u << t->e2) / kCols, ntr);
+  switch (t->e1) {
+#define QCF_L(E)                                                                                            \
+  case E:                                                                                                   \
+    qcf_col_fwd<E><<<grid, qcf_threads(E), col_smem(E), st>>>(in, stride_bytes, nplanes, one_plane, t->e2, \
+                                                               t->T1, t->fs, Y);                            \
+    break;
+    QCF_CASES(QCF_L)
+#undef QCF_L
+  }
+}
+void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const QcfAhatTab &ahat, int mode,
+                double2 *out, double scale) {
+  const dim3 grid((1u << t->e1) / kCols, ntr);
+  switch (t->e2) {
+#define QCF_L(E)                                                                                       \
+  case E:                                                                                              \
+    qcf_row<E><<<grid, qcf_threads(E), row_smem(E), st>>>(Y, t->e1, t->T2, ahat, mode, out, scale);   \
+    break;
+    QCF_CASES(QCF_L)
+#undef QCF_L
+  }
+}
+void launch_col_inv(const QcfTables *t, int ntr, cudaStream_t st, const double2 *Y, uint8_t *out,
+                    uint64_t stride_bytes, int nplanes, int accumulate) {
+  const dim3 grid((1u << t->e2) / kCols, ntr);
+  switch (t->e1) {
+#define QCF_L(E)                                                                                          \
+  case E:                                                                                                 \
+    qcf_col_inv<E><<<grid, qcf_threads(E), col_smem(E), st>>>(Y, t->e2, t->T1, t->fs, out, stride_bytes, \
+                                                               nplanes, accumulate);                      \
+    break;
+    QCF_CASES(QCF_L)
+#undef QCF_L
+  }
+}
+
+}  // namespace
+
+bool qcf_supported(int e) { return e >= 10 && e <= kQcfMaxE; }
+
+int qcf_get_tables(cuot_ctx *ctx, int e, QcfTables **out) {
+  if (!qcf_supported(e)) return fail(CUOT_ENOTSUP, "QC FFT backend: n = 2^%d outside [2^10, 2^%d]", e, kQcfMaxE);
+  if (ctx->qcf_tables[e]) {
+    *out = static_cast<QcfTables *>(ctx->qcf_tables[e]);
+    return CUOT_OK;
+  }
+  CUOT_TRY(set_attrs());
+  QcfTables *t = new QcfTables{};
+  t->e = e;
+  t->e1 = e / 2;
+  t->e2 = e - t->e1;
+  const uint64_t N1 = 1ull << t->e1, N2 = 1ull << t->e2;
+  int st = CUOT_OK;
+  if ((st = qcf_alloc((void **)&t->T1, N1 * 16)) || (st = qcf_alloc((void **)&t->T2, N2 * 16)) ||
+      (st = qcf_alloc((void **)&t->fs, N2 * qcf_fs_width(t->e1) * 16))) {
+    qcf_free(t);
+    return st;
+  }
+  qcf_gen_roots<<<8, 256>>>(t->e1, t->T1);
+  qcf_gen_roots<<<8, 256>>>(t->e2, t->T2);
+  qcf_gen_fourstep<<<256, 256>>>(t->e1, t->e2, t->fs);
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    qcf_free(t);
+    return fail(CUOT_ECUDA, "QC FFT table generation failed");
+  }
+  ctx->qcf_tables[e] = t;
+  *out = t;
+  return CUOT_OK;
+}
+
+void qcf_free_ctx_tables(cuot_ctx *ctx) {
+  for (int e = 0; e < 32; e++) {
+    qcf_free(static_cast<QcfTables *>(ctx->qcf_tables[e]));
+    ctx->qcf_tables[e] = nullptr;
+  }
+}
+
+int qcf_build_ahat(const QcfTables *t, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
+  const uint64_t n = 1ull << t->e;
+  launch_col_fwd(t, 1, st, reinterpret_cast<const uint8_t *>(a_d), n / 8, 1, 1, static_cast<double2 *>(Y));
+  launch_row(t, 1, st, static_cast<double2 *>(Y), QcfAhatTab{}, 1, static_cast<double2 *>(ahat), 1.0 / double(n));
+  return launch_status(2);
+}
+
+int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
+               int accumulate, int nplanes, void *Y, int batch, cudaStream_t st) {
+  batch = (batch + 3) & ~3;
+  int launches = 0;
+  for (int p0 = 0; p0 < nplanes; p0 += batch) {
+    const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
+    const int ntr = (nb + 3) / 4;
+    QcfAhatTab tab = ahat;
+    tab.first += p0 / 4;
+    launch_col_fwd(t, ntr, st, reinterpret_cast<const uint8_t *>(in + uint64_t(p0) * stride), stride * 8, nb, 0,
+                   static_cast<double2 *>(Y));
+    launch_row(t, ntr, st, static_cast<double2 *>(Y), tab, 0, nullptr, 0.0);
+    launch_col_inv(t, ntr, st, static_cast<const double2 *>(Y), reinterpret_cast<uint8_t *>(out + uint64_t(p0) * stride),
+                   stride * 8, nb, accumulate);
+    launches += 3;
+  }
+  return launch_status(launches);
+}
+
+}  // namespace cuot

@@ -52,9 +52,16 @@ uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
 /* Tuning knobs of the single-instance calls made on this context (the
  * autotuner in cuot_b200/autotune.py sets them from its measurements):
  *   CUOT_TUNE_PPRF_THREADS  threads per tree CTA, 128 or 256 (default 256)
- *   CUOT_TUNE_QC_PLANES     planes per NTT pass, 0 = automatic (~64 MiB) */
+ *   CUOT_TUNE_QC_PLANES     planes per QC pass, 0 = automatic (512 MiB of
+ *                           intermediate)
+ *   CUOT_TUNE_QC_BACKEND    transform of the exact QC encode: 0 automatic
+ *                           (fp64 FFT for n <= 2^20, else NTT), 1 NTT mod
+ *                           469762049, 2 FFT where n <= 2^20.  Plans and
+ *                           batches keep the backend they were created with;
+ *                           set it before creating them. */
 #define CUOT_TUNE_PPRF_THREADS 1
 #define CUOT_TUNE_QC_PLANES 2
+#define CUOT_TUNE_QC_BACKEND 3
 int cuot_ctx_set_tuning(cuot_ctx *ctx, int key, int64_t value);
 
 /* ---- AES-128 ECB ---------------------------------------------------------
