@@ -295,13 +295,13 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
     const int njobs = int(c.items.size()) * 2;
     for (int j = 0; j < njobs; j++) {
       const cuot_batch_item &it = b->items[c.items[j / 2]];
-      CUOT_TRY(transpose_launch(j % 2 ? it.w_d : it.v_d, n, 16, 0, 128, c.planes + uint64_t(j) * n * 16, st));
+      CUOT_TRY(qc_job_to_layout(ctx, c.e, j % 2 ? it.w_d : it.v_d, c.planes + uint64_t(j) * n * 16, st));
     }
     CUOT_TRY(qc_encode_jobs(ctx, c.e, reinterpret_cast<uint64_t *>(c.planes), njobs, c.ahats.data(), b->Y,
                             c.batch, st));
     for (int j = 0; j < njobs; j++) {
       const cuot_batch_item &it = b->items[c.items[j / 2]];
-      CUOT_TRY(transpose_launch(c.planes + uint64_t(j) * n * 16, 128, n / 8, 0, n, j % 2 ? it.w_d : it.v_d, st));
+      CUOT_TRY(qc_job_from_layout(ctx, c.e, c.planes + uint64_t(j) * n * 16, j % 2 ? it.w_d : it.v_d, st));
     }
     for (int i : c.items) {
       const cuot_batch_item &it = b->items[i];

@@ -46,6 +46,9 @@ uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch);
 int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st);
 int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void *const *ahats,
                    void *Y, int batch, cudaStream_t st);
+// n = 2^e blocks into a job's encode layout (16n bytes) and back.
+int qc_job_to_layout(const cuot_ctx *ctx, int e, const cuot_block *in, void *job, cudaStream_t st);
+int qc_job_from_layout(const cuot_ctx *ctx, int e, const void *job, cuot_block *out, cudaStream_t st);
 int qc_default_batch(uint64_t n, int nplanes);
 // FP64 FFT backend of the QC encode (qc_fft.cu): n = 2^e, 10 <= e <= kQcfMaxE.
 constexpr int kQcfMaxE = 20;
@@ -65,6 +68,14 @@ int qcf_build_ahat(const QcfTables *t, const uint64_t *a_d, void *Y, void *ahat,
 // written or XORed (accumulate); Y holds round4(batch) * 4n bytes.
 int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
                int accumulate, int nplanes, void *Y, int batch, cudaStream_t st);
+// The same encode on the tile layout (qcf_gather's output, 16n bytes per 32
+// transforms), in place; batch: planes per launch group.
+int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles, int ntransforms, void *Y,
+                     int batch, cudaStream_t st);
+// n = 2^e blocks -> tile layout of their 128 planes, and back (optionally
+// XORed with xor_in).
+int qcf_gather(int e, const cuot_block *in, uint32_t *tiles, cudaStream_t st);
+int qcf_scatter(int e, const uint32_t *tiles, const cuot_block *xor_in, cuot_block *out, cudaStream_t st);
 int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
                      uint64_t col_hi, void *out, cudaStream_t st);
 }  // namespace cuot

@@ -739,6 +739,13 @@ static int engine(cuot_ctx *ctx, int e, bool fft, QcEngine *g) {
   return set_attrs(g->t);
 }
 
+static QcfAhatTab single_tab(const void *ahat) {
+  QcfAhatTab tab{};
+  tab.p[0] = ahat;
+  tab.per = 1 << 30;
+  return tab;
+}
+
 // A_hat of `a` (NTT: n Shoup pairs; FFT: n complex doubles) using Y as scratch.
 static int eng_ahat(const QcEngine &g, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
   if (g.fft) return qcf_build_ahat(g.f, a_d, Y, ahat, st);
@@ -749,20 +756,22 @@ static int eng_ahat(const QcEngine &g, const uint64_t *a_d, void *Y, void *ahat,
 // written or XORed into (accumulate).
 static int eng_encode(const QcEngine &g, const void *ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
                       int accumulate, int nplanes, void *Y, int batch, cudaStream_t st) {
-  if (g.fft) {
-    QcfAhatTab tab{};
-    tab.p[0] = ahat;
-    tab.per = 1 << 30;
-    return qcf_encode(g.f, tab, in, out, stride, accumulate, nplanes, Y, batch, st);
-  }
+  if (g.fft) return qcf_encode(g.f, single_tab(ahat), in, out, stride, accumulate, nplanes, Y, batch, st);
   return encode_planes_strided(g.t, static_cast<const uint2 *>(ahat), in, out, stride, accumulate, nplanes,
                                static_cast<uint32_t *>(Y), batch, st);
 }
 
-// Dual LPN of n blocks in place: transpose to 128 planes, encode, transpose back.
+// Dual LPN of n blocks in place: transpose to 128 planes (the FFT: to its
+// tile layout), encode, transpose back.  planes: 16n bytes.
 static int eng_dual_lpn(const QcEngine &g, int e, const void *ahat, cuot_block *io_d, uint8_t *planes, void *Y,
                         int batch, cudaStream_t st) {
   const uint64_t n = 1ull << e;
+  if (g.fft) {
+    uint32_t *tiles = reinterpret_cast<uint32_t *>(planes);
+    CUOT_TRY(qcf_gather(e, io_d, tiles, st));
+    CUOT_TRY(qcf_encode_tiles(g.f, single_tab(ahat), tiles, 32, Y, batch, st));
+    return qcf_scatter(e, tiles, nullptr, io_d, st);
+  }
   uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
   CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
   CUOT_TRY(eng_encode(g, ahat, pl, pl, n / 64, 0, 128, Y, batch, st));
@@ -774,6 +783,12 @@ static int eng_dual_lpn(const QcEngine &g, int e, const void *ahat, cuot_block *
 static int eng_dual_lpn_r2(const QcEngine &g, int e, const void *ahat, const cuot_block *in_d, cuot_block *out_d,
                            uint8_t *planes, void *Y, int batch, cudaStream_t st) {
   const uint64_t n = 1ull << e;
+  if (g.fft) {
+    uint32_t *tiles = reinterpret_cast<uint32_t *>(planes);
+    CUOT_TRY(qcf_gather(e, in_d + n, tiles, st));
+    CUOT_TRY(qcf_encode_tiles(g.f, single_tab(ahat), tiles, 32, Y, batch, st));
+    return qcf_scatter(e, tiles, in_d, out_d, st);
+  }
   uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
   CUOT_TRY(transpose_launch(in_d, 2 * n, 16, 0, 128, planes, st));
   CUOT_TRY(eng_encode(g, ahat, pl + n / 64, pl, n / 32, 1, 128, Y, batch, st));
@@ -796,29 +811,45 @@ int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, void *Y, void *ahat
   return eng_ahat(g, a_d, Y, ahat, st);
 }
 
-// Encodes `njobs` consecutive groups of 128 planes in place; group j uses
-// ahats[j] (host array of device pointers).  Y holds qc_y_bytes(batch).
+int qc_job_to_layout(const cuot_ctx *ctx, int e, const cuot_block *in, void *job, cudaStream_t st) {
+  if (use_fft(ctx, e)) return qcf_gather(e, in, static_cast<uint32_t *>(job), st);
+  return transpose_launch(in, 1ull << e, 16, 0, 128, job, st);
+}
+
+int qc_job_from_layout(const cuot_ctx *ctx, int e, const void *job, cuot_block *out, cudaStream_t st) {
+  if (use_fft(ctx, e)) return qcf_scatter(e, static_cast<const uint32_t *>(job), nullptr, out, st);
+  return transpose_launch(job, 128, (1ull << e) / 8, 0, 1ull << e, out, st);
+}
+
+// Encodes `njobs` consecutive jobs (16n bytes each: 128 planes, or the FFT's
+// tile layout) in place; job j uses ahats[j] (host array of device
+// pointers).  Y holds qc_y_bytes(batch).
 int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void *const *ahats, void *Y,
                    int batch, cudaStream_t st) {
   QcEngine g;
   CUOT_TRY(engine(ctx, e, use_fft(ctx, e), &g));
   const uint64_t n = 1ull << e;
+  if (g.fft) {
+    int bt = batch < 4 ? 1 : batch / 4;
+    if (bt > 32 * 15) bt = 32 * 15;  // a launch may span at most 16 jobs
+    uint32_t *tiles = reinterpret_cast<uint32_t *>(planes);
+    for (int t0 = 0; t0 < 32 * njobs; t0 += bt) {
+      const int ntr = 32 * njobs - t0 < bt ? 32 * njobs - t0 : bt;
+      QcfAhatTab tab{};
+      tab.per = 32;
+      tab.first = t0 % 32;
+      for (int j = 0; j < 16 && t0 / 32 + j < njobs; j++) tab.p[j] = ahats[t0 / 32 + j];
+      CUOT_TRY(qcf_encode_tiles(g.f, tab, tiles + uint64_t(t0) * (n / 8), ntr, Y, 4 * ntr, st));
+    }
+    return CUOT_OK;
+  }
   const int nplanes = 128 * njobs;
   // a launch may span at most kAhatTab jobs
   if (batch > 128 * (kAhatTab - 1)) batch = 128 * (kAhatTab - 1);
-  if (g.fft) batch = (batch + 3) & ~3;
   int launches = 0;
   for (int p0 = 0; p0 < nplanes; p0 += batch) {
     const int nb = nplanes - p0 < batch ? nplanes - p0 : batch;
     uint64_t *pl = planes + uint64_t(p0) * (n / 64);
-    if (g.fft) {
-      QcfAhatTab tab{};
-      tab.per = 32;
-      tab.first = (p0 % 128) / 4;
-      for (int j = 0; j < 16 && p0 / 128 + j < njobs; j++) tab.p[j] = ahats[p0 / 128 + j];
-      CUOT_TRY(qcf_encode(g.f, tab, pl, pl, n / 64, 0, nb, Y, nb, st));
-      continue;
-    }
     const int N1 = 1 << g.t->e1, N2 = 1 << g.t->e2;
     AhatTab tab{};
     tab.per = 128;

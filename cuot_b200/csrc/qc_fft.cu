@@ -212,11 +212,14 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 
 // Pass A.  grid (N2 / 8, transforms).  in: plane p at in + p * stride_bytes;
 // transform y holds planes 4y .. 4y+3 (< nplanes); one_plane: `a` (real
-// part only).
+// part only).  With tiles != nullptr the input is in the tile layout
+// instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
+// columns of the CTA's tile in row j1 (qcf_gather).
 template <int E1>
 __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2,
-    const double2 *__restrict__ T1, const double2 *__restrict__ fs, double2 *__restrict__ Y) {
+    const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
+    double2 *__restrict__ Y) {
   constexpr int N1 = 1 << E1, ld = N1 + 1, W = qcf_fs_ld(E1);
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
@@ -226,13 +229,18 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
   const int p0 = 4 * blockIdx.y;
   stage(Ts, T1, N1);
   stage_fs<E1>(fss, fs, c0);
-  for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
-    const uint64_t byte = ((uint64_t(j1) << e2) | uint64_t(c0)) >> 3;
-    uint32_t word = 0;
+  if (tiles) {
+    const uint32_t *tp = tiles + (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + blockIdx.x;
+    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) bits[j1] = __ldg(tp + (uint64_t(j1) << (e2 - 3)));
+  } else {
+    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
+      const uint64_t byte = ((uint64_t(j1) << e2) | uint64_t(c0)) >> 3;
+      uint32_t word = 0;
 #pragma unroll
-    for (int q = 0; q < 4; q++)
-      if (p0 + q < nplanes) word |= uint32_t(__ldg(in + uint64_t(p0 + q) * stride_bytes + byte)) << (8 * q);
-    bits[j1] = word;
+      for (int q = 0; q < 4; q++)
+        if (p0 + q < nplanes) word |= uint32_t(__ldg(in + uint64_t(p0 + q) * stride_bytes + byte)) << (8 * q);
+      bits[j1] = word;
+    }
   }
   __syncthreads();
   {  // pass 0 from the bits
@@ -281,6 +289,9 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
 // Pass B.  grid (N1 / 8, transforms).  mode 0: forward, pointwise by the
 // transform's A_hat (ahat.p[(ahat.first + y) / ahat.per]), inverse, in place.
 // mode 1: forward only, times `scale`, written to `out` (builds A_hat).
+// A_hat is stored in the order the last pass consumes it: for the 8 rows
+// from r0, element m of item w of row c at r0 * N2 + (m * items + w) * 8 + c,
+// so each warp reads 512 contiguous bytes per load.
 template <int E2>
 __global__ void __launch_bounds__(qcf_threads(E2), 1) qcf_row(
     double2 *__restrict__ Y, int e1, const double2 *__restrict__ T2, QcfAhatTab ahat, int mode,
@@ -323,14 +334,14 @@ __global__ void __launch_bounds__(qcf_threads(E2), 1) qcf_row(
       for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + i0 + m];
       dif_regs<Q::K>(x);
       if (mode == 1) {
-        double2 *o = out + (uint64_t(r0 + c) << E2) + i0;
+        double2 *o = out + (uint64_t(r0) << E2) + it;
 #pragma unroll
-        for (int m = 0; m < Q::R; m++) o[m] = make_double2(x[m].x * scale, x[m].y * scale);
+        for (int m = 0; m < Q::R; m++) o[m * kCols * Q::items] = make_double2(x[m].x * scale, x[m].y * scale);
         continue;
       }
-      const double2 *a = ah + (uint64_t(c) << E2) + i0;
+      const double2 *a = ah + it;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m]));
+      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m * kCols * Q::items]));
       dit_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
@@ -357,11 +368,12 @@ __global__ void __launch_bounds__(qcf_threads(E2), 1) qcf_row(
 }
 
 // Pass C.  grid (N2 / 8, transforms).  out: plane p at out + p * stride_bytes,
-// written (accumulate == 0) or XORed into (accumulate == 1).
+// written (accumulate == 0) or XORed into (accumulate == 1); with tiles !=
+// nullptr the result goes to the tile layout instead (one word per row).
 template <int E1>
 __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_inv(
     const double2 *__restrict__ Y, int e2, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
-    uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate) {
+    uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles) {
   constexpr int N1 = 1 << E1, ld = N1 + 1;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
@@ -407,17 +419,105 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_inv(
         const uint32_t re = uint32_t(__double2loint(x[m].x + kRoundMagic));
         const uint32_t im = uint32_t(__double2loint(x[m].y + kRoundMagic));
         const uint32_t pl[4] = {re & 1u, (re >> 21) & 1u, im & 1u, (im >> 21) & 1u};
-        const uint64_t byte = ((uint64_t(i0 + Q::M * m) << e2) | uint64_t(c0)) >> 3;
+        const int j1 = i0 + Q::M * m;
+        uint32_t word = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) word |= ((__ballot_sync(0xffffffffu, pl[q]) >> (lane & ~7)) & 0xffu) << (8 * q);
+        if (c != 0) continue;
+        if (tiles) {
+          tiles[(uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (uint64_t(j1) << (e2 - 3)) + blockIdx.x] = word;
+          continue;
+        }
+        const uint64_t byte = ((uint64_t(j1) << e2) | uint64_t(c0)) >> 3;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          const uint32_t mask = __ballot_sync(0xffffffffu, pl[q]);
-          if (c == 0 && p0 + q < nplanes) {
-            const uint8_t v = uint8_t(mask >> (lane & ~7));
+          if (p0 + q < nplanes) {
+            const uint8_t v = uint8_t(word >> (8 * q));
             uint8_t *o = out + uint64_t(p0 + q) * stride_bytes + byte;
             *o = accumulate ? uint8_t(*o ^ v) : v;
           }
         }
       }
+    }
+  }
+}
+
+// 8x8 bit-matrix transpose of x (row i = byte i, column j = bit j) by three
+// delta swaps (H. S. Warren, Hacker's Delight, 2nd ed., section 7-3).
+__device__ __forceinline__ uint64_t transpose8(uint64_t x) {
+  uint64_t t;
+  t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+  x ^= t ^ (t << 7);
+  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+  x ^= t ^ (t << 14);
+  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+  x ^= t ^ (t << 28);
+  return x;
+}
+
+// Tile layout of 128 planes of n = N1 * N2 bits (the dual LPN's input and
+// output): word tiles[t][j1][g] (t < 32 transforms, g < N2 / 8 column tiles)
+// holds, in byte q, bits (N2 j1 + 8 g + c), c < 8, of plane 4t + q.  The
+// 8 blocks j = 8 (N2/8 j1 + g) + c of the block vector give all 32 words of
+// one (j1, g): per 32-bit word wd and byte k of the blocks, the 8x8 bit
+// transpose of those 8 bytes yields planes 32 wd + 8 k + b in byte b, i.e.
+// words t = 8 wd + 2 k (low half) and t + 1 (high half).
+__global__ void __launch_bounds__(256) qcf_gather(const uint4 *__restrict__ in, uint64_t ngroups,
+                                                  uint32_t *__restrict__ tiles) {
+  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups;
+       g += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t w[8][4];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const uint4 v = __ldg(&in[8 * g + c]);
+      w[c][0] = v.x; w[c][1] = v.y; w[c][2] = v.z; w[c][3] = v.w;
+    }
+#pragma unroll
+    for (int wd = 0; wd < 4; wd++) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        uint64_t x = 0;
+#pragma unroll
+        for (int c = 0; c < 8; c++) x |= uint64_t((w[c][wd] >> (8 * k)) & 0xffu) << (8 * c);
+        x = transpose8(x);
+        const int t = 8 * wd + 2 * k;
+        tiles[uint64_t(t) * ngroups + g] = uint32_t(x);
+        tiles[uint64_t(t + 1) * ngroups + g] = uint32_t(x >> 32);
+      }
+    }
+  }
+}
+
+// The inverse of qcf_gather; out[j] = (xor_in ? xor_in[j] : 0) ^ block j.
+__global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ tiles, uint64_t ngroups,
+                                                   const uint4 *__restrict__ xor_in, uint4 *__restrict__ out) {
+  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups;
+       g += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t w[8][4];
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+#pragma unroll
+      for (int wd = 0; wd < 4; wd++) w[c][wd] = 0;
+#pragma unroll
+    for (int wd = 0; wd < 4; wd++) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int t = 8 * wd + 2 * k;
+        uint64_t x = uint64_t(__ldg(&tiles[uint64_t(t) * ngroups + g])) |
+                     uint64_t(__ldg(&tiles[uint64_t(t + 1) * ngroups + g])) << 32;
+        x = transpose8(x);
+#pragma unroll
+        for (int c = 0; c < 8; c++) w[c][wd] |= uint32_t((x >> (8 * c)) & 0xffu) << (8 * k);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      uint4 v = make_uint4(w[c][0], w[c][1], w[c][2], w[c][3]);
+      if (xor_in) {
+        const uint4 a = __ldg(&xor_in[8 * g + c]);
+        v.x ^= a.x; v.y ^= a.y; v.z ^= a.z; v.w ^= a.w;
+      }
+      out[8 * g + c] = v;
     }
   }
 }
@@ -504,13 +604,13 @@ int set_attrs() {
 }
 
 void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t *in, uint64_t stride_bytes,
-                    int nplanes, int one_plane, double2 *Y) {
+                    int nplanes, int one_plane, const uint32_t *tiles, double2 *Y) {
   const dim3 grid((1u << t->e2) / kCols, ntr);
   switch (t->e1) {
 #define QCF_L(E)                                                                                            \
   case E:                                                                                                   \
     qcf_col_fwd<E><<<grid, qcf_threads(E), col_smem(E), st>>>(in, stride_bytes, nplanes, one_plane, t->e2, \
-                                                               t->T1, t->fs, Y);                            \
+                                                               tiles, t->T1, t->fs, Y);                     \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
@@ -529,13 +629,13 @@ void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const 
   }
 }
 void launch_col_inv(const QcfTables *t, int ntr, cudaStream_t st, const double2 *Y, uint8_t *out,
-                    uint64_t stride_bytes, int nplanes, int accumulate) {
+                    uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *tiles) {
   const dim3 grid((1u << t->e2) / kCols, ntr);
   switch (t->e1) {
 #define QCF_L(E)                                                                                          \
   case E:                                                                                                 \
     qcf_col_inv<E><<<grid, qcf_threads(E), col_smem(E), st>>>(Y, t->e2, t->T1, t->fs, out, stride_bytes, \
-                                                               nplanes, accumulate);                      \
+                                                               nplanes, accumulate, tiles);               \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
@@ -585,7 +685,7 @@ void qcf_free_ctx_tables(cuot_ctx *ctx) {
 
 int qcf_build_ahat(const QcfTables *t, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
   const uint64_t n = 1ull << t->e;
-  launch_col_fwd(t, 1, st, reinterpret_cast<const uint8_t *>(a_d), n / 8, 1, 1, static_cast<double2 *>(Y));
+  launch_col_fwd(t, 1, st, reinterpret_cast<const uint8_t *>(a_d), n / 8, 1, 1, nullptr, static_cast<double2 *>(Y));
   launch_row(t, 1, st, static_cast<double2 *>(Y), QcfAhatTab{}, 1, static_cast<double2 *>(ahat), 1.0 / double(n));
   return launch_status(2);
 }
@@ -600,13 +700,44 @@ int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, u
     QcfAhatTab tab = ahat;
     tab.first += p0 / 4;
     launch_col_fwd(t, ntr, st, reinterpret_cast<const uint8_t *>(in + uint64_t(p0) * stride), stride * 8, nb, 0,
-                   static_cast<double2 *>(Y));
+                   nullptr, static_cast<double2 *>(Y));
     launch_row(t, ntr, st, static_cast<double2 *>(Y), tab, 0, nullptr, 0.0);
     launch_col_inv(t, ntr, st, static_cast<const double2 *>(Y), reinterpret_cast<uint8_t *>(out + uint64_t(p0) * stride),
-                   stride * 8, nb, accumulate);
+                   stride * 8, nb, accumulate, nullptr);
     launches += 3;
   }
   return launch_status(launches);
+}
+
+int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles, int ntransforms, void *Y,
+                     int batch, cudaStream_t st) {
+  const int bt = batch < 4 ? 1 : batch / 4;  // transforms per launch group
+  const uint64_t words = 1ull << (t->e - 3);  // per transform
+  int launches = 0;
+  for (int t0 = 0; t0 < ntransforms; t0 += bt) {
+    const int ntr = ntransforms - t0 < bt ? ntransforms - t0 : bt;
+    QcfAhatTab tab = ahat;
+    tab.first += t0;
+    uint32_t *tp = tiles + uint64_t(t0) * words;
+    launch_col_fwd(t, ntr, st, nullptr, 0, 4 * ntr, 0, tp, static_cast<double2 *>(Y));
+    launch_row(t, ntr, st, static_cast<double2 *>(Y), tab, 0, nullptr, 0.0);
+    launch_col_inv(t, ntr, st, static_cast<const double2 *>(Y), nullptr, 0, 4 * ntr, 0, tp);
+    launches += 3;
+  }
+  return launch_status(launches);
+}
+
+int qcf_gather(int e, const cuot_block *in, uint32_t *tiles, cudaStream_t st) {
+  const uint64_t ng = 1ull << (e - 3);
+  qcf_gather<<<unsigned((ng + 255) / 256), 256, 0, st>>>(reinterpret_cast<const uint4 *>(in), ng, tiles);
+  return launch_status();
+}
+
+int qcf_scatter(int e, const uint32_t *tiles, const cuot_block *xor_in, cuot_block *out, cudaStream_t st) {
+  const uint64_t ng = 1ull << (e - 3);
+  qcf_scatter<<<unsigned((ng + 255) / 256), 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
+                                                           reinterpret_cast<uint4 *>(out));
+  return launch_status();
 }
 
 }  // namespace cuot
