@@ -61,7 +61,9 @@ __host__ __device__ constexpr int qcf_threads(int L) { return L >= 10 ? 512 : L 
 __host__ __device__ constexpr int qcf_fs_lo(int e1) { return (e1 + 1) / 2; }
 __host__ __device__ constexpr int qcf_fs_width(int e1) { return (1 << qcf_fs_lo(e1)) + (1 << (e1 - qcf_fs_lo(e1))); }
 __host__ __device__ constexpr int qcf_fs_ld(int e1) { return qcf_fs_width(e1) + 1; }
-constexpr int kCols = 8;  // transforms (columns or rows) per CTA
+constexpr int kCols = 8;  // columns per CTA of the column passes
+constexpr int kRows = 4;  // rows per CTA of the row pass (two CTAs fit an SM)
+__host__ __device__ constexpr int qcf_row_threads(int L) { return qcf_threads(L) / 2 < 32 ? 32 : qcf_threads(L) / 2; }
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -158,16 +160,32 @@ __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int ba
   }
 }
 
-// One pass entirely in shared memory (xs rows of ld complex values).
-template <int L, int P, bool INV>
-__device__ __forceinline__ void smem_pass(double2 *xs, int ld, const double2 *T) {
+// Shared-memory position of element i of a transform.  NT = 8 transforms per
+// CTA: rows of N + 1 values, the 8 lanes of a quarter-warp are the 8
+// transforms at one item, no swizzle.  NT = 4: rows of N + 2 values, a
+// quarter-warp is 4 transforms x 2 consecutive items, and flipping bit 0 by
+// bit K_last of i keeps both the early passes (items differ in bit 0) and the
+// last pass (items differ in bit K_last) conflict-free.
+template <int L, int NT>
+__device__ __forceinline__ int spos(int i) {
+  if constexpr (NT == 8) return i;
+  return i ^ ((i >> qcf_k(L, qcf_npass(L) - 1)) & 1);
+}
+template <int NT>
+__host__ __device__ constexpr int sld(int N) { return NT == 8 ? N + 1 : N + 2; }
+
+// One pass entirely in shared memory (xs rows of sld<NT>(N) complex values).
+template <int L, int P, bool INV, int NT>
+__device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
   using Q = Pass<L, P>;
-  for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-    const int c = it & (kCols - 1), w = it / kCols;
-    double2 *row = xs + c * ld + Q::first(w);
+  constexpr int ld = sld<NT>(1 << L);
+  for (int it = threadIdx.x; it < NT * Q::items; it += blockDim.x) {
+    const int c = it & (NT - 1), w = it / NT;
+    double2 *row = xs + c * ld;
+    const int i0 = Q::first(w);
     double2 x[Q::R];
 #pragma unroll
-    for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
+    for (int m = 0; m < Q::R; m++) x[m] = row[spos<L, NT>(i0 + Q::M * m)];
     if (!INV) {
       dif_regs<Q::K>(x);
       pass_twiddle<L, P, false>(x, Q::base(w), T);
@@ -176,16 +194,16 @@ __device__ __forceinline__ void smem_pass(double2 *xs, int ld, const double2 *T)
       dit_regs<Q::K>(x);
     }
 #pragma unroll
-    for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
+    for (int m = 0; m < Q::R; m++) row[spos<L, NT>(i0 + Q::M * m)] = x[m];
   }
 }
 
 // Middle passes [1, npass - 1) forward, or in reverse order inverse.
-template <int L, bool INV>
-__device__ __forceinline__ void middle_passes(double2 *xs, int ld, const double2 *T) {
+template <int L, bool INV, int NT>
+__device__ __forceinline__ void middle_passes(double2 *xs, const double2 *T) {
   if constexpr (qcf_npass(L) == 3) {
     __syncthreads();
-    smem_pass<L, 1, INV>(xs, ld, T);
+    smem_pass<L, 1, INV, NT>(xs, T);
   }
   __syncthreads();
 }
@@ -265,7 +283,7 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
       for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
     }
   }
-  middle_passes<E1, false>(xs, ld, Ts);
+  middle_passes<E1, false, kCols>(xs, Ts);
   {  // last pass (M = 1), then the four-step twiddle, to global
     using Q = Pass<E1, NP - 1>;
     static_assert(Q::M == 1, "last pass");
@@ -286,28 +304,28 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
   }
 }
 
-// Pass B.  grid (N1 / 8, transforms).  mode 0: forward, pointwise by the
+// Pass B.  grid (N1 / 4, transforms).  mode 0: forward, pointwise by the
 // transform's A_hat (ahat.p[(ahat.first + y) / ahat.per]), inverse, in place.
 // mode 1: forward only, times `scale`, written to `out` (builds A_hat).
-// A_hat is stored in the order the last pass consumes it: for the 8 rows
-// from r0, element m of item w of row c at r0 * N2 + (m * items + w) * 8 + c,
+// A_hat is stored in the order the last pass consumes it: for the 4 rows
+// from r0, element m of item w of row c at r0 * N2 + (m * items + w) * 4 + c,
 // so each warp reads 512 contiguous bytes per load.
 template <int E2>
-__global__ void __launch_bounds__(qcf_threads(E2), 1) qcf_row(
+__global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
     double2 *__restrict__ Y, int e1, const double2 *__restrict__ T2, QcfAhatTab ahat, int mode,
     double2 *__restrict__ out, double scale) {
-  constexpr int N2 = 1 << E2, ld = N2 + 1;
+  constexpr int N2 = 1 << E2, ld = sld<kRows>(N2);
   constexpr int NP = qcf_npass(E2);
   extern __shared__ double2 sm[];
-  double2 *xs = sm, *Ts = xs + kCols * ld;
-  const int r0 = blockIdx.x * kCols;
+  double2 *xs = sm, *Ts = xs + kRows * ld;
+  const int r0 = blockIdx.x * kRows;
   stage(Ts, T2, N2);
   double2 *Yp = Y + (uint64_t(blockIdx.y) << (e1 + E2)) + (uint64_t(r0) << E2);
   __syncthreads();
   {  // pass 0 from global
     using Q = Pass<E2, 0>;
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < kRows * Q::items; it += blockDim.x) {
+      const int c = it & (kRows - 1), w = it / kRows;
       const int i0 = Q::first(w);
       const double2 *src = Yp + (uint64_t(c) << E2) + i0;
       double2 x[Q::R];
@@ -315,49 +333,50 @@ __global__ void __launch_bounds__(qcf_threads(E2), 1) qcf_row(
       for (int m = 0; m < Q::R; m++) x[m] = src[Q::M * m];
       dif_regs<Q::K>(x);
       pass_twiddle<E2, 0, false>(x, Q::base(w), Ts);
-      double2 *row = xs + c * ld + i0;
+      double2 *row = xs + c * ld;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
+      for (int m = 0; m < Q::R; m++) row[spos<E2, kRows>(i0 + Q::M * m)] = x[m];
     }
   }
-  middle_passes<E2, false>(xs, ld, Ts);
+  middle_passes<E2, false, kRows>(xs, Ts);
   {  // last forward pass; pointwise product; first inverse pass
     using Q = Pass<E2, NP - 1>;
     const double2 *ah = mode == 0 ? static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
                                         (uint64_t(r0) << E2)
                                   : nullptr;
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < kRows * Q::items; it += blockDim.x) {
+      const int c = it & (kRows - 1), w = it / kRows;
       const int i0 = Q::first(w);
+      double2 *row = xs + c * ld;
       double2 x[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + i0 + m];
+      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, kRows>(i0 + m)];
       dif_regs<Q::K>(x);
       if (mode == 1) {
         double2 *o = out + (uint64_t(r0) << E2) + it;
 #pragma unroll
-        for (int m = 0; m < Q::R; m++) o[m * kCols * Q::items] = make_double2(x[m].x * scale, x[m].y * scale);
+        for (int m = 0; m < Q::R; m++) o[m * kRows * Q::items] = make_double2(x[m].x * scale, x[m].y * scale);
         continue;
       }
       const double2 *a = ah + it;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m * kCols * Q::items]));
+      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m * kRows * Q::items]));
       dit_regs<Q::K>(x);
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
+      for (int m = 0; m < Q::R; m++) row[spos<E2, kRows>(i0 + m)] = x[m];
     }
   }
   if (mode == 1) return;
-  middle_passes<E2, true>(xs, ld, Ts);
+  middle_passes<E2, true, kRows>(xs, Ts);
   {  // inverse of pass 0, to global
     using Q = Pass<E2, 0>;
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < kRows * Q::items; it += blockDim.x) {
+      const int c = it & (kRows - 1), w = it / kRows;
       const int i0 = Q::first(w);
-      const double2 *row = xs + c * ld + i0;
+      const double2 *row = xs + c * ld;
       double2 x[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
+      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, kRows>(i0 + Q::M * m)];
       pass_twiddle<E2, 0, true>(x, Q::base(w), Ts);
       dit_regs<Q::K>(x);
       double2 *dst = Yp + (uint64_t(c) << E2) + i0;
@@ -400,7 +419,7 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_inv(
       for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
     }
   }
-  middle_passes<E1, true>(xs, ld, Ts);
+  middle_passes<E1, true, kCols>(xs, Ts);
   {  // inverse of pass 0; round; the 8 columns' bits of each plane form a byte
     using Q = Pass<E1, 0>;
     const int lane = threadIdx.x & 31;
@@ -576,7 +595,7 @@ int col_smem(int e1) {
 }
 int row_smem(int e2) {
   const int N2 = 1 << e2;
-  return (kCols * (N2 + 1) + N2) * 16;
+  return (kRows * sld<kRows>(N2) + N2) * 16;
 }
 
 #define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10)
@@ -618,11 +637,11 @@ void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t 
 }
 void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const QcfAhatTab &ahat, int mode,
                 double2 *out, double scale) {
-  const dim3 grid((1u << t->e1) / kCols, ntr);
+  const dim3 grid((1u << t->e1) / kRows, ntr);
   switch (t->e2) {
-#define QCF_L(E)                                                                                       \
-  case E:                                                                                              \
-    qcf_row<E><<<grid, qcf_threads(E), row_smem(E), st>>>(Y, t->e1, t->T2, ahat, mode, out, scale);   \
+#define QCF_L(E)                                                                                         \
+  case E:                                                                                                \
+    qcf_row<E><<<grid, qcf_row_threads(E), row_smem(E), st>>>(Y, t->e1, t->T2, ahat, mode, out, scale);  \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
