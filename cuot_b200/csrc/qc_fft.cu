@@ -20,12 +20,12 @@
 // butterfly shared by four planes), against several integer instructions
 // per plane in the number-theoretic transform of qc.cu.
 //
-// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= N2 = 2^e2 <= 1024), input
+// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= 512, N1 <= N2 <= 2048), input
 // index j = N2*j1 + j2, frequency k = k1 + N1*k2:
 //   A (columns): 8 columns j2 of one transform per CTA: load the plane bits,
 //     N1-point DIF FFT over j1 (frequencies land in bit-reversed row order r),
 //     multiply by w_n^(j2 * rev(r)), store Y[r][j2].
-//   B (rows): 8 rows per CTA: N2-point DIF FFT, multiply by A_hat (the
+//   B (rows): 4 rows (2 at N2 = 2048) per CTA: N2-point DIF FFT, multiply by A_hat (the
 //     transform of `a` in the same layout, scaled by 1/n), N2-point DIT
 //     inverse, store.
 //   C (columns): multiply by w_n^-(j2 * rev(r)), N1-point DIT inverse over r,
@@ -42,7 +42,7 @@ namespace cuot {
 
 constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
 
-// Radix plan of an N = 2^L point transform, 5 <= L <= 10: K bits per pass.
+// Radix plan of an N = 2^L point transform, 5 <= L <= 11: K bits per pass.
 __host__ __device__ constexpr int qcf_npass(int L) { return L <= 8 ? 2 : 3; }
 __host__ __device__ constexpr int qcf_k(int L, int p) {
   return L == 5 ? (p == 0 ? 3 : 2)
@@ -50,7 +50,8 @@ __host__ __device__ constexpr int qcf_k(int L, int p) {
        : L == 7 ? (p == 0 ? 4 : 3)
        : L == 8 ? 4
        : L == 9 ? 3
-       : (p == 0 ? 4 : 3);
+       : L == 10 ? (p == 0 ? 4 : 3)
+       : (p == 2 ? 3 : 4);
 }
 // log2 of the sub-transform size at the start of pass p
 __host__ __device__ constexpr int qcf_ls(int L, int p) { return p == 0 ? L : qcf_ls(L, p - 1) - qcf_k(L, p - 1); }
@@ -62,8 +63,15 @@ __host__ __device__ constexpr int qcf_fs_lo(int e1) { return (e1 + 1) / 2; }
 __host__ __device__ constexpr int qcf_fs_width(int e1) { return (1 << qcf_fs_lo(e1)) + (1 << (e1 - qcf_fs_lo(e1))); }
 __host__ __device__ constexpr int qcf_fs_ld(int e1) { return qcf_fs_width(e1) + 1; }
 constexpr int kCols = 8;  // columns per CTA of the column passes
-constexpr int kRows = 4;  // rows per CTA of the row pass (two CTAs fit an SM)
-__host__ __device__ constexpr int qcf_row_threads(int L) { return qcf_threads(L) / 2 < 32 ? 32 : qcf_threads(L) / 2; }
+// Rows per CTA of the row pass, so that two CTAs fit an SM: 4 up to 1024
+// points, 2 for 2048.
+__host__ __device__ constexpr int qcf_rows(int L) { return L >= 11 ? 2 : 4; }
+__host__ __device__ constexpr int qcf_row_threads(int L) {
+  return L >= 11 ? 256 : qcf_threads(L) / 2 < 32 ? 32 : qcf_threads(L) / 2;
+}
+// Split of n = 2^e into N1 = 2^e1 column points (at most 512, so two column
+// CTAs fit an SM) and N2 = 2^(e - e1) row points.
+__host__ __device__ constexpr int qcf_e1(int e) { return e / 2 < 9 ? e / 2 : 9; }
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -162,17 +170,18 @@ __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int ba
 
 // Shared-memory position of element i of a transform.  NT = 8 transforms per
 // CTA: rows of N + 1 values, the 8 lanes of a quarter-warp are the 8
-// transforms at one item, no swizzle.  NT = 4: rows of N + 2 values, a
-// quarter-warp is 4 transforms x 2 consecutive items, and flipping bit 0 by
-// bit K_last of i keeps both the early passes (items differ in bit 0) and the
-// last pass (items differ in bit K_last) conflict-free.
+// transforms at one item, no swizzle.  NT = 4 (2): rows of N + 2 (N + 4)
+// values, a quarter-warp is 4 transforms x 2 consecutive items (2 x 4), and
+// XORing bits [0, 1) ([0, 2)) of i with the bits above K_last keeps both the
+// early passes (items differ in the low bits) and the last pass (items differ
+// from bit K_last up) conflict-free.
 template <int L, int NT>
 __device__ __forceinline__ int spos(int i) {
   if constexpr (NT == 8) return i;
-  return i ^ ((i >> qcf_k(L, qcf_npass(L) - 1)) & 1);
+  return i ^ ((i >> qcf_k(L, qcf_npass(L) - 1)) & (NT == 4 ? 1 : 3));
 }
 template <int NT>
-__host__ __device__ constexpr int sld(int N) { return NT == 8 ? N + 1 : N + 2; }
+__host__ __device__ constexpr int sld(int N) { return NT == 8 ? N + 1 : NT == 4 ? N + 2 : N + 4; }
 
 // One pass entirely in shared memory (xs rows of sld<NT>(N) complex values).
 template <int L, int P, bool INV, int NT>
@@ -234,7 +243,7 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 // instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
 // columns of the CTA's tile in row j1 (qcf_gather).
 template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
+__global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_fwd(
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     double2 *__restrict__ Y) {
@@ -304,28 +313,29 @@ __global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_fwd(
   }
 }
 
-// Pass B.  grid (N1 / 4, transforms).  mode 0: forward, pointwise by the
+// Pass B.  grid (N1 / qcf_rows(e2), transforms).  mode 0: forward, pointwise by the
 // transform's A_hat (ahat.p[(ahat.first + y) / ahat.per]), inverse, in place.
 // mode 1: forward only, times `scale`, written to `out` (builds A_hat).
-// A_hat is stored in the order the last pass consumes it: for the 4 rows
-// from r0, element m of item w of row c at r0 * N2 + (m * items + w) * 4 + c,
+// A_hat is stored in the order the last pass consumes it: for the NT rows
+// from r0, element m of item w of row c at r0 * N2 + (m * items + w) * NT + c,
 // so each warp reads 512 contiguous bytes per load.
 template <int E2>
 __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
     double2 *__restrict__ Y, int e1, const double2 *__restrict__ T2, QcfAhatTab ahat, int mode,
     double2 *__restrict__ out, double scale) {
-  constexpr int N2 = 1 << E2, ld = sld<kRows>(N2);
+  constexpr int NT = qcf_rows(E2);
+  constexpr int N2 = 1 << E2, ld = sld<NT>(N2);
   constexpr int NP = qcf_npass(E2);
   extern __shared__ double2 sm[];
-  double2 *xs = sm, *Ts = xs + kRows * ld;
-  const int r0 = blockIdx.x * kRows;
+  double2 *xs = sm, *Ts = xs + NT * ld;
+  const int r0 = blockIdx.x * NT;
   stage(Ts, T2, N2);
   double2 *Yp = Y + (uint64_t(blockIdx.y) << (e1 + E2)) + (uint64_t(r0) << E2);
   __syncthreads();
   {  // pass 0 from global
     using Q = Pass<E2, 0>;
-    for (int it = threadIdx.x; it < kRows * Q::items; it += blockDim.x) {
-      const int c = it & (kRows - 1), w = it / kRows;
+    for (int it = threadIdx.x; it < NT * Q::items; it += blockDim.x) {
+      const int c = it & (NT - 1), w = it / NT;
       const int i0 = Q::first(w);
       const double2 *src = Yp + (uint64_t(c) << E2) + i0;
       double2 x[Q::R];
@@ -335,48 +345,48 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
       pass_twiddle<E2, 0, false>(x, Q::base(w), Ts);
       double2 *row = xs + c * ld;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) row[spos<E2, kRows>(i0 + Q::M * m)] = x[m];
+      for (int m = 0; m < Q::R; m++) row[spos<E2, NT>(i0 + Q::M * m)] = x[m];
     }
   }
-  middle_passes<E2, false, kRows>(xs, Ts);
+  middle_passes<E2, false, NT>(xs, Ts);
   {  // last forward pass; pointwise product; first inverse pass
     using Q = Pass<E2, NP - 1>;
     const double2 *ah = mode == 0 ? static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
                                         (uint64_t(r0) << E2)
                                   : nullptr;
-    for (int it = threadIdx.x; it < kRows * Q::items; it += blockDim.x) {
-      const int c = it & (kRows - 1), w = it / kRows;
+    for (int it = threadIdx.x; it < NT * Q::items; it += blockDim.x) {
+      const int c = it & (NT - 1), w = it / NT;
       const int i0 = Q::first(w);
       double2 *row = xs + c * ld;
       double2 x[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, kRows>(i0 + m)];
+      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, NT>(i0 + m)];
       dif_regs<Q::K>(x);
       if (mode == 1) {
         double2 *o = out + (uint64_t(r0) << E2) + it;
 #pragma unroll
-        for (int m = 0; m < Q::R; m++) o[m * kRows * Q::items] = make_double2(x[m].x * scale, x[m].y * scale);
+        for (int m = 0; m < Q::R; m++) o[m * NT * Q::items] = make_double2(x[m].x * scale, x[m].y * scale);
         continue;
       }
       const double2 *a = ah + it;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m * kRows * Q::items]));
+      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m * NT * Q::items]));
       dit_regs<Q::K>(x);
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) row[spos<E2, kRows>(i0 + m)] = x[m];
+      for (int m = 0; m < Q::R; m++) row[spos<E2, NT>(i0 + m)] = x[m];
     }
   }
   if (mode == 1) return;
-  middle_passes<E2, true, kRows>(xs, Ts);
+  middle_passes<E2, true, NT>(xs, Ts);
   {  // inverse of pass 0, to global
     using Q = Pass<E2, 0>;
-    for (int it = threadIdx.x; it < kRows * Q::items; it += blockDim.x) {
-      const int c = it & (kRows - 1), w = it / kRows;
+    for (int it = threadIdx.x; it < NT * Q::items; it += blockDim.x) {
+      const int c = it & (NT - 1), w = it / NT;
       const int i0 = Q::first(w);
       const double2 *row = xs + c * ld;
       double2 x[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, kRows>(i0 + Q::M * m)];
+      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, NT>(i0 + Q::M * m)];
       pass_twiddle<E2, 0, true>(x, Q::base(w), Ts);
       dit_regs<Q::K>(x);
       double2 *dst = Yp + (uint64_t(c) << E2) + i0;
@@ -390,7 +400,7 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
 // written (accumulate == 0) or XORed into (accumulate == 1); with tiles !=
 // nullptr the result goes to the tile layout instead (one word per row).
 template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), 1) qcf_col_inv(
+__global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_inv(
     const double2 *__restrict__ Y, int e2, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles) {
   constexpr int N1 = 1 << E1, ld = N1 + 1;
@@ -595,10 +605,12 @@ int col_smem(int e1) {
 }
 int row_smem(int e2) {
   const int N2 = 1 << e2;
-  return (kRows * sld<kRows>(N2) + N2) * 16;
+  const int ld = qcf_rows(e2) == 4 ? sld<4>(N2) : sld<2>(N2);
+  return (qcf_rows(e2) * ld + N2) * 16;
 }
 
-#define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10)
+#define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9)
+#define QCF_ROW_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11)
 
 int set_attrs() {
   static bool done[64] = {false};
@@ -610,10 +622,13 @@ int set_attrs() {
   ok &= cudaFuncSetAttribute(qcf_col_fwd<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E)) == \
         cudaSuccess;                                                                                   \
   ok &= cudaFuncSetAttribute(qcf_col_inv<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E)) == \
-        cudaSuccess;                                                                                   \
+        cudaSuccess;
+#define QCF_SETR(E) \
   ok &= cudaFuncSetAttribute(qcf_row<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem(E)) == cudaSuccess;
   QCF_CASES(QCF_SET)
+  QCF_ROW_CASES(QCF_SETR)
 #undef QCF_SET
+#undef QCF_SETR
   if (!ok) {
     cudaGetLastError();
     return fail(CUOT_ECUDA, "QC FFT shared-memory attribute failed");
@@ -637,13 +652,13 @@ void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t 
 }
 void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const QcfAhatTab &ahat, int mode,
                 double2 *out, double scale) {
-  const dim3 grid((1u << t->e1) / kRows, ntr);
+  const dim3 grid((1u << t->e1) / qcf_rows(t->e2), ntr);
   switch (t->e2) {
 #define QCF_L(E)                                                                                         \
   case E:                                                                                                \
     qcf_row<E><<<grid, qcf_row_threads(E), row_smem(E), st>>>(Y, t->e1, t->T2, ahat, mode, out, scale);  \
     break;
-    QCF_CASES(QCF_L)
+    QCF_ROW_CASES(QCF_L)
 #undef QCF_L
   }
 }
@@ -674,7 +689,7 @@ int qcf_get_tables(cuot_ctx *ctx, int e, QcfTables **out) {
   CUOT_TRY(set_attrs());
   QcfTables *t = new QcfTables{};
   t->e = e;
-  t->e1 = e / 2;
+  t->e1 = qcf_e1(e);
   t->e2 = e - t->e1;
   const uint64_t N1 = 1ull << t->e1, N2 = 1ull << t->e2;
   int st = CUOT_OK;
