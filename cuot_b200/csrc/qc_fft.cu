@@ -55,6 +55,13 @@ __host__ __device__ constexpr int qcf_k(int L, int p) {
 }
 // log2 of the sub-transform size at the start of pass p
 __host__ __device__ constexpr int qcf_ls(int L, int p) { return p == 0 ? L : qcf_ls(L, p - 1) - qcf_k(L, p - 1); }
+// Twiddle table of an N-point transform in pass order: pass p's factors
+// w_S^(base q) (q in [1, 2^K), base < M = S / 2^K) at tw_off(p) + (q-1) M + base,
+// so lanes at consecutive bases read consecutive entries and lanes at the
+// same base read the same entry (no bank conflicts).  At most N entries.
+__host__ __device__ constexpr int qcf_tw_off(int L, int p) {
+  return p == 0 ? 0 : qcf_tw_off(L, p - 1) + ((1 << qcf_k(L, p - 1)) - 1) * ((1 << qcf_ls(L, p - 1)) >> qcf_k(L, p - 1));
+}
 __host__ __device__ constexpr int qcf_threads(int L) { return L >= 10 ? 512 : L == 9 ? 256 : L == 8 ? 128 : 64; }
 // four-step factor tables per column: 2^lo + 2^(e1 - lo) entries (global
 // row stride), staged with an odd row stride so the 8 columns of a
@@ -155,15 +162,17 @@ struct Pass {
 };
 
 // Twiddles of a DIF pass after its butterflies: x[m] holds frequency
-// q = rev_K(m) of its sub-transform; multiply by w_S^(base q) = T[base q 2^(L-LS)].
+// q = rev_K(m) of its sub-transform; multiply by w_S^(base q) (table in pass
+// order, qcf_tw_off).
 template <int L, int P, bool INV>
 __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int base, const double2 *T) {
   using Q = Pass<L, P>;
   if (Q::M == 1) return;
+  const double2 *Tp = T + qcf_tw_off(L, P) + base;
 #pragma unroll
   for (int m = 1; m < Q::R; m++) {
     const int q = __brev(m) >> (32 - Q::K);
-    const double2 w = T[(base * q) << (L - Q::LS)];
+    const double2 w = Tp[(q - 1) * Q::M];
     x[m] = INV ? cmulc(x[m], w) : cmul(x[m], w);
   }
 }
@@ -551,12 +560,18 @@ __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ 
   }
 }
 
-// Table generation (one-time per n).  T[k] = w_N^k, k < N.
+// Table generation (one-time per n).  T: the pass-ordered twiddles of an
+// N = 2^L point transform (entries past the last pass's offset unused).
 __global__ void qcf_gen_roots(int L, double2 *T) {
   const int N = 1 << L;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    int p = 0;
+    while (p + 1 < qcf_npass(L) && k >= qcf_tw_off(L, p + 1)) p++;
+    const int K = qcf_k(L, p), LS = qcf_ls(L, p), M = (1 << LS) >> K;
+    const int q = (k - qcf_tw_off(L, p)) / M + 1, base = (k - qcf_tw_off(L, p)) % M;
+    const int e = (base * q) & ((1 << LS) - 1);
     double s, c;
-    sincospi(2.0 * double(k) / double(N), &s, &c);
+    sincospi(2.0 * double(e) / double(1 << LS), &s, &c);
     T[k] = make_double2(c, -s);
   }
 }
