@@ -172,8 +172,8 @@ class Instance:
         self.delta[0] |= 1
         self.choice = rng.integers(0, 2, t * h).astype(np.uint8)
         # device buffers
-        self.sctx = cuot_b200.Context(torch.cuda.current_device())
-        self.rctx = cuot_b200.Context(torch.cuda.current_device())
+        self.sctx = new_context(cuot_b200, torch.cuda.current_device())
+        self.rctx = new_context(cuot_b200, torch.cuda.current_device())
         self.d_roots = dev(self.roots)
         self.d_choice = dev(self.choice)
         self.leaves_s, self.leaves_r = emp(self.nleaves), emp(self.nleaves)
@@ -255,17 +255,55 @@ class Instance:
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
 # stage's kernels per step, summed from one ncu launch capture of the same
-# bench command (ncu starts every kernel with cold caches, so the NTT
-# intermediate that steady state keeps in L2 is counted).
+# bench command (ncu starts every kernel with cold caches, so intermediate
+# that steady state keeps in L2 is counted).  sot_n20 runs the fp64 FFT
+# backend (gather, 3 transform passes, scatter per role); the NTT figure is
+# the same workload with the NTT backend, which scales the SOT encodes of
+# larger n.
 NCU_TRAFFIC_PER_STEP = {
     "ferret_b13:lpn": 570.44e6,
-    "sot_n20:dual_lpn": 3990.2e6,
+    "sot_n20:dual_lpn": 4050.8e6,
+    "sot_n20_ntt:dual_lpn": 3990.2e6,
 }
 
-def ntt_butterflies(n: int) -> int:
-    """Radix-2 butterflies of one SOT dual LPN, both roles: 128 planes, a
-    forward and an inverse n-point transform each."""
-    return 2 * 128 * 2 * (n // 2) * (n.bit_length() - 1)
+QC_FFT_MAX_LOG_N = 20  # the fp64 FFT encodes n <= 2^20 (exactness bound); the NTT the rest
+QC_BACKENDS = {"auto": 0, "ntt": 1, "fft": 2}
+_qc_backend = 0
+
+
+def new_context(cuot_b200, device: int):
+    """A libcuot context with the QC backend chosen on the command line."""
+    c = cuot_b200.Context(device)
+    if _qc_backend:
+        c.set_tuning(c.TUNE_QC_BACKEND, _qc_backend)
+    return c
+
+
+def qc_transform_work(ns) -> dict:
+    """Arithmetic of the SOT dual LPNs of one step (both roles, 128 planes
+    each) for instance sizes `ns`: fp64 flops of the FFT backend (4 planes per
+    complex transform: 32 forward + 32 inverse n-point transforms per role at
+    the standard 5 n log2 n flops, plus 6n per pointwise product) and radix-2
+    butterflies of the NTT backend (128 forward + 128 inverse per role)."""
+    flops = bfly = 0
+    for n in ns:
+        lg = n.bit_length() - 1
+        if lg <= QC_FFT_MAX_LOG_N:
+            flops += 2 * 32 * (2 * 5 * n * lg + 6 * n)
+        else:
+            bfly += 2 * 128 * 2 * (n // 2) * lg
+    return {"fft_fp64_flops": flops, "ntt_butterflies": bfly}
+
+
+def qc_transform_report(ns, ms: float) -> dict:
+    w = qc_transform_work(ns)
+    out = {"backend": "fft (n <= 2^20) / ntt (larger n)", "stage_ms": ms, **w,
+           "model": "fft: 5 n log2 n flops per complex transform + 6n per product; ntt: n/2 log2 n butterflies"}
+    if w["fft_fp64_flops"] and not w["ntt_butterflies"]:
+        out["fp64_tflops"] = w["fft_fp64_flops"] / (ms / 1e3) / 1e12
+        out["fp64_peak_nominal_tflops"] = 37.0
+        out["frac_of_nominal"] = out["fp64_tflops"] / 37.0
+    return out
 
 
 AES_PEAK_MODEL = ("T-table AES: 160 shared-memory lookups per block (10 rounds x 16), one conflict-free "
@@ -481,7 +519,7 @@ def run_batch(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     spec = WORKLOADS[args.workload]
-    ctx = cuot_b200.Context(local)
+    ctx = new_context(cuot_b200, local)
     insts = mixed_workload(ctx, count=spec["count"], seed=2024 + rank, lo=spec["lo"], hi=spec["hi"])
     cots = sum(i.n for i in insts)
     stream = torch.cuda.Stream()
@@ -593,11 +631,14 @@ def run_batch(args):
     peaks, peak_kind = measured_peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
     # traffic: the batch is too large for a multi-metric ncu capture; the SOT
-    # encode runs the same NTT kernels as sot_n20, whose captured DRAM bytes
-    # per COT (both roles) scale it; other stages have no capture (null)
+    # encode runs the same kernels as sot_n20 (FFT for n <= 2^20, NTT above),
+    # whose captured DRAM bytes per COT (both roles) scale it; other stages
+    # have no capture (null)
     traffic = None
     if dom == "sot_encode":
-        traffic = NCU_TRAFFIC_PER_STEP["sot_n20:dual_lpn"] / (1 << 20) * n_sot
+        per_cot = {True: NCU_TRAFFIC_PER_STEP["sot_n20:dual_lpn"] / (1 << 20),
+                   False: NCU_TRAFFIC_PER_STEP["sot_n20_ntt:dual_lpn"] / (1 << 20)}
+        traffic = sum(i.n * per_cot[i.n.bit_length() - 1 <= QC_FFT_MAX_LOG_N] for i in insts if i.kind != KIND_FERRET)
     props = torch.cuda.get_device_properties(local)
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
     aes_peak = props.multi_processor_count * 32 * mhz * 1e6 / 160
@@ -608,13 +649,12 @@ def run_batch(args):
     for k, cnt in aes_counts.items():
         a = cnt / (stages[k] / 1e3)
         aes[k] = {"aes_per_step": cnt, "aes_per_s": a, "frac": a / aes_peak}
-    bfly = sum(ntt_butterflies(i.n) for i in insts if i.kind != KIND_FERRET)
     out = {
         "metric": metric_name(args.workload),
         "value": world * cots / (ms / 1e3), "unit": "COTs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "instances": len(insts),
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "qc_backend": args.qc_backend, "instances": len(insts),
                    "cots_per_step_per_gpu": cots, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "plain": {"value": world * cots / (ms_plain / 1e3), "ms_per_step": ms_plain,
@@ -625,10 +665,10 @@ def run_batch(args):
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": alg[dom],
-                     "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu capture "
-                              "by SOT COTs (3,805 DRAM bytes per COT, cold cache per kernel)"},
+                     "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu captures "
+                              "by SOT COTs (FFT sizes 3,863, NTT sizes 3,805 DRAM bytes per COT, cold cache per kernel)"},
         "aes_roofline": aes,
-        "ntt": {"butterflies_per_step": bfly, "butterflies_per_s": bfly / (stages["sot_encode"] / 1e3)},
+        "qc_transform": qc_transform_report([i.n for i in insts if i.kind != KIND_FERRET], stages["sot_encode"]),
         "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": launches * args.steps,
@@ -705,7 +745,7 @@ def run_session(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     p = FERRET_B13
     st = torch.cuda.Stream()
-    ctx = cuot_b200.Context(local)
+    ctx = new_context(cuot_b200, local)
     sess = FerretSession(ctx, ctx, p, seed=b"bench-session-%d" % rank, stream=st)
     for _ in range(args.warmup):
         sess.extend_f2k()
@@ -760,7 +800,7 @@ def run_session(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "usable_cots_per_step_per_gpu":
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "qc_backend": args.qc_backend, "usable_cots_per_step_per_gpu":
                    p.ot_limit, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "roofline": {"bound": "hbm", "kernel": "extension (PPRF + LPN, both roles)", "achieved": achieved,
@@ -906,7 +946,7 @@ def run_ours(args):
         "value": value, "unit": "COTs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "cots_per_step_per_gpu": n,
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "qc_backend": args.qc_backend, "cots_per_step_per_gpu": n,
                    "parallelism": f"replicas x{world} (independent instances per GPU)",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "stages_ms": {k: v[0] for k, v in stages.items()},
@@ -923,8 +963,7 @@ def run_ours(args):
     }
     out["aes_roofline"] = aes_roofline(inst, stages, clocks, torch.cuda.get_device_properties(local))
     if inst.spec["kind"] == "sot":
-        b = ntt_butterflies(inst.n)
-        out["ntt"] = {"butterflies_per_step": b, "butterflies_per_s": b / (lpn_ms / 1e3)}
+        out["qc_transform"] = qc_transform_report([inst.n], lpn_ms)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample(args.workload, threads)
@@ -950,7 +989,11 @@ def main():
                     help="requests of the served stream reported with mixed64 (0: skip; the full served configuration is 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--qc-backend", default="auto", choices=sorted(QC_BACKENDS),
+                    help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^20, NTT above)")
     args = ap.parse_args()
+    global _qc_backend
+    _qc_backend = QC_BACKENDS[args.qc_backend]
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
