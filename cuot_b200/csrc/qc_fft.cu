@@ -164,7 +164,8 @@ struct Pass {
 // Twiddles of a DIF pass after its butterflies: x[m] holds frequency
 // q = rev_K(m) of its sub-transform; multiply by w_S^(base q) (table in pass
 // order, qcf_tw_off).
-template <int L, int P, bool INV>
+// TG: T is in global memory (read through L1) instead of shared memory.
+template <int L, int P, bool INV, bool TG = false>
 __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int base, const double2 *T) {
   using Q = Pass<L, P>;
   if (Q::M == 1) return;
@@ -172,7 +173,7 @@ __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int ba
 #pragma unroll
   for (int m = 1; m < Q::R; m++) {
     const int q = __brev(m) >> (32 - Q::K);
-    const double2 w = Tp[(q - 1) * Q::M];
+    const double2 w = TG ? __ldg(&Tp[(q - 1) * Q::M]) : Tp[(q - 1) * Q::M];
     x[m] = INV ? cmulc(x[m], w) : cmul(x[m], w);
   }
 }
@@ -193,7 +194,7 @@ template <int NT>
 __host__ __device__ constexpr int sld(int N) { return NT == 8 ? N + 1 : NT == 4 ? N + 2 : N + 4; }
 
 // One pass entirely in shared memory (xs rows of sld<NT>(N) complex values).
-template <int L, int P, bool INV, int NT>
+template <int L, int P, bool INV, int NT, bool TG = false>
 __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
   using Q = Pass<L, P>;
   constexpr int ld = sld<NT>(1 << L);
@@ -206,9 +207,9 @@ __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
     for (int m = 0; m < Q::R; m++) x[m] = row[spos<L, NT>(i0 + Q::M * m)];
     if (!INV) {
       dif_regs<Q::K>(x);
-      pass_twiddle<L, P, false>(x, Q::base(w), T);
+      pass_twiddle<L, P, false, TG>(x, Q::base(w), T);
     } else {
-      pass_twiddle<L, P, true>(x, Q::base(w), T);
+      pass_twiddle<L, P, true, TG>(x, Q::base(w), T);
       dit_regs<Q::K>(x);
     }
 #pragma unroll
@@ -217,11 +218,11 @@ __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
 }
 
 // Middle passes [1, npass - 1) forward, or in reverse order inverse.
-template <int L, bool INV, int NT>
+template <int L, bool INV, int NT, bool TG = false>
 __device__ __forceinline__ void middle_passes(double2 *xs, const double2 *T) {
   if constexpr (qcf_npass(L) == 3) {
     __syncthreads();
-    smem_pass<L, 1, INV, NT>(xs, T);
+    smem_pass<L, 1, INV, NT, TG>(xs, T);
   }
   __syncthreads();
 }
@@ -252,18 +253,18 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 // instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
 // columns of the CTA's tile in row j1 (qcf_gather).
 template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_fwd(
+__global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_fwd(
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     double2 *__restrict__ Y) {
   constexpr int N1 = 1 << E1, ld = N1 + 1, W = qcf_fs_ld(E1);
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
-  double2 *xs = sm, *Ts = xs + kCols * ld, *fss = Ts + N1;
+  double2 *xs = sm, *fss = xs + kCols * ld;
   uint32_t *bits = reinterpret_cast<uint32_t *>(fss + kCols * W);
+  const double2 *Ts = T1;  // pass twiddles read through L1
   const int c0 = blockIdx.x * kCols;
   const int p0 = 4 * blockIdx.y;
-  stage(Ts, T1, N1);
   stage_fs<E1>(fss, fs, c0);
   if (tiles) {
     const uint32_t *tp = tiles + (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + blockIdx.x;
@@ -295,13 +296,13 @@ __global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_fwd(
         }
       }
       dif_regs<Q::K>(x);
-      pass_twiddle<E1, 0, false>(x, Q::base(w), Ts);
+      pass_twiddle<E1, 0, false, true>(x, Q::base(w), Ts);
       double2 *row = xs + c * ld + i0;
 #pragma unroll
       for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
     }
   }
-  middle_passes<E1, false, kCols>(xs, Ts);
+  middle_passes<E1, false, kCols, true>(xs, Ts);
   {  // last pass (M = 1), then the four-step twiddle, to global
     using Q = Pass<E1, NP - 1>;
     static_assert(Q::M == 1, "last pass");
@@ -409,16 +410,16 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
 // written (accumulate == 0) or XORed into (accumulate == 1); with tiles !=
 // nullptr the result goes to the tile layout instead (one word per row).
 template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_inv(
+__global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_inv(
     const double2 *__restrict__ Y, int e2, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles) {
   constexpr int N1 = 1 << E1, ld = N1 + 1;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
-  double2 *xs = sm, *Ts = xs + kCols * ld, *fss = Ts + N1;
+  double2 *xs = sm, *fss = xs + kCols * ld;
+  const double2 *Ts = T1;  // pass twiddles read through L1
   const int c0 = blockIdx.x * kCols;
   const int p0 = 4 * blockIdx.y;
-  stage(Ts, T1, N1);
   stage_fs<E1>(fss, fs, c0);
   __syncthreads();
   {  // inverse of the last pass, from global
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_inv(
       for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
     }
   }
-  middle_passes<E1, true, kCols>(xs, Ts);
+  middle_passes<E1, true, kCols, true>(xs, Ts);
   {  // inverse of pass 0; round; the 8 columns' bits of each plane form a byte
     using Q = Pass<E1, 0>;
     const int lane = threadIdx.x & 31;
@@ -449,7 +450,7 @@ __global__ void __launch_bounds__(qcf_threads(E1), 2) qcf_col_inv(
       double2 x[Q::R];
 #pragma unroll
       for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
-      pass_twiddle<E1, 0, true>(x, Q::base(w), Ts);
+      pass_twiddle<E1, 0, true, true>(x, Q::base(w), Ts);
       dit_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) {
@@ -616,7 +617,7 @@ void qcf_free(QcfTables *t) {
 
 int col_smem(int e1) {
   const int N1 = 1 << e1;
-  return (kCols * (N1 + 1) + N1 + kCols * qcf_fs_ld(e1)) * 16 + N1 * 4;
+  return (kCols * (N1 + 1) + kCols * qcf_fs_ld(e1)) * 16 + N1 * 4;
 }
 int row_smem(int e2) {
   const int N2 = 1 << e2;
