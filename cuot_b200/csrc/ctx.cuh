@@ -76,6 +76,21 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
 // XORed with xor_in).
 int qcf_gather(int e, const cuot_block *in, uint32_t *tiles, cudaStream_t st);
 int qcf_scatter(int e, const uint32_t *tiles, const cuot_block *xor_in, cuot_block *out, cudaStream_t st);
+// GF(2) Karatsuba over the FFT (qc_kara.cu): the dual LPN of n = 2^e,
+// kQcfMaxE < e <= kQcfMaxE + kQckMaxLevels, as 3^(e - kQcfMaxE) exact
+// 2^kQcfMaxE FFT dual LPNs.
+constexpr int kQckMaxLevels = 2;
+bool qck_supported(int e);
+uint64_t qck_ahat_bytes(int e);          // the leaves' transforms
+uint64_t qck_scratch_bytes(int e);       // block scratch of a dual LPN
+uint64_t qck_bits_scratch_bytes(int e);  // bit scratch of the A_hat build
+// bits: qck_bits_scratch_bytes(e); Y: 16 * 2^kQcfMaxE bytes.
+int qck_build_ahat(const QcfTables *leaf, int e, const uint64_t *a_d, void *bits, void *Y, void *ahat,
+                   cudaStream_t st);
+// out = (xor_in ^) a * in blockwise (n blocks; in == out allowed); Y holds the
+// leaf FFT passes' intermediate for `batch` planes.
+int qck_dual_lpn(const QcfTables *leaf, int e, const void *ahat, const cuot_block *in, const cuot_block *xor_in,
+                 cuot_block *out, void *scratch, void *Y, int batch, cudaStream_t st);
 int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
                      uint64_t col_hi, void *out, cudaStream_t st);
 }  // namespace cuot

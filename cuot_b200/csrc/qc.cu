@@ -712,11 +712,23 @@ static int default_batch(uint64_t n, int nplanes) {
 }
 
 // ---- backend selection -------------------------------------------------------
-// The fp64 FFT (qc_fft.cu) for n <= 2^20 unless the context asks for the NTT.
-static bool use_fft(const cuot_ctx *ctx, int e) { return ctx->qc_backend != 1 && qcf_supported(e); }
+// Transform of the dual LPN of n = 2^e: the fp64 FFT (qc_fft.cu) up to 2^20,
+// GF(2) Karatsuba over it (qc_kara.cu) for 2^21 and 2^22, the NTT above and
+// whenever the context asks for it.  Plane encodes (cuot_qc_encode and
+// cuot_qc_plan_encode) take the FFT or the NTT.
+enum QcKind { kQcNtt = 0, kQcFft = 1, kQcKara = 2 };
+
+static QcKind dual_kind(const cuot_ctx *ctx, int e) {
+  if (ctx->qc_backend == 1) return kQcNtt;
+  if (qcf_supported(e)) return kQcFft;
+  if (qck_supported(e)) return kQcKara;
+  return kQcNtt;
+}
+
+static QcKind plane_kind(const cuot_ctx *ctx, int e) { return dual_kind(ctx, e) == kQcFft ? kQcFft : kQcNtt; }
 
 // Intermediate bytes of a pass over `batch` planes: 4 bytes per plane and
-// coefficient for both backends (the FFT packs 4 planes in 16 bytes, in
+// coefficient for both transforms (the FFT packs 4 planes in 16 bytes, in
 // whole transforms, and builds A_hat in one 16n-byte transform).
 static uint64_t y_bytes(bool fft, int e, int batch) {
   if (!fft) return uint64_t(batch) << (e + 2);
@@ -724,17 +736,53 @@ static uint64_t y_bytes(bool fft, int e, int batch) {
   return (b < 4 ? 4 : b) << (e + 2);
 }
 
+// Planes per pass of the Karatsuba leaves (2^20-point FFTs).
+static int leaf_batch(const cuot_ctx *ctx) {
+  return ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(1ull << kQcfMaxE, 128);
+}
+
+// Bytes of A_hat: NTT n Shoup pairs; FFT n complex doubles; Karatsuba the
+// 3^L leaf transforms, followed (with_planes) by the NTT's for plane encodes.
+static uint64_t ahat_bytes(QcKind k, int e, bool with_planes) {
+  if (k == kQcFft) return 16ull << e;
+  if (k == kQcKara) return qck_ahat_bytes(e) + (with_planes ? 8ull << e : 0);
+  return 8ull << e;
+}
+
+// Scratch of the A_hat build.
+static uint64_t ahat_scratch_bytes(QcKind k, int e) {
+  if (k == kQcFft) return 16ull << e;
+  if (k == kQcKara) {
+    const uint64_t kb = qck_bits_scratch_bytes(e) + (16ull << kQcfMaxE);
+    return kb > (4ull << e) ? kb : (4ull << e);
+  }
+  return 4ull << e;
+}
+
+// Scratch of a dual LPN (rate 1, or rate 1/2 with r2): the planes / tile
+// words (and the 2n-bit planes of the rate-1/2 form) or the Karatsuba
+// split blocks, then the pass intermediate.
+static uint64_t dual_scratch_bytes(const cuot_ctx *ctx, QcKind k, int e, int batch, bool r2) {
+  if (k == kQcKara) return qck_scratch_bytes(e) + y_bytes(true, kQcfMaxE, leaf_batch(ctx));
+  return ((r2 ? 32ull : 16ull) << e) + y_bytes(k == kQcFft, e, batch);
+}
+static uint64_t dual_y_offset(QcKind k, int e, bool r2) {
+  if (k == kQcKara) return qck_scratch_bytes(e);
+  return (r2 ? 32ull : 16ull) << e;
+}
+
 struct QcEngine {
-  bool fft;
-  QcTables *t;
-  QcfTables *f;
+  QcKind kind;
+  QcTables *t;   // NTT tables (NTT, and Karatsuba plans' plane encodes)
+  QcfTables *f;  // FFT tables (FFT: of n; Karatsuba: of the 2^20 leaves)
 };
 
-static int engine(cuot_ctx *ctx, int e, bool fft, QcEngine *g) {
-  g->fft = fft;
+static int engine(cuot_ctx *ctx, int e, QcKind kind, QcEngine *g) {
+  g->kind = kind;
   g->t = nullptr;
   g->f = nullptr;
-  if (fft) return qcf_get_tables(ctx, e, &g->f);
+  if (kind == kQcFft) return qcf_get_tables(ctx, e, &g->f);
+  if (kind == kQcKara) CUOT_TRY(qcf_get_tables(ctx, kQcfMaxE, &g->f));
   CUOT_TRY(get_tables(ctx, e, &g->t));
   return set_attrs(g->t);
 }
@@ -746,90 +794,116 @@ static QcfAhatTab single_tab(const void *ahat) {
   return tab;
 }
 
-// A_hat of `a` (NTT: n Shoup pairs; FFT: n complex doubles) using Y as scratch.
-static int eng_ahat(const QcEngine &g, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
-  if (g.fft) return qcf_build_ahat(g.f, a_d, Y, ahat, st);
-  return build_ahat(g.t, a_d, static_cast<uint32_t *>(Y), static_cast<uint2 *>(ahat), st);
+// A_hat of `a` into ahat (ahat_bytes(kind, e, with_planes)); scr holds
+// ahat_scratch_bytes(kind, e).
+static int eng_ahat(const QcEngine &g, int e, const uint64_t *a_d, void *scr, void *ahat, bool with_planes,
+                    cudaStream_t st) {
+  if (g.kind == kQcFft) return qcf_build_ahat(g.f, a_d, scr, ahat, st);
+  if (g.kind == kQcKara) {
+    const uint64_t bb = qck_bits_scratch_bytes(e);
+    CUOT_TRY(qck_build_ahat(g.f, e, a_d, scr, static_cast<uint8_t *>(scr) + bb, ahat, st));
+    if (!with_planes) return CUOT_OK;
+    ahat = static_cast<uint8_t *>(ahat) + qck_ahat_bytes(e);
+  }
+  return build_ahat(g.t, a_d, static_cast<uint32_t *>(scr), static_cast<uint2 *>(ahat), st);
 }
 
 // Planes p < nplanes: in + p * stride -> out + p * stride (64-bit words),
-// written or XORed into (accumulate).
-static int eng_encode(const QcEngine &g, const void *ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
+// written or XORed into (accumulate).  A Karatsuba plan encodes planes with
+// the NTT A_hat stored after its leaves.
+static int eng_encode(const QcEngine &g, int e, const void *ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
                       int accumulate, int nplanes, void *Y, int batch, cudaStream_t st) {
-  if (g.fft) return qcf_encode(g.f, single_tab(ahat), in, out, stride, accumulate, nplanes, Y, batch, st);
+  if (g.kind == kQcFft) return qcf_encode(g.f, single_tab(ahat), in, out, stride, accumulate, nplanes, Y, batch, st);
+  if (g.kind == kQcKara) ahat = static_cast<const uint8_t *>(ahat) + qck_ahat_bytes(e);
   return encode_planes_strided(g.t, static_cast<const uint2 *>(ahat), in, out, stride, accumulate, nplanes,
                                static_cast<uint32_t *>(Y), batch, st);
 }
 
-// Dual LPN of n blocks in place: transpose to 128 planes (the FFT: to its
-// tile layout), encode, transpose back.  planes: 16n bytes.
-static int eng_dual_lpn(const QcEngine &g, int e, const void *ahat, cuot_block *io_d, uint8_t *planes, void *Y,
-                        int batch, cudaStream_t st) {
+// Dual LPN of n blocks: out = (xor_in ^) a * in blockwise; r2 = the rate-1/2
+// form (in holds 2n blocks: out = in[0, n) ^ a * in[n, 2n)).  scr holds
+// dual_scratch_bytes.
+static int eng_dual(cuot_ctx *ctx, const QcEngine &g, int e, const void *ahat, const cuot_block *in, cuot_block *out,
+                    bool r2, uint8_t *scr, int batch, cudaStream_t st) {
   const uint64_t n = 1ull << e;
-  if (g.fft) {
-    uint32_t *tiles = reinterpret_cast<uint32_t *>(planes);
-    CUOT_TRY(qcf_gather(e, io_d, tiles, st));
+  void *Y = scr + dual_y_offset(g.kind, e, r2);
+  const cuot_block *src = r2 ? in + n : in;
+  const cuot_block *xor_in = r2 ? in : nullptr;
+  if (g.kind == kQcKara) return qck_dual_lpn(g.f, e, ahat, src, xor_in, out, scr, Y, leaf_batch(ctx), st);
+  if (g.kind == kQcFft) {
+    uint32_t *tiles = reinterpret_cast<uint32_t *>(scr);
+    CUOT_TRY(qcf_gather(e, src, tiles, st));
     CUOT_TRY(qcf_encode_tiles(g.f, single_tab(ahat), tiles, 32, Y, batch, st));
-    return qcf_scatter(e, tiles, nullptr, io_d, st);
+    return qcf_scatter(e, tiles, xor_in, out, st);
   }
-  uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
-  CUOT_TRY(transpose_launch(io_d, n, 16, 0, 128, planes, st));
-  CUOT_TRY(eng_encode(g, ahat, pl, pl, n / 64, 0, 128, Y, batch, st));
-  return transpose_launch(planes, 128, n / 8, 0, n, io_d, st);
-}
-
-// Rate-1/2 dual LPN: out[i] = in[i] ^ (a * in[n..2n))[i] blockwise, i < n.
-// planes: 128 planes of 2n bits (stride n/32 words).
-static int eng_dual_lpn_r2(const QcEngine &g, int e, const void *ahat, const cuot_block *in_d, cuot_block *out_d,
-                           uint8_t *planes, void *Y, int batch, cudaStream_t st) {
-  const uint64_t n = 1ull << e;
-  if (g.fft) {
-    uint32_t *tiles = reinterpret_cast<uint32_t *>(planes);
-    CUOT_TRY(qcf_gather(e, in_d + n, tiles, st));
-    CUOT_TRY(qcf_encode_tiles(g.f, single_tab(ahat), tiles, 32, Y, batch, st));
-    return qcf_scatter(e, tiles, in_d, out_d, st);
+  uint64_t *pl = reinterpret_cast<uint64_t *>(scr);
+  if (!r2) {
+    CUOT_TRY(transpose_launch(in, n, 16, 0, 128, scr, st));
+    CUOT_TRY(eng_encode(g, e, ahat, pl, pl, n / 64, 0, 128, Y, batch, st));
+    return transpose_launch(scr, 128, n / 8, 0, n, out, st);
   }
-  uint64_t *pl = reinterpret_cast<uint64_t *>(planes);
-  CUOT_TRY(transpose_launch(in_d, 2 * n, 16, 0, 128, planes, st));
-  CUOT_TRY(eng_encode(g, ahat, pl + n / 64, pl, n / 32, 1, 128, Y, batch, st));
-  return transpose_launch(planes, 128, n / 4, 0, n, out_d, st);
+  // 128 planes of 2n bits (stride n/32 words); e1's product XORed into e0's
+  CUOT_TRY(transpose_launch(in, 2 * n, 16, 0, 128, scr, st));
+  CUOT_TRY(eng_encode(g, e, ahat, pl + n / 64, pl, n / 32, 1, 128, Y, batch, st));
+  return transpose_launch(scr, 128, n / 4, 0, n, out, st);
 }
 
 // ---- helpers for the batched engine (batch.cu) ----------------------------
 int qc_prepare(cuot_ctx *ctx, int e) {
   QcEngine g;
-  return engine(ctx, e, use_fft(ctx, e), &g);
+  return engine(ctx, e, dual_kind(ctx, e), &g);
 }
 
-uint64_t qc_ahat_bytes(const cuot_ctx *ctx, int e) { return (use_fft(ctx, e) ? 16ull : 8ull) << e; }
+uint64_t qc_ahat_bytes(const cuot_ctx *ctx, int e) { return ahat_bytes(dual_kind(ctx, e), e, false); }
 
-uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch) { return y_bytes(use_fft(ctx, e), e, batch); }
+uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch) {
+  const QcKind k = dual_kind(ctx, e);
+  const uint64_t y = k == kQcKara ? dual_scratch_bytes(ctx, k, e, batch, false) : y_bytes(k == kQcFft, e, batch);
+  const uint64_t a = ahat_scratch_bytes(k, e);
+  return y > a ? y : a;
+}
 
 int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
   QcEngine g;
-  CUOT_TRY(engine(ctx, e, use_fft(ctx, e), &g));
-  return eng_ahat(g, a_d, Y, ahat, st);
+  CUOT_TRY(engine(ctx, e, dual_kind(ctx, e), &g));
+  return eng_ahat(g, e, a_d, Y, ahat, false, st);
 }
 
 int qc_job_to_layout(const cuot_ctx *ctx, int e, const cuot_block *in, void *job, cudaStream_t st) {
-  if (use_fft(ctx, e)) return qcf_gather(e, in, static_cast<uint32_t *>(job), st);
+  const QcKind k = dual_kind(ctx, e);
+  if (k == kQcFft) return qcf_gather(e, in, static_cast<uint32_t *>(job), st);
+  if (k == kQcKara) {
+    if (cudaMemcpyAsync(job, in, 16ull << e, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return launch_status(0);
+    return CUOT_OK;
+  }
   return transpose_launch(in, 1ull << e, 16, 0, 128, job, st);
 }
 
 int qc_job_from_layout(const cuot_ctx *ctx, int e, const void *job, cuot_block *out, cudaStream_t st) {
-  if (use_fft(ctx, e)) return qcf_scatter(e, static_cast<const uint32_t *>(job), nullptr, out, st);
+  const QcKind k = dual_kind(ctx, e);
+  if (k == kQcFft) return qcf_scatter(e, static_cast<const uint32_t *>(job), nullptr, out, st);
+  if (k == kQcKara) {
+    if (cudaMemcpyAsync(out, job, 16ull << e, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return launch_status(0);
+    return CUOT_OK;
+  }
   return transpose_launch(job, 128, (1ull << e) / 8, 0, 1ull << e, out, st);
 }
 
-// Encodes `njobs` consecutive jobs (16n bytes each: 128 planes, or the FFT's
-// tile layout) in place; job j uses ahats[j] (host array of device
-// pointers).  Y holds qc_y_bytes(batch).
+// Encodes `njobs` consecutive jobs (16n bytes each: 128 planes, the FFT's
+// tile layout, or the blocks themselves for Karatsuba) in place; job j uses
+// ahats[j] (host array of device pointers).  Y holds qc_y_bytes(batch).
 int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void *const *ahats, void *Y,
                    int batch, cudaStream_t st) {
   QcEngine g;
-  CUOT_TRY(engine(ctx, e, use_fft(ctx, e), &g));
+  CUOT_TRY(engine(ctx, e, dual_kind(ctx, e), &g));
   const uint64_t n = 1ull << e;
-  if (g.fft) {
+  if (g.kind == kQcKara) {
+    for (int j = 0; j < njobs; j++) {
+      cuot_block *blk = reinterpret_cast<cuot_block *>(planes) + uint64_t(j) * n;
+      CUOT_TRY(eng_dual(ctx, g, e, ahats[j], blk, blk, false, static_cast<uint8_t *>(Y), batch, st));
+    }
+    return CUOT_OK;
+  }
+  if (g.kind == kQcFft) {
     int bt = batch < 4 ? 1 : batch / 4;
     if (bt > 32 * 15) bt = 32 * 15;  // a launch may span at most 16 jobs
     uint32_t *tiles = reinterpret_cast<uint32_t *>(planes);
@@ -875,7 +949,7 @@ struct cuot_qc_plan {
   cuot_ctx *ctx;
   int e;
   uint64_t n;
-  bool fft;
+  QcKind kind;
   void *ahat;
   int batch;
 };
@@ -910,13 +984,13 @@ int cuot_qc_plan_create(cuot_ctx *ctx, const uint64_t *a_d, uint64_t n, void *st
   int e;
   CUOT_TRY(check_n(n, &e));
   DeviceGuard dg(ctx);
-  cuot_qc_plan *pl = new cuot_qc_plan{ctx, e, n, use_fft(ctx, e), nullptr, 0};
+  cuot_qc_plan *pl = new cuot_qc_plan{ctx, e, n, dual_kind(ctx, e), nullptr, 0};
   QcEngine g;
-  int st = engine(ctx, e, pl->fft, &g);
-  if (st == CUOT_OK) st = dev_alloc(&pl->ahat, (pl->fft ? 16 : 8) * n);
+  int st = engine(ctx, e, pl->kind, &g);
+  if (st == CUOT_OK) st = dev_alloc(&pl->ahat, ahat_bytes(pl->kind, e, true));
   void *scr = nullptr;
-  if (st == CUOT_OK) st = scratch(ctx, y_bytes(pl->fft, e, 1), &scr);
-  if (st == CUOT_OK) st = eng_ahat(g, a_d, scr, pl->ahat, static_cast<cudaStream_t>(stream));
+  if (st == CUOT_OK) st = scratch(ctx, ahat_scratch_bytes(pl->kind, e), &scr);
+  if (st == CUOT_OK) st = eng_ahat(g, e, a_d, scr, pl->ahat, true, static_cast<cudaStream_t>(stream));
   if (st != CUOT_OK) {
     if (pl->ahat) cudaFree(pl->ahat);
     delete pl;
@@ -946,11 +1020,11 @@ int cuot_qc_plan_encode(cuot_qc_plan *pl, uint64_t *planes_io_d, int nplanes, vo
   cuot_ctx *ctx = pl->ctx;
   DeviceGuard dg(ctx);
   QcEngine g;
-  CUOT_TRY(engine(ctx, pl->e, pl->fft, &g));
+  CUOT_TRY(engine(ctx, pl->e, pl->kind, &g));
   const int batch = pl->batch < nplanes ? pl->batch : nplanes;
   void *scr;
-  CUOT_TRY(scratch(ctx, y_bytes(pl->fft, pl->e, batch), &scr));
-  return eng_encode(g, pl->ahat, planes_io_d, planes_io_d, pl->n / 64, 0, nplanes, scr, batch,
+  CUOT_TRY(scratch(ctx, y_bytes(pl->kind == kQcFft, pl->e, batch), &scr));
+  return eng_encode(g, pl->e, pl->ahat, planes_io_d, planes_io_d, pl->n / 64, 0, nplanes, scr, batch,
                     static_cast<cudaStream_t>(stream));
 }
 
@@ -959,13 +1033,12 @@ int cuot_qc_plan_dual_lpn(cuot_qc_plan *pl, cuot_block *io_d, void *stream) {
   cuot_ctx *ctx = pl->ctx;
   DeviceGuard dg(ctx);
   QcEngine g;
-  CUOT_TRY(engine(ctx, pl->e, pl->fft, &g));
-  const uint64_t n = pl->n;
+  CUOT_TRY(engine(ctx, pl->e, pl->kind, &g));
   const int batch = pl->batch < 128 ? pl->batch : 128;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 16 + y_bytes(pl->fft, pl->e, batch), &scr));
-  uint8_t *planes = static_cast<uint8_t *>(scr);
-  return eng_dual_lpn(g, pl->e, pl->ahat, io_d, planes, planes + n * 16, batch, static_cast<cudaStream_t>(stream));
+  CUOT_TRY(scratch(ctx, dual_scratch_bytes(ctx, pl->kind, pl->e, batch, false), &scr));
+  return eng_dual(ctx, g, pl->e, pl->ahat, io_d, io_d, false, static_cast<uint8_t *>(scr), batch,
+                  static_cast<cudaStream_t>(stream));
 }
 
 int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *pl, const cuot_block *in_d, cuot_block *out_d, void *stream) {
@@ -973,14 +1046,12 @@ int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *pl, const cuot_block *in_d, cuot_bloc
   cuot_ctx *ctx = pl->ctx;
   DeviceGuard dg(ctx);
   QcEngine g;
-  CUOT_TRY(engine(ctx, pl->e, pl->fft, &g));
-  const uint64_t n = pl->n;
+  CUOT_TRY(engine(ctx, pl->e, pl->kind, &g));
   const int batch = pl->batch < 128 ? pl->batch : 128;
   void *scr;
-  CUOT_TRY(scratch(ctx, n * 32 + y_bytes(pl->fft, pl->e, batch), &scr));
-  uint8_t *planes = static_cast<uint8_t *>(scr);
-  return eng_dual_lpn_r2(g, pl->e, pl->ahat, in_d, out_d, planes, planes + n * 32, batch,
-                         static_cast<cudaStream_t>(stream));
+  CUOT_TRY(scratch(ctx, dual_scratch_bytes(ctx, pl->kind, pl->e, batch, true), &scr));
+  return eng_dual(ctx, g, pl->e, pl->ahat, in_d, out_d, true, static_cast<uint8_t *>(scr), batch,
+                  static_cast<cudaStream_t>(stream));
 }
 
 int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, uint64_t n,
@@ -990,57 +1061,51 @@ int cuot_qc_encode(cuot_ctx *ctx, const uint64_t *a_d, uint64_t *planes_io_d, ui
   CUOT_TRY(check_n(n, &e));
   DeviceGuard dg(ctx);
   QcEngine g;
-  const bool fft = use_fft(ctx, e);
-  CUOT_TRY(engine(ctx, e, fft, &g));
+  const QcKind kind = plane_kind(ctx, e);
+  CUOT_TRY(engine(ctx, e, kind, &g));
   int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, nplanes);
   if (batch > nplanes) batch = nplanes;
-  const uint64_t ab = (fft ? 16 : 8) * n;
+  const uint64_t ab = ahat_bytes(kind, e, false);
   void *scr;
-  CUOT_TRY(scratch(ctx, ab + y_bytes(fft, e, batch), &scr));
+  CUOT_TRY(scratch(ctx, ab + y_bytes(kind == kQcFft, e, batch), &scr));
   void *Y = static_cast<uint8_t *>(scr) + ab;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(eng_ahat(g, a_d, Y, scr, st));
-  return eng_encode(g, scr, planes_io_d, planes_io_d, n / 64, 0, nplanes, Y, batch, st);
+  CUOT_TRY(eng_ahat(g, e, a_d, Y, scr, false, st));
+  return eng_encode(g, e, scr, planes_io_d, planes_io_d, n / 64, 0, nplanes, Y, batch, st);
+}
+
+// One-shot dual LPN (both forms): A_hat and the dual LPN's scratch in the
+// context's arena.
+static int one_shot_dual(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *in_d, cuot_block *out_d, uint64_t n,
+                         bool r2, void *stream) {
+  int e;
+  CUOT_TRY(check_n(n, &e));
+  DeviceGuard dg(ctx);
+  QcEngine g;
+  const QcKind kind = dual_kind(ctx, e);
+  CUOT_TRY(engine(ctx, e, kind, &g));
+  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
+  if (batch > 128) batch = 128;
+  const uint64_t ab = ahat_bytes(kind, e, false), ds = dual_scratch_bytes(ctx, kind, e, batch, r2);
+  const uint64_t as = ahat_scratch_bytes(kind, e);
+  void *scr;
+  CUOT_TRY(scratch(ctx, ab + (ds > as ? ds : as), &scr));
+  uint8_t *work = static_cast<uint8_t *>(scr) + ab;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUOT_TRY(eng_ahat(g, e, a_d, work, scr, false, st));
+  return eng_dual(ctx, g, e, scr, in_d, out_d, r2, work, batch, st);
 }
 
 int cuot_sot_dual_lpn(cuot_ctx *ctx, const uint64_t *a_d, cuot_block *io_d, uint64_t n,
                       void *stream) {
   if (!ctx || !a_d || !io_d) return fail(CUOT_EINVAL, "bad argument");
-  int e;
-  CUOT_TRY(check_n(n, &e));
-  DeviceGuard dg(ctx);
-  QcEngine g;
-  const bool fft = use_fft(ctx, e);
-  CUOT_TRY(engine(ctx, e, fft, &g));
-  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
-  if (batch > 128) batch = 128;
-  const uint64_t ab = (fft ? 16 : 8) * n;
-  void *scr;
-  CUOT_TRY(scratch(ctx, ab + n * 16 + y_bytes(fft, e, batch), &scr));
-  uint8_t *planes = static_cast<uint8_t *>(scr) + ab;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(eng_ahat(g, a_d, planes + n * 16, scr, st));
-  return eng_dual_lpn(g, e, scr, io_d, planes, planes + n * 16, batch, st);
+  return one_shot_dual(ctx, a_d, io_d, io_d, n, false, stream);
 }
 
 int cuot_sot_dual_lpn_r2(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *in_d, uint64_t n,
                          cuot_block *out_d, void *stream) {
   if (!ctx || !a_d || !in_d || !out_d) return fail(CUOT_EINVAL, "bad argument");
-  int e;
-  CUOT_TRY(check_n(n, &e));
-  DeviceGuard dg(ctx);
-  QcEngine g;
-  const bool fft = use_fft(ctx, e);
-  CUOT_TRY(engine(ctx, e, fft, &g));
-  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
-  if (batch > 128) batch = 128;
-  const uint64_t ab = (fft ? 16 : 8) * n;
-  void *scr;
-  CUOT_TRY(scratch(ctx, ab + n * 32 + y_bytes(fft, e, batch), &scr));
-  uint8_t *planes = static_cast<uint8_t *>(scr) + ab;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  CUOT_TRY(eng_ahat(g, a_d, planes + n * 32, scr, st));
-  return eng_dual_lpn_r2(g, e, scr, in_d, out_d, planes, planes + n * 32, batch, st);
+  return one_shot_dual(ctx, a_d, in_d, out_d, n, true, stream);
 }
 
 int cuot_qc_encode_sparse(cuot_ctx *ctx, const uint64_t *a_d, const uint64_t *pos_d, int weight,

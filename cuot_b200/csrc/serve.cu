@@ -266,7 +266,10 @@ int cuot_server_create(int device, const cuot_server_config *cfg, cuot_server **
   const uint64_t nmax = 1ull << max_log_n;
   // per slot: PPRF levels (16n) or dual LPN (8n transform + 16n planes + the
   // NTT batch, up to 512 MiB), plus the QC twiddle tables of every size
-  const uint64_t scratch = 24 * nmax + std::max<uint64_t>(4 * nmax, 512ull << 20) + (64ull << 20);
+  // (n = 2^21 and 2^22 dual LPNs run as Karatsuba over 2^20 FFTs: their
+  // leaf transforms, split blocks and pass intermediate need up to 778 MiB)
+  uint64_t scratch = 24 * nmax + std::max<uint64_t>(4 * nmax, 512ull << 20) + (64ull << 20);
+  if (max_log_n >= 21) scratch = std::max<uint64_t>(scratch, 832ull << 20);
   uint64_t tables = 0;
   for (int e = 10; e <= max_log_n; e++) tables += 16 * (1ull << e) + 32 * (1ull << (e / 2 + 1));
   int lo_prio = 0, hi_prio = 0;

@@ -1,9 +1,10 @@
-"""The two transforms of the exact QC encode -- the fp64 FFT (four planes
-per complex transform, default for n <= 2^20) and the NTT mod 469762049 --
-against the oracle and against each other: every supported FFT size, plane
-counts that leave a partial transform, the maximum-magnitude inputs (all-ones
-`a` and planes: every convolution coefficient equals its bound n), the
-rate-1/2 form with odd batches, and the full 128-plane dual LPN at n = 2^20."""
+"""The transforms of the exact QC encode -- the fp64 FFT (four planes per
+complex transform, default for n <= 2^20), GF(2) Karatsuba over it (dual LPN
+at n = 2^21, 2^22) and the NTT mod 469762049 -- against the oracle and
+against each other: every supported FFT size, plane counts that leave a
+partial transform, the maximum-magnitude inputs (all-ones `a` and planes:
+every convolution coefficient equals its bound n), the rate-1/2 form with odd
+batches, the full 128-plane dual LPN at n = 2^20, and the Karatsuba sizes."""
 import numpy as np
 import pytest
 
@@ -111,3 +112,76 @@ def test_backend_key_is_checked(ctx):
     import cuot_b200
     with pytest.raises(cuot_b200.CuotError):
         ctx.set_tuning(ctx.TUNE_QC_BACKEND, 3)
+
+
+def _ctx(backend):
+    import cuot_b200
+    c = cuot_b200.Context(0)
+    c.set_tuning(c.TUNE_QC_BACKEND, backend)
+    return c
+
+
+@pytest.mark.parametrize("e", [21, 22])
+def test_karatsuba_sizes_match_ntt_and_oracle(e):
+    """n = 2^21 / 2^22 dual LPN: the default backend (GF(2) Karatsuba over
+    2^20 FFTs: one / two levels) gives the NTT's blocks, one-shot and
+    through a plan, and sampled planes match the oracle's product."""
+    n = 1 << e
+    rng = np.random.default_rng(900 + e)
+    x = rng_blocks(rng, n)
+    key = rng_blocks(rng, 1)[0]
+    outs = {}
+    for name, b in (("ntt", NTT), ("auto", 0)):
+        c = _ctx(b)
+        a = gen_a(c, key, n)
+        d = to_dev(x)
+        c.sot_dual_lpn(a, d, n)
+        outs[name] = to_host(d)
+        if name == "auto":
+            plan = c.qc_plan(a, n)
+            d2 = to_dev(x)
+            plan.dual_lpn(d2)
+            outs["plan"] = to_host(d2)
+            # plane encodes through the same plan (NTT A_hat kept beside the leaves)
+            pl = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)[:2].copy()
+            dp = to_dev(pl.view(np.int64))
+            plan.encode(dp, 2)
+            outs["plan_planes"] = to_host(dp).view(np.uint64)
+            del plan
+        a_np = to_host(a).view(np.uint64)
+        torch.cuda.synchronize()
+        c.close()
+    assert np.array_equal(outs["auto"], outs["ntt"])
+    assert np.array_equal(outs["plan"], outs["ntt"])
+    planes = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    outp = oracle.bit_transpose(outs["auto"], n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    for r in (0, 77):
+        assert np.array_equal(outp[r], oracle.gf2_cyclic_mul(a_np, planes[r], n))
+    for r in (0, 1):
+        assert np.array_equal(outs["plan_planes"][r], outp[r])
+
+
+def test_karatsuba_rate_half():
+    """Rate-1/2 form at n = 2^21 through the Karatsuba path: out = e0 ^ a*e1,
+    also with out aliasing the first n input blocks."""
+    n = 1 << 21
+    rng = np.random.default_rng(2121)
+    x = rng_blocks(rng, 2 * n)
+    c = _ctx(0)
+    a = gen_a(c, rng_blocks(rng, 1)[0], n)
+    out = torch.empty((n, 16), dtype=torch.uint8, device="cuda")
+    c.sot_dual_lpn_r2(a, to_dev(x), n, out)
+    d = to_dev(x)
+    plan = c.qc_plan(a, n)
+    plan.dual_lpn_r2(d, d[:n])
+    got, got2 = to_host(out), to_host(d)[:n]
+    a_np = to_host(a).view(np.uint64)
+    del plan
+    torch.cuda.synchronize()
+    c.close()
+    assert np.array_equal(got, got2)
+    p0 = oracle.bit_transpose(x[:n].copy(), n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    p1 = oracle.bit_transpose(x[n:].copy(), n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    po = oracle.bit_transpose(got, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    for r in (3, 100):
+        assert np.array_equal(po[r], p0[r] ^ oracle.gf2_cyclic_mul(a_np, p1[r], n))
