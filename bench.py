@@ -266,7 +266,17 @@ NCU_TRAFFIC_PER_STEP = {
     "sot_n20_ntt:dual_lpn": 3990.2e6,
 }
 
-QC_FFT_MAX_LOG_N = 20  # the fp64 FFT encodes n <= 2^20 (exactness bound); the NTT the rest
+QC_FFT_MAX_LOG_N = 20  # the fp64 FFT encodes n <= 2^20 (exactness bound)
+QC_KARA_MAX_LOG_N = 22  # dual LPNs up to 2^22: GF(2) Karatsuba over 2^20 FFTs; the NTT above
+
+
+def qc_leaves(lg: int) -> int:
+    """2^20-point FFT dual LPNs behind one dual LPN of n = 2^lg (0: NTT)."""
+    if lg <= QC_FFT_MAX_LOG_N:
+        return 1
+    if lg <= QC_KARA_MAX_LOG_N:
+        return 3 ** (lg - QC_FFT_MAX_LOG_N)
+    return 0
 QC_BACKENDS = {"auto": 0, "ntt": 1, "fft": 2}
 _qc_backend = 0
 
@@ -288,8 +298,10 @@ def qc_transform_work(ns) -> dict:
     flops = bfly = 0
     for n in ns:
         lg = n.bit_length() - 1
-        if lg <= QC_FFT_MAX_LOG_N:
-            flops += 2 * 32 * (2 * 5 * n * lg + 6 * n)
+        leaves = qc_leaves(lg)
+        if leaves:
+            m, lm = min(n, 1 << QC_FFT_MAX_LOG_N), min(lg, QC_FFT_MAX_LOG_N)
+            flops += leaves * 2 * 32 * (2 * 5 * m * lm + 6 * m)
         else:
             bfly += 2 * 128 * 2 * (n // 2) * lg
     return {"fft_fp64_flops": flops, "ntt_butterflies": bfly}
@@ -297,8 +309,9 @@ def qc_transform_work(ns) -> dict:
 
 def qc_transform_report(ns, ms: float) -> dict:
     w = qc_transform_work(ns)
-    out = {"backend": "fft (n <= 2^20) / ntt (larger n)", "stage_ms": ms, **w,
-           "model": "fft: 5 n log2 n flops per complex transform + 6n per product; ntt: n/2 log2 n butterflies"}
+    out = {"backend": "fft (n <= 2^20) / karatsuba over 2^20 ffts (2^21, 2^22) / ntt (larger n)", "stage_ms": ms, **w,
+           "model": "fft: 5 m log2 m flops per complex m-point transform + 6m per product, 3^L leaves of "
+                    "m = 2^20 for the Karatsuba sizes; ntt: n/2 log2 n butterflies"}
     if w["fft_fp64_flops"] and not w["ntt_butterflies"]:
         out["fp64_tflops"] = w["fft_fp64_flops"] / (ms / 1e3) / 1e12
         out["fp64_peak_nominal_tflops"] = 37.0
@@ -636,9 +649,14 @@ def run_batch(args):
     # have no capture (null)
     traffic = None
     if dom == "sot_encode":
-        per_cot = {True: NCU_TRAFFIC_PER_STEP["sot_n20:dual_lpn"] / (1 << 20),
-                   False: NCU_TRAFFIC_PER_STEP["sot_n20_ntt:dual_lpn"] / (1 << 20)}
-        traffic = sum(i.n * per_cot[i.n.bit_length() - 1 <= QC_FFT_MAX_LOG_N] for i in insts if i.kind != KIND_FERRET)
+        fft_leaf = NCU_TRAFFIC_PER_STEP["sot_n20:dual_lpn"]  # one 2^20 FFT dual LPN, both roles
+        ntt_cot = NCU_TRAFFIC_PER_STEP["sot_n20_ntt:dual_lpn"] / (1 << 20)
+        traffic = 0.0
+        for i in insts:
+            if i.kind == KIND_FERRET:
+                continue
+            leaves = qc_leaves(i.n.bit_length() - 1)
+            traffic += fft_leaf * leaves * min(i.n, 1 << 20) / (1 << 20) if leaves else i.n * ntt_cot
     props = torch.cuda.get_device_properties(local)
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
     aes_peak = props.multi_processor_count * 32 * mhz * 1e6 / 160
@@ -665,8 +683,9 @@ def run_batch(args):
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": alg[dom],
-                     "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu captures "
-                              "by SOT COTs (FFT sizes 3,863, NTT sizes 3,805 DRAM bytes per COT, cold cache per kernel)"},
+                     "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu captures: "
+                              "3,863 DRAM bytes per COT for FFT sizes, 3^L times a 2^20 FFT dual LPN for the "
+                              "Karatsuba sizes, 3,805 per COT for NTT sizes (cold cache per kernel)"},
         "aes_roofline": aes,
         "qc_transform": qc_transform_report([i.n for i in insts if i.kind != KIND_FERRET], stages["sot_encode"]),
         "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
