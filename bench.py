@@ -323,6 +323,23 @@ AES_PEAK_MODEL = ("T-table AES: 160 shared-memory lookups per block (10 rounds x
                   "32-lane lookup wavefront per clock per SM; peak = SMs x 32 x median SM clock / 160")
 
 
+LPN_L1_MODEL = ("L1 wavefronts per LPN row: index-AES table lookups (145 per block for d = 10 blocks of a "
+                "4-row group plus 15 shared round-1 lookups, i.e. (145 d + 15) / 4 per row, 32 lanes per "
+                "wavefront) + d random 16-byte kk gathers (one line, one wavefront each) + the row's 16-byte "
+                "read and write (1/8 wavefront each); peak rows/s = SMs x median SM clock / wavefronts per row")
+
+
+def lpn_l1_roofline(rows: int, d: int, ms: float, clocks: dict, props) -> dict:
+    """LPN rows per second against the L1 wavefront bound the index AES and
+    the kk gathers share (both go through the L1/shared data pipe)."""
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    per_row = (145 * d + 15) / 4 / 32 + d + 0.25
+    peak = props.multi_processor_count * mhz * 1e6 / per_row
+    achieved = rows / (ms / 1e3)
+    return {"rows_per_step": rows, "rows_per_s": achieved, "peak_rows_per_s": peak, "frac": achieved / peak,
+            "wavefronts_per_row": per_row, "model": LPN_L1_MODEL}
+
+
 def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
     """AES blocks per second of the AES-bound stages against the T-table
     lookup roofline (the integer-pipe figure that bounds the PPRF and the
@@ -337,6 +354,8 @@ def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
     for k, cnt in counts.items():
         a = cnt / (stages[k][0] / 1e3)
         res[k] = {"aes_per_step": cnt, "aes_per_s": a, "frac": a / peak}
+    if "lpn" in counts and inst.d == 10:
+        res["lpn_l1_roofline"] = lpn_l1_roofline(2 * inst.n, inst.d, stages["lpn"][0], clocks, props)
     return res
 
 
@@ -667,6 +686,9 @@ def run_batch(args):
     for k, cnt in aes_counts.items():
         a = cnt / (stages[k] / 1e3)
         aes[k] = {"aes_per_step": cnt, "aes_per_s": a, "frac": a / aes_peak}
+    fer_rows = sum(2 * i.n for i in insts if i.kind == KIND_FERRET and i.d == 10)
+    if fer_rows and stages.get("lpn"):
+        aes["lpn_l1_roofline"] = lpn_l1_roofline(fer_rows, 10, stages["lpn"], clocks, props)
     out = {
         "metric": metric_name(args.workload),
         "value": world * cots / (ms / 1e3), "unit": "COTs/s", "n_gpus": world, "steps": args.steps,
