@@ -359,14 +359,24 @@ def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
     return res
 
 
-def e2e_inputs(inst: Instance, host):
+def device_inputs(inst: Instance, slot: int = 0) -> dict:
+    """Device input buffers of input set `slot`: set 0 is the instance's own,
+    set 1 a second copy for double-buffered host steps (HostPipeline
+    input_sets=2)."""
+    names = ["roots", "choice"] + (["kk_s", "kk_r"] if inst.spec["kind"] == "ferret" else ["b0", "b1", "mc"])
+    base = {k: getattr(inst, "d_" + k) for k in names}
+    if slot == 0:
+        return base
+    if not hasattr(inst, "_din1"):
+        inst._din1 = {k: v.clone() for k, v in base.items()}
+    return inst._din1
+
+
+def e2e_inputs(inst: Instance, host, slot: int = 0):
     """(pinned host tensor, device tensor) pairs of one step's inputs."""
-    pairs = [(host["roots"], inst.d_roots), (host["choice"], inst.d_choice)]
-    if inst.spec["kind"] == "ferret":
-        pairs += [(host["kk_s"], inst.d_kk_s), (host["kk_r"], inst.d_kk_r)]
-    else:
-        pairs += [(host["b0"], inst.d_b0), (host["b1"], inst.d_b1), (host["mc"], inst.d_mc)]
-    return pairs
+    din = device_inputs(inst, slot)
+    names = ["roots", "choice"] + (["kk_s", "kk_r"] if inst.spec["kind"] == "ferret" else ["b0", "b1", "mc"])
+    return [(host[k], din[k]) for k in names]
 
 
 def e2e_outputs(inst: Instance, host):
@@ -377,30 +387,31 @@ def e2e_outputs(inst: Instance, host):
     return pairs
 
 
-def e2e_compute(inst: Instance, host, stream) -> int:
-    """The step's device work through the public API on `stream`.  Ferret's
-    level sums and secret sums go to the host inside the step, as in
-    dev_layer.cu:40-41,50; returns those bytes."""
+def e2e_compute(inst: Instance, host, stream, slot: int = 0) -> int:
+    """The step's device work through the public API on `stream`, reading
+    input set `slot`.  Ferret's level sums and secret sums go to the host
+    inside the step, as in dev_layer.cu:40-41,50; returns those bytes."""
     torch = inst.torch
+    din = device_inputs(inst, slot)
     d2h = 0
     with torch.cuda.stream(stream):
         if inst.spec["kind"] == "ferret":
-            inst.sctx.ferret_pprf_sender(inst.d_roots, inst.h, inst.delta, inst.leaves_s, inst.lsum, inst.rsum,
+            inst.sctx.ferret_pprf_sender(din["roots"], inst.h, inst.delta, inst.leaves_s, inst.lsum, inst.rsum,
                                          inst.ss, stream=stream)
             for k, d in (("lsum", inst.lsum), ("rsum", inst.rsum), ("ss", inst.ss)):
                 host[k].copy_(d, non_blocking=True)
                 d2h += host[k].numel()
-            torch.where(inst.d_choice.view(-1, 1).bool(), inst.rsum, inst.lsum, out=inst.mc)
-            inst.rctx.ferret_pprf_recver(inst.mc, inst.d_choice, inst.ss, inst.h, inst.leaves_r, stream=stream)
+            torch.where(din["choice"].view(-1, 1).bool(), inst.rsum, inst.lsum, out=inst.mc)
+            inst.rctx.ferret_pprf_recver(inst.mc, din["choice"], inst.ss, inst.h, inst.leaves_r, stream=stream)
             if inst.mal:
                 inst.sctx.ferret_chi_sum(inst.leaves_s, inst.h, inst.d_chiseed, inst.chi_v, stream=stream)
                 inst.rctx.ferret_chi_sum(inst.leaves_r, inst.h, inst.d_chiseed, inst.chi_w, stream=stream)
-            inst.sctx.lpn_primal(inst.seed, inst.d_kk_s, inst.leaves_s, d=inst.d, stream=stream)
-            inst.rctx.lpn_primal(inst.seed, inst.d_kk_r, inst.leaves_r, d=inst.d, stream=stream)
+            inst.sctx.lpn_primal(inst.seed, din["kk_s"], inst.leaves_s, d=inst.d, stream=stream)
+            inst.rctx.lpn_primal(inst.seed, din["kk_r"], inst.leaves_r, d=inst.d, stream=stream)
         else:
-            inst.sctx.sot_pprf_sender(inst.d_roots, inst.h, inst.delta, inst.d_b0, inst.d_b1, inst.leaves_s,
+            inst.sctx.sot_pprf_sender(din["roots"], inst.h, inst.delta, din["b0"], din["b1"], inst.leaves_s,
                                       inst.m0, inst.m1, stream=stream)
-            inst.rctx.sot_pprf_recver(inst.m0, inst.m1, inst.d_mc, inst.d_choice, inst.t, inst.h, inst.leaves_r,
+            inst.rctx.sot_pprf_recver(inst.m0, inst.m1, din["mc"], din["choice"], inst.t, inst.h, inst.leaves_r,
                                       stream=stream)
             n = inst.n
             if inst.r2:
@@ -619,34 +630,42 @@ def run_batch(args):
     clocks = clk.stop()
     ms_plain = timed(batch.run_plain)
 
-    # e2e: inputs from pinned host memory, outputs back, through the public API
+    # e2e: inputs from pinned host memory, outputs back, through the public
+    # API.  Two device input sets (a second batch over copies of the inputs,
+    # same outputs): step j's input copy runs during step j-1.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    host_in, host_out = [], []
-    for i in insts:
-        ins = [(pin(i.roots), i.d_roots), (pin(i.choice), i.d_choice)]
-        if i.kind == KIND_FERRET:
-            ins += [(pin(i.kk_s), i.d_kk_s), (pin(i.kk_r), i.d_kk_r)]
-        else:
-            ins += [(pin(i.base0), i.d_b0), (pin(i.base1), i.d_b1), (pin(i.mc), i.d_mc)]
+    insts2 = [i.input_copy() for i in insts]
+    batch2 = Batch(ctx, insts2, use_graph=True, **tuned)
+    batch2.run(stream)
+    batches = [batch, batch2]
+    host_in, host_out = [[], []], []
+    for i, i2 in zip(insts, insts2):
+        names = ["roots", "choice"] + (["kk_s", "kk_r"] if i.kind == KIND_FERRET else ["base0", "base1", "mc"])
+        dev = {"roots": "d_roots", "choice": "d_choice", "kk_s": "d_kk_s", "kk_r": "d_kk_r",
+               "base0": "d_b0", "base1": "d_b1", "mc": "d_mc"}
+        for k in names:
+            hs = pin(getattr(i, k))
+            host_in[0].append((hs, getattr(i, dev[k])))
+            host_in[1].append((hs, getattr(i2, dev[k])))
         outs = [(torch.empty_like(i.v, device="cpu").pin_memory(), i.v), (torch.empty_like(i.w, device="cpu").pin_memory(), i.w)]
         if i.kind != KIND_FERRET:
             outs.append((torch.empty_like(i.cbits, device="cpu").pin_memory(), i.cbits))
-        host_in += ins
         host_out += outs
-    h2d = sum(hs.numel() * hs.element_size() for hs, _ in host_in)
+    h2d = sum(hs.numel() * hs.element_size() for hs, _ in host_in[0])
     d2h = sum(hs.numel() * hs.element_size() for hs, _ in host_out)
 
     # the host copy of step i overlaps step i+1's compute (HostPipeline)
     from cuot_b200.pipeline import HostPipeline
-    pipe = HostPipeline([dv for _, dv in host_out], stream=stream)
+    pipe = HostPipeline([dv for _, dv in host_out], stream=stream, input_sets=2)
 
-    def run_flushed(st):
+    def run_flushed(st, slot):
         with torch.cuda.stream(st):
             flush.zero_()  # L2 flush between steps, as in the device-timed loop
-        batch.run(st)
+        batches[slot].run(st)
 
     def e2e(st):
-        pipe.step(host_in, run_flushed, [hs for hs, _ in host_out])
+        slot = pipe.slot
+        pipe.step(host_in[slot], lambda s: run_flushed(s, slot), [hs for hs, _ in host_out])
 
     e2e(stream)
     pipe.join()
@@ -716,6 +735,7 @@ def run_batch(args):
         "clocks": clocks,
     }
     batch.close()
+    batch2.close()
     if args.serve_requests > 0:
         out["served"] = run_served(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -932,16 +952,19 @@ def run_ours(args):
     host = make_host(inst)
     stream = torch.cuda.Stream()
     outs = e2e_outputs(inst, host)
-    pipe = HostPipeline([d for d, _ in outs], stream=stream)
+    # two device input sets: step j's input copy runs during step j-1
+    pipe = HostPipeline([d for d, _ in outs], stream=stream, input_sets=2)
 
-    def compute(st, extra):
+    def compute(st, extra, slot):
         with torch.cuda.stream(st):
             flush.zero_()  # L2 flush between steps, as in the device-timed loop
-        extra.append(e2e_compute(inst, host, st))
+        extra.append(e2e_compute(inst, host, st, slot))
 
     def e2e_one():
         extra = []
-        h2d, d2h = pipe.step(e2e_inputs(inst, host), lambda st: compute(st, extra), [h for _, h in outs])
+        slot = pipe.slot
+        h2d, d2h = pipe.step(e2e_inputs(inst, host, slot), lambda st: compute(st, extra, slot),
+                             [h for _, h in outs])
         return h2d, d2h + extra[0]
     for _ in range(max(1, args.warmup)):
         e2e_one()

@@ -66,6 +66,19 @@ class Instance:
             self.d_punct = dev(self.punct)
             self.cbits = torch.empty(self.n // 64, dtype=torch.int64, device="cuda")
 
+    INPUTS = {KIND_FERRET: ("d_roots", "d_choice", "d_kk_s", "d_kk_r"),
+              KIND_SOT: ("d_roots", "d_choice", "d_b0", "d_b1", "d_mc")}
+
+    def input_copy(self) -> "Instance":
+        """The same instance with its own copy of the per-step device inputs
+        (same outputs and polynomial): a second batch over these copies lets
+        host steps double-buffer their inputs (HostPipeline input_sets=2)."""
+        import copy
+        other = copy.copy(self)
+        for name in self.INPUTS[self.kind]:
+            setattr(other, name, getattr(self, name).clone())
+        return other
+
     def item(self) -> BatchItem:
         it = BatchItem()
         it.kind, it.h, it.t = self.kind, self.h, self.t

@@ -33,3 +33,33 @@ def test_pipeline_keeps_every_steps_results(ctx):
         assert (h[0] == 11 * i + 1).all()
         exp = oracle.prg(bytes([11 * i + 1] * 16), 1024)
         assert np.array_equal(h[1:1024], exp[1:1024])
+
+
+def test_double_buffered_inputs_reach_their_own_step(ctx):
+    """input_sets = 2: step j's input copy runs on its own stream while step
+    j-1 computes; every step must still see its own inputs (a copy that
+    overtook the last reader of its buffer set would show up as another
+    step's seed)."""
+    from cuot_b200.pipeline import HostPipeline
+    n = 1 << 22
+    out = torch.empty((n, 16), dtype=torch.uint8, device="cuda")
+    seed_d = [torch.empty((1, 16), dtype=torch.uint8, device="cuda") for _ in range(2)]
+    st = torch.cuda.Stream()
+    pipe = HostPipeline([out], stream=st, input_sets=2)
+    steps = 6
+    hosts = [torch.empty((n, 16), dtype=torch.uint8).pin_memory() for _ in range(steps)]
+    seeds = [torch.full((1, 16), 7 * i + 3, dtype=torch.uint8).pin_memory() for i in range(steps)]
+
+    def compute(s, slot):
+        # a long kernel first, so the next step's input copy has time to overtake
+        ctx.prg_fill(bytes(16), out, stream=s)
+        with torch.cuda.stream(s):
+            out[0].copy_(seed_d[slot][0])
+    for i in range(steps):
+        slot = pipe.slot
+        assert slot == i % 2
+        pipe.step([(seeds[i], seed_d[slot])], lambda s, slot=slot: compute(s, slot), [hosts[i]])
+    pipe.join()
+    st.synchronize()
+    for i in range(steps):
+        assert (hosts[i].numpy()[0] == 7 * i + 3).all(), i
