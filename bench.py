@@ -340,6 +340,39 @@ def lpn_l1_roofline(rows: int, d: int, ms: float, clocks: dict, props) -> dict:
             "wavefronts_per_row": per_row, "model": LPN_L1_MODEL}
 
 
+def transpose_roofline(inst: Instance, flush, peaks: dict, peak_kind: str, reps: int = 10) -> dict:
+    """The 128-plane bit transpose (cuot_bit_transpose, blocks -> planes and
+    back) of the instance's n blocks against HBM: 32n algorithmic bytes per
+    direction (16n read + 16n write), L2 flushed before each timed call."""
+    torch = inst.torch
+    res = {}
+    for tag, n in (("config", inst.n), ("streaming_2^24", 1 << 24)):
+        src = inst.leaves_s[:n] if n <= inst.leaves_s.shape[0] else \
+            torch.randint(0, 256, (n, 16), dtype=torch.uint8, device="cuda")
+        planes = torch.empty((n, 16), dtype=torch.uint8, device="cuda")
+        back = torch.empty_like(planes)
+        for name, fn in (("blocks_to_planes", lambda: inst.sctx.bit_transpose(src, n, 16, 0, 128, planes)),
+                         ("planes_to_blocks", lambda: inst.sctx.bit_transpose(planes, 128, n // 8, 0, n, back))):
+            fn()
+            ms = 0.0
+            for _ in range(reps):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                fn()
+                b.record()
+                torch.cuda.synchronize()
+                ms += a.elapsed_time(b) / reps
+            gbs = 32 * n / (ms / 1e3) / 1e9
+            res[f"{tag}:{name}"] = {"n": n, "ms": ms, "achieved_gbs": gbs, "frac": gbs / peaks["hbm_gbs"]}
+        del planes, back, src
+    res.update({"algorithmic_bytes": "32n per direction", "peak_gbs": peaks["hbm_gbs"],
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "note": "the standalone transpose of the reference's operator surface; the FFT dual LPN uses "
+                        "its own gather/scatter into the column-tile layout instead"})
+    return res
+
+
 def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
     """AES blocks per second of the AES-bound stages against the T-table
     lookup roofline (the integer-pipe figure that bounds the PPRF and the
@@ -1026,6 +1059,8 @@ def run_ours(args):
         "clocks": clocks,
     }
     out["aes_roofline"] = aes_roofline(inst, stages, clocks, torch.cuda.get_device_properties(local))
+    if inst.spec["kind"] == "sot":
+        out["transpose"] = transpose_roofline(inst, flush, peaks, peak_kind)
     if inst.spec["kind"] == "sot":
         out["qc_transform"] = qc_transform_report([inst.n], lpn_ms)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

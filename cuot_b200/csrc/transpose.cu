@@ -29,7 +29,7 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
 }
 
 constexpr int kTrThreads = 256;     // 8 warps
-constexpr int kTrGroups = 32;       // row groups of 32 rows per CTA
+constexpr int kTrGroups = 32;       // row groups of 32 rows per CTA (128 B of each plane row)
 constexpr int kTrStride = kTrGroups + 1;
 
 // blocks -> planes.  in: rows x 16 bytes.  out: nplanes rows of rows/8 bytes.
@@ -41,11 +41,19 @@ __global__ void __launch_bounds__(kTrThreads) tr_blocks_to_planes(
   const uint64_t ngroups = rows / 32;
   const uint64_t g0 = uint64_t(blockIdx.x) * kTrGroups;
   const int wlo = col_lo / 32, nw = nplanes / 32;
-  for (int gg = warp; gg < kTrGroups; gg += kTrThreads / 32) {
-    const uint64_t g = g0 + gg;
-    if (g >= ngroups) break;
-    const uint4 v = __ldcs(in + g * 32 + lane);
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+  // all of a warp's row groups are loaded before any is transposed, so each
+  // warp keeps kPer loads in flight
+  constexpr int kPer = kTrGroups / (kTrThreads / 32);
+  uint4 v[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; j++) {
+    const uint64_t g = g0 + warp + j * (kTrThreads / 32);
+    v[j] = g < ngroups ? __ldcs(in + g * 32 + lane) : make_uint4(0, 0, 0, 0);
+  }
+#pragma unroll
+  for (int j = 0; j < kPer; j++) {
+    const int gg = warp + j * (kTrThreads / 32);
+    const uint32_t w[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       if (q < wlo || q >= wlo + nw) continue;
@@ -57,7 +65,9 @@ __global__ void __launch_bounds__(kTrThreads) tr_blocks_to_planes(
   const uint64_t words_per_plane = rows / 32;
   const int gvalid = int(ngroups - g0 < uint64_t(kTrGroups) ? ngroups - g0 : uint64_t(kTrGroups));
   for (int p = warp; p < nplanes; p += kTrThreads / 32) {
-    if (lane < gvalid) out[uint64_t(p) * words_per_plane + g0 + lane] = st[p * kTrStride + lane];
+#pragma unroll
+    for (int x = lane; x < kTrGroups; x += 32)
+      if (x < gvalid) out[uint64_t(p) * words_per_plane + g0 + x] = st[p * kTrStride + x];
   }
 }
 
@@ -71,8 +81,24 @@ __global__ void __launch_bounds__(kTrThreads) tr_planes_to_blocks(
   const uint64_t ngroups = ncols / 32;
   const uint64_t g0 = uint64_t(blockIdx.x) * kTrGroups;
   const int gvalid = int(ngroups - g0 < uint64_t(kTrGroups) ? ngroups - g0 : uint64_t(kTrGroups));
-  for (int p = warp; p < nrows; p += kTrThreads / 32)
-    if (lane < gvalid) st[p * kTrStride + lane] = __ldcs(in + uint64_t(p) * in_row_words + g0 + lane);
+  // each warp's plane rows are loaded together (up to 16 loads in flight per
+  // 32-word chunk of the rows)
+  constexpr int kPer = 128 / (kTrThreads / 32);
+#pragma unroll
+  for (int x0 = 0; x0 < kTrGroups; x0 += 32) {
+    const int x = x0 + lane;
+    uint32_t v[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int p = warp + j * (kTrThreads / 32);
+      v[j] = (p < nrows && x < gvalid) ? __ldcs(in + uint64_t(p) * in_row_words + g0 + x) : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int p = warp + j * (kTrThreads / 32);
+      if (p < nrows && x < gvalid) st[p * kTrStride + x] = v[j];
+    }
+  }
   __syncthreads();
   const int nq = nrows / 32;
   for (int gg = warp; gg < gvalid; gg += kTrThreads / 32) {
