@@ -1,4 +1,8 @@
-// qc.cu -- exact quasi-cyclic encode over GF(2)[x]/(x^n - 1) (SOT dual LPN).
+// qc.cu -- exact quasi-cyclic encode over GF(2)[x]/(x^n - 1) (SOT dual LPN):
+// the entry points, the choice of transform per size (the fp64 FFT of
+// qc_fft.cu up to 2^20, GF(2) Karatsuba over it in qc_kara.cu for dual LPNs
+// at 2^21 and 2^22, the number-theoretic transform below otherwise), the
+// sparse encode and the AES-CTR helpers.
 //
 // The reference multiplies with float32 cuFFT and recovers bits by truncating
 // the unnormalised result (silent/quasi_cyclic.cu:34-49, 118-128), which is

@@ -55,10 +55,11 @@ uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
  *   CUOT_TUNE_QC_PLANES     planes per QC pass, 0 = automatic (512 MiB of
  *                           intermediate)
  *   CUOT_TUNE_QC_BACKEND    transform of the exact QC encode: 0 automatic
- *                           (fp64 FFT for n <= 2^20, else NTT), 1 NTT mod
- *                           469762049, 2 FFT where n <= 2^20.  Plans and
- *                           batches keep the backend they were created with;
- *                           set it before creating them. */
+ *                           (fp64 FFT for n <= 2^20; dual LPNs at 2^21 and
+ *                           2^22 as GF(2) Karatsuba over 2^20 FFTs; the NTT
+ *                           mod 469762049 above), 1 the NTT everywhere, 2 as
+ *                           0.  Plans and batches keep the backend they were
+ *                           created with; set it before creating them. */
 #define CUOT_TUNE_PPRF_THREADS 1
 #define CUOT_TUNE_QC_PLANES 2
 #define CUOT_TUNE_QC_BACKEND 3
@@ -225,9 +226,11 @@ int cuot_ferret_chi_sum(cuot_ctx *ctx, const cuot_block *leaves_d, uint64_t t,
  * gpu/gpu_ops.cu:102-109).  encode: every plane r (n bits, planes
  * consecutive) becomes a * plane_r mod (x^n - 1) over GF(2), exactly
  * (replaces the float cuFFT path of QuasiCyclic::encode_dense,
- * quasi_cyclic.cu:118-128).  n a power of two in [2^10, 2^25] (the
- * row pass keeps 2^ceil(log n / 2) twiddle pairs of both directions in
- * shared memory).
+ * quasi_cyclic.cu:118-128).  n a power of two in [2^10, 2^25].  The
+ * product is an fp64 FFT carrying four planes per transform for n <= 2^20
+ * (exact: the rounding error of the convolution stays below 1/2), GF(2)
+ * Karatsuba over that FFT for dual LPNs at 2^21 and 2^22, and a number-
+ * theoretic transform mod 469762049 otherwise (CUOT_TUNE_QC_BACKEND).
  * encode_sparse: out = a * e mod (x^n - 1), e = indicator of pos_d[0..w)
  * (QuasiCyclic::encode_sparse, quasi_cyclic.cu:130-161).
  * dual_lpn: io_d holds n blocks; block j becomes XOR_{i: a_i = 1}
@@ -281,8 +284,8 @@ int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *plan, const cuot_block *in_d,
  * one device program: one persistent PPRF launch over all trees of all
  * senders (per-tree work queue, deepest trees first), one over all
  * receivers, one persistent LPN launch over all Ferret rows of both roles,
- * and for SOT one set of NTT passes per transform size spanning the planes
- * of every instance of that size.  On first run the whole program is
+ * and for SOT one set of QC transform passes per transform size spanning
+ * the planes of every instance of that size.  On first run the whole program is
  * captured into a CUDA graph (cfg.use_graph) and replayed afterwards.
  * No counterpart call in the reference, which runs one instance per call
  * (FerretCOT::extend, ferret_cot.hpp:80-91; SOT roles, silent/roles.h).
@@ -320,7 +323,7 @@ typedef struct {
   int pprf_threads;        /* threads per tree CTA: 128 or 256 (0: 256) */
   int ctas_per_sm;         /* persistent PPRF/LPN grid: CTAs per SM (0: 3) */
   int lpn_rows_per_task;   /* LPN work-queue granularity, multiple of 4 (0: 65536) */
-  int qc_planes_per_pass;  /* planes per NTT pass (0: ~64 MiB of intermediate) */
+  int qc_planes_per_pass;  /* planes per QC pass (0: 512 MiB of intermediate) */
   int use_graph;           /* capture into a CUDA graph on first run */
 } cuot_batch_config;
 
