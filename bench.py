@@ -431,8 +431,10 @@ def e2e_compute(inst: Instance, host, stream, slot: int = 0) -> int:
         if inst.spec["kind"] == "ferret":
             inst.sctx.ferret_pprf_sender(din["roots"], inst.h, inst.delta, inst.leaves_s, inst.lsum, inst.rsum,
                                          inst.ss, stream=stream)
+            # the sums go to the host mid-step through SM stores: a DMA copy
+            # would wait behind the previous step's outputs on the copy engine
             for k, d in (("lsum", inst.lsum), ("rsum", inst.rsum), ("ss", inst.ss)):
-                host[k].copy_(d, non_blocking=True)
+                inst.cb.copy_to_host(d, host[k], stream=stream)
                 d2h += host[k].numel()
             torch.where(din["choice"].view(-1, 1).bool(), inst.rsum, inst.lsum, out=inst.mc)
             inst.rctx.ferret_pprf_recver(inst.mc, din["choice"], inst.ss, inst.h, inst.leaves_r, stream=stream)

@@ -57,6 +57,18 @@ def declared_symbols() -> list[str]:
     return sorted(set(re.findall(r"\b(cuot_[a-z0-9_]+)\s*\(", txt)))
 
 
+def copy_to_host(src, dst, stream=None):
+    """Device tensor -> pinned host tensor through SM stores
+    (cuot_copy_to_host): does not queue behind copy-engine transfers."""
+    if not src.is_cuda or dst.is_cuda or not dst.is_pinned():
+        raise ValueError("expected a CUDA source and a pinned host destination")
+    nbytes = src.numel() * src.element_size()
+    if dst.numel() * dst.element_size() < nbytes or not src.is_contiguous() or not dst.is_contiguous():
+        raise ValueError("destination too small or not contiguous")
+    _check(load().cuot_copy_to_host(ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr()),
+                                    ctypes.c_uint64(nbytes), _stream(stream)), "cuot_copy_to_host")
+
+
 def _check(status: int, where: str):
     if status != 0:
         raise CuotError(status, where)

@@ -170,6 +170,17 @@ int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t
   return launch_status();
 }
 
+// Device -> mapped host memory through SM stores (16-byte words when both
+// ends and the size allow it, bytes otherwise).
+__global__ void host_store16(const uint4 *__restrict__ src, uint4 *__restrict__ dst, uint64_t n) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    dst[i] = __ldg(&src[i]);
+}
+__global__ void host_store1(const uint8_t *__restrict__ src, uint8_t *__restrict__ dst, uint64_t n) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+}
+
 }  // namespace cuot
 
 using namespace cuot;
@@ -186,4 +197,25 @@ extern "C" int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows
   DeviceGuard g(ctx);
   return transpose_launch(in_d, rows, row_bytes, col_lo, col_hi, out_d,
                           static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int cuot_copy_to_host(const void *src_d, void *dst_h, uint64_t bytes, void *stream) {
+  if (bytes == 0) return CUOT_OK;
+  if (!src_d || !dst_h) return fail(CUOT_EINVAL, "null argument");
+  void *dst = nullptr;
+  if (cudaHostGetDevicePointer(&dst, dst_h, 0) != cudaSuccess || !dst) {
+    cudaGetLastError();
+    return fail(CUOT_EINVAL, "destination is not mapped pinned host memory");
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool v16 = (reinterpret_cast<uintptr_t>(src_d) % 16 == 0) && (reinterpret_cast<uintptr_t>(dst) % 16 == 0) &&
+                   bytes % 16 == 0;
+  const uint64_t n = v16 ? bytes / 16 : bytes;
+  uint64_t grid = (n + 255) / 256;
+  if (grid > 148 * 8) grid = 148 * 8;
+  if (v16)
+    host_store16<<<unsigned(grid), 256, 0, st>>>(static_cast<const uint4 *>(src_d), static_cast<uint4 *>(dst), n);
+  else
+    host_store1<<<unsigned(grid), 256, 0, st>>>(static_cast<const uint8_t *>(src_d), static_cast<uint8_t *>(dst), n);
+  return launch_status();
 }

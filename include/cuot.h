@@ -176,6 +176,20 @@ int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
                        uint64_t row_bytes, uint64_t col_lo, uint64_t col_hi,
                        void *out_d, void *stream);
 
+/* ---- host transfer -----------------------------------------------------------
+ * Copies `bytes` of device memory to mapped pinned host memory with the SMs'
+ * own stores instead of a copy engine.  For the small results a caller needs
+ * on the host in the middle of a step (the level and secret sums that
+ * cuda_mpcot_sender returns, dev_layer.cu:40-41): on B200 a DMA copy waits
+ * behind every copy already queued on the engines, in either direction, so
+ * with the previous step's outputs still streaming to the host (hundreds of
+ * MB) it would hold the step up; this copy does not queue there.  dst_h must
+ * be pinned and mapped (cudaHostAlloc / cudaMallocHost, or cudaHostRegister
+ * with cudaHostRegisterMapped); otherwise CUOT_EINVAL.  Stream-ordered on the
+ * current device; the bytes are in host memory once the stream passes an
+ * event recorded after the call.  No counterpart call in the reference. */
+int cuot_copy_to_host(const void *src_d, void *dst_h, uint64_t bytes, void *stream);
+
 /* ---- Ferret session: set-up + rcot buffer loop -------------------------------
  * FerretCOT's data flow (ferret_cot.hpp:99-210) with both parties on one GPU
  * and an ideal transport between them (the receiver's MPCOT OT messages are

@@ -63,3 +63,26 @@ def test_double_buffered_inputs_reach_their_own_step(ctx):
     st.synchronize()
     for i in range(steps):
         assert (hosts[i].numpy()[0] == 7 * i + 3).all(), i
+
+
+def test_copy_to_host_through_sm_stores(ctx):
+    """cuot_copy_to_host: device bytes land in pinned host memory, with
+    16-byte and byte-granular paths (aligned and odd sizes / offsets), two
+    calls in a row; an unpinned destination is refused."""
+    import cuot_b200
+    rng = np.random.default_rng(3)
+    for nbytes in (16 * 4097, 1000003):
+        src = torch.from_numpy(rng.integers(0, 256, nbytes, dtype=np.uint8)).cuda()
+        dst = torch.zeros(nbytes + 1, dtype=torch.uint8).pin_memory()
+        for view in (dst[:nbytes], dst[1:]):
+            view.zero_()
+            cuot_b200.copy_to_host(src, view)
+            torch.cuda.synchronize()
+            assert np.array_equal(view.numpy(), src.cpu().numpy())
+    import ctypes
+    pageable = np.zeros(64, np.uint8)
+    st = cuot_b200.load().cuot_copy_to_host(ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(pageable.ctypes.data),
+                                            ctypes.c_uint64(64), None)
+    assert st == 1 and b"mapped" in cuot_b200.load().cuot_last_error()
+    with pytest.raises(ValueError):
+        cuot_b200.copy_to_host(src[:16], torch.zeros(16, dtype=torch.uint8))
