@@ -717,7 +717,8 @@ def run_batch(args):
     peaks, peak_kind = measured_peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
     # traffic: the batch is too large for a multi-metric ncu capture; the SOT
-    # encode runs the same kernels as sot_n20 (FFT for n <= 2^20, NTT above),
+    # encode runs the same kernels as sot_n20 (FFT up to 2^20, Karatsuba over
+    # it at 2^21 and 2^22, NTT above),
     # whose captured DRAM bytes per COT (both roles) scale it; other stages
     # have no capture (null)
     traffic = None
@@ -1091,7 +1092,8 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--qc-backend", default="auto", choices=sorted(QC_BACKENDS),
-                    help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^20, NTT above)")
+                    help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^20, Karatsuba over it for "
+                         "dual LPNs at 2^21 and 2^22, NTT above)")
     args = ap.parse_args()
     global _qc_backend
     _qc_backend = QC_BACKENDS[args.qc_backend]

@@ -7,7 +7,7 @@ batches.  Knobs:
   pprf_threads        threads per tree CTA (128 / 256)
   ctas_per_sm         persistent-grid CTAs per SM of the batched PPRF / LPN
   lpn_rows_per_task   LPN work-queue granularity (the LPN tile)
-  qc_planes_per_pass  planes per NTT pass
+  qc_planes_per_pass  planes per QC transform pass
 The GGM expansion runs all levels of a tree in one kernel, so there is no
 separate levels-per-pass knob.
 """
@@ -99,7 +99,7 @@ def tune_batch(ctx, instances, table: TuningTable | None = None, reps: int = 2, 
 
 def tune_single(ctx, inst, table: TuningTable | None = None, reps: int = 3):
     """Tunes the single-instance knobs for one instance shape (threads per
-    tree for the PPRF; planes per NTT pass for SOT), applies the winners to
+    tree for the PPRF; planes per QC transform pass for SOT), applies the winners to
     `ctx` and records them under (kind, n, depth)."""
     import torch
     table = table or TuningTable()
