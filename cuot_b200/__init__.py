@@ -133,7 +133,7 @@ class Context:
     def scratch_bytes(self) -> int:
         return int(self.lib.cuot_ctx_scratch_bytes(self.h))
 
-    TUNE_PPRF_THREADS, TUNE_QC_PLANES, TUNE_QC_BACKEND = 1, 2, 3
+    TUNE_PPRF_THREADS, TUNE_QC_PLANES, TUNE_QC_BACKEND, TUNE_QC_STREAMS = 1, 2, 3, 4
 
     def set_tuning(self, key: int, value: int):
         _check(self.lib.cuot_ctx_set_tuning(self.h, C.c_int(key), C.c_int64(value)), "cuot_ctx_set_tuning")

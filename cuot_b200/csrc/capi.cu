@@ -89,6 +89,7 @@ int cuot_ctx_create(int device, cuot_ctx **out) {
   c->device = device;
   c->pprf_threads = 256;
   c->qc_planes_per_pass = 0;
+  c->qc_streams = 2;
   int st = CUOT_OK;
   if (cudaMalloc(&c->t0_d, 256 * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
@@ -145,6 +146,10 @@ int cuot_ctx_set_tuning(cuot_ctx *c, int key, int64_t value) {
     case CUOT_TUNE_QC_BACKEND:
       if (value < 0 || value > 2) return fail(CUOT_EINVAL, "QC backend must be 0 (automatic), 1 (NTT) or 2 (FFT)");
       c->qc_backend = int(value);
+      return CUOT_OK;
+    case CUOT_TUNE_QC_STREAMS:
+      if (value != 1 && value != 2) return fail(CUOT_EINVAL, "QC streams must be 1 or 2");
+      c->qc_streams = int(value);
       return CUOT_OK;
     default:
       return fail(CUOT_EINVAL, "unknown tuning key %d", key);

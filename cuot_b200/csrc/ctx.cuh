@@ -12,6 +12,7 @@ struct cuot_ctx {
   int pprf_threads;        // threads per tree CTA (128 or 256)
   int qc_planes_per_pass;  // 0: automatic
   int qc_backend;          // CUOT_TUNE_QC_BACKEND value: 0 automatic, 1 NTT, 2 FFT
+  int qc_streams;          // CUOT_TUNE_QC_STREAMS value: 1 or 2 (FFT group schedule)
 };
 
 namespace cuot {

@@ -594,6 +594,7 @@ __global__ void qcf_gen_fourstep(int e1, int e2, double2 *fs) {
 struct QcfTables {
   int e, e1, e2;
   double2 *T1, *T2, *fs;
+  const cuot_ctx *owner;  // context that caches the tables (its qc_streams)
   cudaStream_t aux;    // second stream of the two-stream group schedule
   cudaEvent_t ev[2];   // fork / join
 };
@@ -710,6 +711,7 @@ int qcf_get_tables(cuot_ctx *ctx, int e, QcfTables **out) {
   CUOT_TRY(set_attrs());
   QcfTables *t = new QcfTables{};
   t->e = e;
+  t->owner = ctx;
   t->e1 = qcf_e1(e);
   t->e2 = e - t->e1;
   const uint64_t N1 = 1ull << t->e1, N2 = 1ull << t->e2;
@@ -783,10 +785,12 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
   // in flight stays in L2 and one group's passes fill the other's wave tails.
   // Measured on B200 (one role's 128 planes): n = 2^20, G = 2: 0.78 ms
   // against 0.80 ms for one launch group of all 32 transforms; n = 2^18,
-  // G = 8: 0.20 against 0.23 ms.  It needs Y for 2G transforms.
+  // G = 8: 0.20 against 0.23 ms.  It needs Y for 2G transforms.  A context
+  // with CUOT_TUNE_QC_STREAMS = 1 keeps every group on the caller's stream
+  // (callers that already run several encodes at once, such as the server).
   uint64_t g64 = (32ull << 20) / ybytes;
   const int G = g64 < 1 ? 1 : int(g64);
-  if (2 * G <= bt && ntransforms > G) {
+  if (t->owner->qc_streams == 2 && 2 * G <= bt && ntransforms > G) {
     cudaEventRecord(t->ev[0], st);
     cudaStreamWaitEvent(t->aux, t->ev[0], 0);
     int g = 0;

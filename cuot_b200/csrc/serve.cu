@@ -284,6 +284,8 @@ int cuot_server_create(int device, const cuot_server_config *cfg, cuot_server **
   int st = CUOT_OK;
   for (auto &s : sv->slots) {
     if ((st = cuot_ctx_create(device, &s.ctx)) || (st = cuot_ctx_reserve(s.ctx, scratch))) break;
+    // the slots already overlap their requests: one stream per FFT encode
+    if ((st = cuot_ctx_set_tuning(s.ctx, CUOT_TUNE_QC_STREAMS, 1))) break;
     if (cudaStreamCreateWithPriority(&s.lo, cudaStreamNonBlocking, lo_prio) != cudaSuccess ||
         cudaStreamCreateWithPriority(&s.hi, cudaStreamNonBlocking, hi_prio) != cudaSuccess ||
         cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {

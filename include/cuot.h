@@ -59,10 +59,20 @@ uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
  *                           2^22 as GF(2) Karatsuba over 2^20 FFTs; the NTT
  *                           mod 469762049 above), 1 the NTT everywhere, 2 as
  *                           0.  Plans and batches keep the backend they were
- *                           created with; set it before creating them. */
+ *                           created with; set it before creating them.
+ *   CUOT_TUNE_QC_STREAMS    streams of one FFT encode, 1 or 2 (default 2:
+ *                           groups of about 32 MiB of intermediate alternate
+ *                           between the caller's stream and a second stream
+ *                           of the context, joined back before the call
+ *                           returns).  1 keeps all work on the caller's
+ *                           stream, for callers that already overlap several
+ *                           encodes (the server's slots).  Applies to later
+ *                           calls and plans; a graph batch keeps the value
+ *                           of its first run (the graph is captured then). */
 #define CUOT_TUNE_PPRF_THREADS 1
 #define CUOT_TUNE_QC_PLANES 2
 #define CUOT_TUNE_QC_BACKEND 3
+#define CUOT_TUNE_QC_STREAMS 4
 int cuot_ctx_set_tuning(cuot_ctx *ctx, int key, int64_t value);
 
 /* ---- AES-128 ECB ---------------------------------------------------------

@@ -4,7 +4,8 @@ at n = 2^21, 2^22) and the NTT mod 469762049 -- against the oracle and
 against each other: every supported FFT size, plane counts that leave a
 partial transform, the maximum-magnitude inputs (all-ones `a` and planes:
 every convolution coefficient equals its bound n), the rate-1/2 form with odd
-batches, the full 128-plane dual LPN at n = 2^20, and the Karatsuba sizes."""
+batches, the full 128-plane dual LPN at n = 2^20, the Karatsuba sizes, and
+the one- and two-stream FFT group schedules."""
 import numpy as np
 import pytest
 
@@ -185,3 +186,36 @@ def test_karatsuba_rate_half():
     po = oracle.bit_transpose(got, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
     for r in (3, 100):
         assert np.array_equal(po[r], p0[r] ^ oracle.gf2_cyclic_mul(a_np, p1[r], n))
+
+
+@pytest.mark.parametrize("e", [17, 20])
+def test_one_and_two_stream_encodes_agree(e):
+    """CUOT_TUNE_QC_STREAMS = 1 (every group on the caller's stream) and 2
+    (groups alternate with the context's second stream) give the oracle's
+    blocks; the key accepts only 1 and 2."""
+    import cuot_b200
+    n = 1 << e
+    rng = np.random.default_rng(1700 + e)
+    x = rng_blocks(rng, n)
+    key = rng_blocks(rng, 1)[0]
+    outs = []
+    for streams in (1, 2):
+        c = _ctx(0)
+        c.set_tuning(c.TUNE_QC_STREAMS, streams)
+        a = gen_a(c, key, n)
+        d = to_dev(x)
+        plan = c.qc_plan(a, n)
+        plan.dual_lpn(d)
+        outs.append(to_host(d))
+        a_np = to_host(a).view(np.uint64)
+        del plan
+        for bad in (0, 3):
+            with pytest.raises(cuot_b200.CuotError):
+                c.set_tuning(c.TUNE_QC_STREAMS, bad)
+        torch.cuda.synchronize()
+        c.close()
+    assert np.array_equal(outs[0], outs[1])
+    planes = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    outp = oracle.bit_transpose(outs[0], n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    for r in (0, 90):
+        assert np.array_equal(outp[r], oracle.gf2_cyclic_mul(a_np, planes[r], n))
