@@ -38,6 +38,9 @@ int scratch(cuot_ctx *ctx, uint64_t bytes, void **out);
 int pprf_init_device();
 // Frees the context's cached QC tables (qc.cu).
 void qc_free_ctx_tables(cuot_ctx *ctx);
+// Scratch bytes of the one-shot dual LPN (cuot_sot_dual_lpn, or with r2
+// cuot_sot_dual_lpn_r2) of n = 2^e on ctx (qc.cu).
+uint64_t qc_one_shot_dual_bytes(const cuot_ctx *ctx, int e, bool r2);
 // QC helpers used by the batched engine (qc.cu).  The backend (NTT or FFT)
 // of an n = 2^e encode follows the context's CUOT_TUNE_QC_BACKEND; A_hat
 // and intermediate sizes depend on it.
@@ -52,7 +55,7 @@ int qc_job_to_layout(const cuot_ctx *ctx, int e, const cuot_block *in, void *job
 int qc_job_from_layout(const cuot_ctx *ctx, int e, const void *job, cuot_block *out, cudaStream_t st);
 int qc_default_batch(uint64_t n, int nplanes);
 // FP64 FFT backend of the QC encode (qc_fft.cu): n = 2^e, 10 <= e <= kQcfMaxE.
-constexpr int kQcfMaxE = 20;
+constexpr int kQcfMaxE = 21;
 // A_hat of each transform y of a launch: p[(first + y) / per] (4 planes per transform).
 struct QcfAhatTab {
   const void *p[16];

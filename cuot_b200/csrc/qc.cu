@@ -1,7 +1,7 @@
 // qc.cu -- exact quasi-cyclic encode over GF(2)[x]/(x^n - 1) (SOT dual LPN):
 // the entry points, the choice of transform per size (the fp64 FFT of
-// qc_fft.cu up to 2^20, GF(2) Karatsuba over it in qc_kara.cu for dual LPNs
-// at 2^21 and 2^22, the number-theoretic transform below otherwise), the
+// qc_fft.cu up to 2^21, GF(2) Karatsuba over it in qc_kara.cu for dual LPNs
+// at 2^22 and 2^23, the number-theoretic transform below otherwise), the
 // sparse encode and the AES-CTR helpers.
 //
 // The reference multiplies with float32 cuFFT and recovers bits by truncating
@@ -716,8 +716,8 @@ static int default_batch(uint64_t n, int nplanes) {
 }
 
 // ---- backend selection -------------------------------------------------------
-// Transform of the dual LPN of n = 2^e: the fp64 FFT (qc_fft.cu) up to 2^20,
-// GF(2) Karatsuba over it (qc_kara.cu) for 2^21 and 2^22, the NTT above and
+// Transform of the dual LPN of n = 2^e: the fp64 FFT (qc_fft.cu) up to 2^21,
+// GF(2) Karatsuba over it (qc_kara.cu) for 2^22 and 2^23, the NTT above and
 // whenever the context asks for it.  Plane encodes (cuot_qc_encode and
 // cuot_qc_plan_encode) take the FFT or the NTT.
 enum QcKind { kQcNtt = 0, kQcFft = 1, kQcKara = 2 };
@@ -740,7 +740,7 @@ static uint64_t y_bytes(bool fft, int e, int batch) {
   return (b < 4 ? 4 : b) << (e + 2);
 }
 
-// Planes per pass of the Karatsuba leaves (2^20-point FFTs).
+// Planes per pass of the Karatsuba leaves (2^21-point FFTs).
 static int leaf_batch(const cuot_ctx *ctx) {
   return ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(1ull << kQcfMaxE, 128);
 }
@@ -778,7 +778,7 @@ static uint64_t dual_y_offset(QcKind k, int e, bool r2) {
 struct QcEngine {
   QcKind kind;
   QcTables *t;   // NTT tables (NTT, and Karatsuba plans' plane encodes)
-  QcfTables *f;  // FFT tables (FFT: of n; Karatsuba: of the 2^20 leaves)
+  QcfTables *f;  // FFT tables (FFT: of n; Karatsuba: of the 2^21 leaves)
 };
 
 static int engine(cuot_ctx *ctx, int e, QcKind kind, QcEngine *g) {
@@ -945,6 +945,19 @@ int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void
 
 int qc_default_batch(uint64_t n, int nplanes) { return default_batch(n, nplanes); }
 
+static int one_shot_batch(const cuot_ctx *ctx, uint64_t n) {
+  const int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
+  return batch > 128 ? 128 : batch;
+}
+
+// Scratch of cuot_sot_dual_lpn (r2: cuot_sot_dual_lpn_r2) at n = 2^e on ctx.
+uint64_t qc_one_shot_dual_bytes(const cuot_ctx *ctx, int e, bool r2) {
+  const QcKind kind = dual_kind(ctx, e);
+  const uint64_t ds = dual_scratch_bytes(ctx, kind, e, one_shot_batch(ctx, 1ull << e), r2);
+  const uint64_t as = ahat_scratch_bytes(kind, e);
+  return ahat_bytes(kind, e, false) + (ds > as ? ds : as);
+}
+
 }  // namespace cuot
 
 using namespace cuot;
@@ -1088,12 +1101,10 @@ static int one_shot_dual(cuot_ctx *ctx, const uint64_t *a_d, const cuot_block *i
   QcEngine g;
   const QcKind kind = dual_kind(ctx, e);
   CUOT_TRY(engine(ctx, e, kind, &g));
-  int batch = ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(n, 128);
-  if (batch > 128) batch = 128;
-  const uint64_t ab = ahat_bytes(kind, e, false), ds = dual_scratch_bytes(ctx, kind, e, batch, r2);
-  const uint64_t as = ahat_scratch_bytes(kind, e);
+  const int batch = one_shot_batch(ctx, n);
+  const uint64_t ab = ahat_bytes(kind, e, false);
   void *scr;
-  CUOT_TRY(scratch(ctx, ab + (ds > as ? ds : as), &scr));
+  CUOT_TRY(scratch(ctx, qc_one_shot_dual_bytes(ctx, e, r2), &scr));
   uint8_t *work = static_cast<uint8_t *>(scr) + ab;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   CUOT_TRY(eng_ahat(g, e, a_d, work, scr, false, st));

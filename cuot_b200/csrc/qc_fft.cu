@@ -1,31 +1,37 @@
 // qc_fft.cu -- exact quasi-cyclic encode through a double-precision complex
-// FFT (the default backend for n = 2^e, 10 <= e <= 20).
+// FFT (the default backend for n = 2^e, 10 <= e <= 21).
 //
 // out_r = a * e_r mod (x^n - 1) over GF(2) is the parity of the integer
-// cyclic convolution, whose coefficients lie in [0, n] (n <= 2^20 < 2^21).
-// Four planes share one complex transform:
-//   x_j = (e0_j + 2^21 e1_j) + i (e2_j + 2^21 e3_j),
-// and since `a` is real, IFFT(FFT(x) . FFT(a)) = (a*e0 + 2^21 a*e1) + i (a*e2
-// + 2^21 a*e3): every product coefficient is an integer below 2^42 whose
-// bits 0 and 21 are the coefficients of two planes.  The computed values
-// differ from those integers by less than 1/2, so rounding recovers them
+// cyclic convolution, whose coefficients lie in [0, n].  Four planes share
+// one complex transform, with base B = 2^21 for n <= 2^20 and B = 2^21 + 1
+// for n = 2^21 (B > n either way):
+//   x_j = (e0_j + B e1_j) + i (e2_j + B e3_j),
+// and since `a` is real, IFFT(FFT(x) . FFT(a)) = (a*e0 + B a*e1) + i (a*e2
+// + B a*e3): every product coefficient is an integer V = c0 + B c1 below
+// 2^43 with c0, c1 in [0, n], so c1 = floor(V / B) and c0 = V - B c1.  For
+// B = 2^21 the two planes' bits are bits 0 and 21 of V; for B = 2^21 + 1,
+// with hi = V >> 21, lo = V mod 2^21 and d = hi - lo, c1 = hi - [d > 0] -
+// [d > B] and c0 has the parity of lo ^ c1 (B odd).  The computed values
+// differ from the integers by less than 1/2, so rounding recovers them
 // exactly: by the error bound for FFT-based convolution (Percival,
 // "Rapid multiplication modulo the sum and difference of highly composite
 // numbers", Math. Comp. 72 (2003), Thm. 5.1) the error is at most
 // ||x||_2 ||a||_2 ((1+eps)^{3m} (1+eps sqrt5)^{3m+1} (1+beta)^{3m} - 1) with
-// m = log2 n = 20, eps = 2^-53 and twiddle error beta <= 4 eps, i.e. below
-// 2^41.5 * 436 * 2^-53 < 0.16 for n = 2^20 (smaller n: smaller bound).
+// m = log2 n, eps = 2^-53 and twiddle error beta <= 4 eps, and ||x||_2
+// ||a||_2 <= sqrt(2n) (1 + B) sqrt(n): below 2^41.5 * 436.4 * 2^-53 < 0.16
+// for n = 2^20 and 2^42.5 * 458.2 * 2^-53 < 0.32 for n = 2^21 (smaller n:
+// smaller bound).
 //
 // Work per plane and radix-2 stage is one fp64 operation (a complex
 // butterfly shared by four planes), against several integer instructions
 // per plane in the number-theoretic transform of qc.cu.
 //
-// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= 512, N1 <= N2 <= 2048), input
+// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= 512, N1 <= N2 <= 4096), input
 // index j = N2*j1 + j2, frequency k = k1 + N1*k2:
 //   A (columns): 8 columns j2 of one transform per CTA: load the plane bits,
 //     N1-point DIF FFT over j1 (frequencies land in bit-reversed row order r),
 //     multiply by w_n^(j2 * rev(r)), store Y[r][j2].
-//   B (rows): 4 rows (2 at N2 = 2048) per CTA: N2-point DIF FFT, multiply by A_hat (the
+//   B (rows): 4 rows (2 at N2 = 2048, 1 at 4096) per CTA: N2-point DIF FFT, multiply by A_hat (the
 //     transform of `a` in the same layout, scaled by 1/n), N2-point DIT
 //     inverse, store.
 //   C (columns): multiply by w_n^-(j2 * rev(r)), N1-point DIT inverse over r,
@@ -42,7 +48,7 @@ namespace cuot {
 
 constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
 
-// Radix plan of an N = 2^L point transform, 5 <= L <= 11: K bits per pass.
+// Radix plan of an N = 2^L point transform, 5 <= L <= 12: K bits per pass.
 __host__ __device__ constexpr int qcf_npass(int L) { return L <= 8 ? 2 : 3; }
 __host__ __device__ constexpr int qcf_k(int L, int p) {
   return L == 5 ? (p == 0 ? 3 : 2)
@@ -51,7 +57,8 @@ __host__ __device__ constexpr int qcf_k(int L, int p) {
        : L == 8 ? 4
        : L == 9 ? 3
        : L == 10 ? (p == 0 ? 4 : 3)
-       : (p == 2 ? 3 : 4);
+       : L == 11 ? (p == 2 ? 3 : 4)
+       : 4;
 }
 // log2 of the sub-transform size at the start of pass p
 __host__ __device__ constexpr int qcf_ls(int L, int p) { return p == 0 ? L : qcf_ls(L, p - 1) - qcf_k(L, p - 1); }
@@ -71,12 +78,18 @@ __host__ __device__ constexpr int qcf_fs_width(int e1) { return (1 << qcf_fs_lo(
 __host__ __device__ constexpr int qcf_fs_ld(int e1) { return qcf_fs_width(e1) + 1; }
 constexpr int kCols = 8;  // columns per CTA of the column passes
 // Rows per CTA of the row pass, so that two CTAs fit an SM: 4 up to 1024
-// points, 2 for 2048.
-__host__ __device__ constexpr int qcf_rows(int L) { return L >= 11 ? 2 : 4; }
+// points, 2 for 2048, 1 for 4096 (its first pass's twiddles are read
+// through L1, only the middle pass's are staged).
+__host__ __device__ constexpr int qcf_rows(int L) { return L >= 12 ? 1 : L == 11 ? 2 : 4; }
+// Row pass reads pass 0's twiddles from global memory through L1.
+__host__ __device__ constexpr bool qcf_row_tg0(int L) { return L >= 12; }
 __host__ __device__ constexpr int qcf_row_threads(int L) {
   return L >= 11 ? 256 : qcf_threads(L) / 2 < 32 ? 32 : qcf_threads(L) / 2;
 }
-// Split of n = 2^e into N1 = 2^e1 column points (at most 512, so two column
+// Packing base 2^21 + qcf_wide(e) (2^21 + 1 for n = 2^21, where a product
+// coefficient can equal 2^21).
+__host__ __device__ constexpr int qcf_wide(int e) { return e >= 21 ? 1 : 0; }
+// Split of n = 2^e into N1 = 2^e1 column points (at most 512, so three column
 // CTAs fit an SM) and N2 = 2^(e - e1) row points.
 __host__ __device__ constexpr int qcf_e1(int e) { return e / 2 < 9 ? e / 2 : 9; }
 
@@ -165,11 +178,12 @@ struct Pass {
 // q = rev_K(m) of its sub-transform; multiply by w_S^(base q) (table in pass
 // order, qcf_tw_off).
 // TG: T is in global memory (read through L1) instead of shared memory.
-template <int L, int P, bool INV, bool TG = false>
+// REL: T points at pass P's part of the table instead of its start.
+template <int L, int P, bool INV, bool TG = false, bool REL = false>
 __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int base, const double2 *T) {
   using Q = Pass<L, P>;
   if (Q::M == 1) return;
-  const double2 *Tp = T + qcf_tw_off(L, P) + base;
+  const double2 *Tp = T + (REL ? 0 : qcf_tw_off(L, P)) + base;
 #pragma unroll
   for (int m = 1; m < Q::R; m++) {
     const int q = __brev(m) >> (32 - Q::K);
@@ -180,21 +194,21 @@ __device__ __forceinline__ void pass_twiddle(double2 (&x)[Pass<L, P>::R], int ba
 
 // Shared-memory position of element i of a transform.  NT = 8 transforms per
 // CTA: rows of N + 1 values, the 8 lanes of a quarter-warp are the 8
-// transforms at one item, no swizzle.  NT = 4 (2): rows of N + 2 (N + 4)
-// values, a quarter-warp is 4 transforms x 2 consecutive items (2 x 4), and
-// XORing bits [0, 1) ([0, 2)) of i with the bits above K_last keeps both the
-// early passes (items differ in the low bits) and the last pass (items differ
-// from bit K_last up) conflict-free.
+// transforms at one item, no swizzle.  NT = 4 (2, 1): rows of N + 2 (N + 4,
+// N) values, a quarter-warp is 4 transforms x 2 consecutive items (2 x 4,
+// 1 x 8), and XORing bits [0, 1) ([0, 2), [0, 3)) of i with the bits above
+// K_last keeps both the early passes (items differ in the low bits) and the
+// last pass (items differ from bit K_last up) conflict-free.
 template <int L, int NT>
 __device__ __forceinline__ int spos(int i) {
   if constexpr (NT == 8) return i;
-  return i ^ ((i >> qcf_k(L, qcf_npass(L) - 1)) & (NT == 4 ? 1 : 3));
+  return i ^ ((i >> qcf_k(L, qcf_npass(L) - 1)) & (NT == 4 ? 1 : NT == 2 ? 3 : 7));
 }
 template <int NT>
-__host__ __device__ constexpr int sld(int N) { return NT == 8 ? N + 1 : NT == 4 ? N + 2 : N + 4; }
+__host__ __device__ constexpr int sld(int N) { return NT == 8 ? N + 1 : NT == 4 ? N + 2 : NT == 2 ? N + 4 : N; }
 
 // One pass entirely in shared memory (xs rows of sld<NT>(N) complex values).
-template <int L, int P, bool INV, int NT, bool TG = false>
+template <int L, int P, bool INV, int NT, bool TG = false, bool REL = false>
 __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
   using Q = Pass<L, P>;
   constexpr int ld = sld<NT>(1 << L);
@@ -207,9 +221,9 @@ __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
     for (int m = 0; m < Q::R; m++) x[m] = row[spos<L, NT>(i0 + Q::M * m)];
     if (!INV) {
       dif_regs<Q::K>(x);
-      pass_twiddle<L, P, false, TG>(x, Q::base(w), T);
+      pass_twiddle<L, P, false, TG, REL>(x, Q::base(w), T);
     } else {
-      pass_twiddle<L, P, true, TG>(x, Q::base(w), T);
+      pass_twiddle<L, P, true, TG, REL>(x, Q::base(w), T);
       dit_regs<Q::K>(x);
     }
 #pragma unroll
@@ -217,12 +231,13 @@ __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
   }
 }
 
-// Middle passes [1, npass - 1) forward, or in reverse order inverse.
-template <int L, bool INV, int NT, bool TG = false>
+// Middle passes [1, npass - 1) forward, or in reverse order inverse (REL:
+// T is pass 1's part of the table).
+template <int L, bool INV, int NT, bool TG = false, bool REL = false>
 __device__ __forceinline__ void middle_passes(double2 *xs, const double2 *T) {
   if constexpr (qcf_npass(L) == 3) {
     __syncthreads();
-    smem_pass<L, 1, INV, NT, TG>(xs, T);
+    smem_pass<L, 1, INV, NT, TG, REL>(xs, T);
   }
   __syncthreads();
 }
@@ -248,16 +263,17 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 }
 
 // Pass A.  grid (N2 / 8, transforms).  in: plane p at in + p * stride_bytes;
-// transform y holds planes 4y .. 4y+3 (< nplanes); one_plane: `a` (real
-// part only).  With tiles != nullptr the input is in the tile layout
+// transform y holds planes 4y .. 4y+3 (< nplanes) with base 2^21 + wide;
+// one_plane: `a` (real part only).  With tiles != nullptr the input is in the tile layout
 // instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
 // columns of the CTA's tile in row j1 (qcf_gather).
 template <int E1>
 __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_fwd(
-    const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2,
+    const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2, int wide,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     double2 *__restrict__ Y) {
   constexpr int N1 = 1 << E1, ld = N1 + 1, W = qcf_fs_ld(E1);
+  const uint32_t base = (1u << 21) + uint32_t(wide);
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
   double2 *xs = sm, *fss = xs + kCols * ld;
@@ -292,7 +308,7 @@ __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_fwd(
         if (one_plane) {
           x[m] = make_double2(double(b & 1u), 0.0);
         } else {
-          x[m] = make_double2(double((b & 1u) | ((b >> 8) & 1u) << 21), double(((b >> 16) & 1u) | ((b >> 24) & 1u) << 21));
+          x[m] = make_double2(double((b & 1u) + ((b >> 8) & 1u) * base), double(((b >> 16) & 1u) + ((b >> 24) & 1u) * base));
         }
       }
       dif_regs<Q::K>(x);
@@ -336,10 +352,16 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
   constexpr int NT = qcf_rows(E2);
   constexpr int N2 = 1 << E2, ld = sld<NT>(N2);
   constexpr int NP = qcf_npass(E2);
+  // G0: pass 0's twiddles through L1 from T2, shared memory holds pass 1's
+  constexpr bool G0 = qcf_row_tg0(E2);
   extern __shared__ double2 sm[];
   double2 *xs = sm, *Ts = xs + NT * ld;
+  const double2 *T0 = G0 ? T2 : Ts;
   const int r0 = blockIdx.x * NT;
-  stage(Ts, T2, N2);
+  if constexpr (G0)
+    stage(Ts, T2 + qcf_tw_off(E2, 1), qcf_tw_off(E2, NP - 1) - qcf_tw_off(E2, 1));
+  else
+    stage(Ts, T2, N2);
   double2 *Yp = Y + (uint64_t(blockIdx.y) << (e1 + E2)) + (uint64_t(r0) << E2);
   __syncthreads();
   {  // pass 0 from global
@@ -352,13 +374,13 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
 #pragma unroll
       for (int m = 0; m < Q::R; m++) x[m] = src[Q::M * m];
       dif_regs<Q::K>(x);
-      pass_twiddle<E2, 0, false>(x, Q::base(w), Ts);
+      pass_twiddle<E2, 0, false, G0>(x, Q::base(w), T0);
       double2 *row = xs + c * ld;
 #pragma unroll
       for (int m = 0; m < Q::R; m++) row[spos<E2, NT>(i0 + Q::M * m)] = x[m];
     }
   }
-  middle_passes<E2, false, NT>(xs, Ts);
+  middle_passes<E2, false, NT, false, G0>(xs, Ts);
   {  // last forward pass; pointwise product; first inverse pass
     using Q = Pass<E2, NP - 1>;
     const double2 *ah = mode == 0 ? static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
@@ -387,7 +409,7 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
     }
   }
   if (mode == 1) return;
-  middle_passes<E2, true, NT>(xs, Ts);
+  middle_passes<E2, true, NT, false, G0>(xs, Ts);
   {  // inverse of pass 0, to global
     using Q = Pass<E2, 0>;
     for (int it = threadIdx.x; it < NT * Q::items; it += blockDim.x) {
@@ -397,7 +419,7 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
       double2 x[Q::R];
 #pragma unroll
       for (int m = 0; m < Q::R; m++) x[m] = row[spos<E2, NT>(i0 + Q::M * m)];
-      pass_twiddle<E2, 0, true>(x, Q::base(w), Ts);
+      pass_twiddle<E2, 0, true, G0>(x, Q::base(w), T0);
       dit_regs<Q::K>(x);
       double2 *dst = Yp + (uint64_t(c) << E2) + i0;
 #pragma unroll
@@ -406,12 +428,31 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
   }
 }
 
+// The two planes' bits (c0 & 1, c1 & 1) of a rounded product coefficient
+// V = c0 + B c1, B = 2^21 + wide, c0 and c1 in [0, 2^21] (see the top of the
+// file); v + 1.5 * 2^52 holds round(v) in the low 51 bits of its mantissa.
+__device__ __forceinline__ void plane_bits(double v, int wide, uint32_t &p0, uint32_t &p1) {
+  const double r = v + kRoundMagic;
+  const uint32_t lw = uint32_t(__double2loint(r));
+  if (!wide) {
+    p0 = lw & 1u;
+    p1 = (lw >> 21) & 1u;
+    return;
+  }
+  const uint32_t hw = uint32_t(__double2hiint(r)) & 0x7FFFFu;  // bits 32..50 of round(v)
+  const uint32_t lo = lw & 0x1FFFFFu, hi = (lw >> 21) | (hw << 11);
+  const int d = int(hi) - int(lo);
+  const uint32_t c1 = hi - uint32_t(d > 0) - uint32_t(d > (1 << 21) + 1);
+  p0 = (lo ^ c1) & 1u;
+  p1 = c1 & 1u;
+}
+
 // Pass C.  grid (N2 / 8, transforms).  out: plane p at out + p * stride_bytes,
 // written (accumulate == 0) or XORed into (accumulate == 1); with tiles !=
 // nullptr the result goes to the tile layout instead (one word per row).
 template <int E1>
 __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_inv(
-    const double2 *__restrict__ Y, int e2, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
+    const double2 *__restrict__ Y, int e2, int wide, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles) {
   constexpr int N1 = 1 << E1, ld = N1 + 1;
   constexpr int NP = qcf_npass(E1);
@@ -454,10 +495,9 @@ __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_inv(
       dit_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) {
-        // round(v) mod 2^32 is the low word of v + 1.5 * 2^52
-        const uint32_t re = uint32_t(__double2loint(x[m].x + kRoundMagic));
-        const uint32_t im = uint32_t(__double2loint(x[m].y + kRoundMagic));
-        const uint32_t pl[4] = {re & 1u, (re >> 21) & 1u, im & 1u, (im >> 21) & 1u};
+        uint32_t pl[4];
+        plane_bits(x[m].x, wide, pl[0], pl[1]);
+        plane_bits(x[m].y, wide, pl[2], pl[3]);
         const int j1 = i0 + Q::M * m;
         uint32_t word = 0;
 #pragma unroll
@@ -627,12 +667,14 @@ int col_smem(int e1) {
 }
 int row_smem(int e2) {
   const int N2 = 1 << e2;
-  const int ld = qcf_rows(e2) == 4 ? sld<4>(N2) : sld<2>(N2);
-  return (qcf_rows(e2) * ld + N2) * 16;
+  const int rows = qcf_rows(e2);
+  const int ld = rows == 4 ? sld<4>(N2) : rows == 2 ? sld<2>(N2) : sld<1>(N2);
+  const int tw = qcf_row_tg0(e2) ? qcf_tw_off(e2, qcf_npass(e2) - 1) - qcf_tw_off(e2, 1) : N2;
+  return (rows * ld + tw) * 16;
 }
 
 #define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9)
-#define QCF_ROW_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11)
+#define QCF_ROW_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 
 int set_attrs() {
   static bool done[64] = {false};
@@ -666,7 +708,7 @@ void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t 
 #define QCF_L(E)                                                                                            \
   case E:                                                                                                   \
     qcf_col_fwd<E><<<grid, qcf_threads(E), col_smem(E), st>>>(in, stride_bytes, nplanes, one_plane, t->e2, \
-                                                               tiles, t->T1, t->fs, Y);                     \
+                                                               qcf_wide(t->e), tiles, t->T1, t->fs, Y);     \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
@@ -690,8 +732,8 @@ void launch_col_inv(const QcfTables *t, int ntr, cudaStream_t st, const double2 
   switch (t->e1) {
 #define QCF_L(E)                                                                                          \
   case E:                                                                                                 \
-    qcf_col_inv<E><<<grid, qcf_threads(E), col_smem(E), st>>>(Y, t->e2, t->T1, t->fs, out, stride_bytes, \
-                                                               nplanes, accumulate, tiles);               \
+    qcf_col_inv<E><<<grid, qcf_threads(E), col_smem(E), st>>>(Y, t->e2, qcf_wide(t->e), t->T1, t->fs, out, \
+                                                               stride_bytes, nplanes, accumulate, tiles); \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L

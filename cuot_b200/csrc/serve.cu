@@ -264,12 +264,10 @@ int cuot_server_create(int device, const cuot_server_config *cfg, cuot_server **
   }
   const int max_log_n = cfg->max_log_n > 0 ? cfg->max_log_n : 24;
   const uint64_t nmax = 1ull << max_log_n;
-  // per slot: PPRF levels (16n) or dual LPN (8n transform + 16n planes + the
-  // NTT batch, up to 512 MiB), plus the QC twiddle tables of every size
-  // (n = 2^21 and 2^22 dual LPNs run as Karatsuba over 2^20 FFTs: their
-  // leaf transforms, split blocks and pass intermediate need up to 778 MiB)
+  // per slot: PPRF levels (16n) or the one-shot dual LPN of any size up to
+  // nmax (transform of `a`, blocks or tile words, pass intermediate; the
+  // library's own sizing), plus the QC twiddle tables of every size
   uint64_t scratch = 24 * nmax + std::max<uint64_t>(4 * nmax, 512ull << 20) + (64ull << 20);
-  if (max_log_n >= 21) scratch = std::max<uint64_t>(scratch, 832ull << 20);
   uint64_t tables = 0;
   for (int e = 10; e <= max_log_n; e++) tables += 16 * (1ull << e) + 32 * (1ull << (e / 2 + 1));
   int lo_prio = 0, hi_prio = 0;
@@ -283,9 +281,11 @@ int cuot_server_create(int device, const cuot_server_config *cfg, cuot_server **
   }
   int st = CUOT_OK;
   for (auto &s : sv->slots) {
-    if ((st = cuot_ctx_create(device, &s.ctx)) || (st = cuot_ctx_reserve(s.ctx, scratch))) break;
+    if ((st = cuot_ctx_create(device, &s.ctx))) break;
     // the slots already overlap their requests: one stream per FFT encode
     if ((st = cuot_ctx_set_tuning(s.ctx, CUOT_TUNE_QC_STREAMS, 1))) break;
+    for (int e = 10; e <= max_log_n; e++) scratch = std::max(scratch, qc_one_shot_dual_bytes(s.ctx, e, false));
+    if ((st = cuot_ctx_reserve(s.ctx, scratch))) break;
     if (cudaStreamCreateWithPriority(&s.lo, cudaStreamNonBlocking, lo_prio) != cudaSuccess ||
         cudaStreamCreateWithPriority(&s.hi, cudaStreamNonBlocking, hi_prio) != cudaSuccess ||
         cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {

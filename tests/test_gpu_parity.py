@@ -206,8 +206,10 @@ def test_qc_encode_vs_oracle(ctx, e, nplanes):
 
 @pytest.mark.parametrize("e", [21, 22, 24, 25])
 def test_qc_encode_large_sizes(ctx, e):
-    """The 2048/4096/8192-point pass kernels (n = 2^21 .. 2^25, the largest
-    size the row pass fits) against the oracle on two planes."""
+    """Plane encodes at n = 2^21 (the FFT's 4096-point row pass, packing base
+    2^21 + 1) and the NTT's 2048/4096/8192-point pass kernels (n = 2^22 ..
+    2^25, the largest size the row pass fits) against the oracle on two
+    planes."""
     n = 1 << e
     rng = np.random.default_rng(e + 1000)
     key = rng_blocks(rng, 1)[0]

@@ -1,11 +1,12 @@
 """The transforms of the exact QC encode -- the fp64 FFT (four planes per
-complex transform, default for n <= 2^20), GF(2) Karatsuba over it (dual LPN
-at n = 2^21, 2^22) and the NTT mod 469762049 -- against the oracle and
-against each other: every supported FFT size, plane counts that leave a
-partial transform, the maximum-magnitude inputs (all-ones `a` and planes:
-every convolution coefficient equals its bound n), the rate-1/2 form with odd
-batches, the full 128-plane dual LPN at n = 2^20, the Karatsuba sizes, and
-the one- and two-stream FFT group schedules."""
+complex transform, default for n <= 2^21; packing base 2^21 + 1 at 2^21),
+GF(2) Karatsuba over it (dual LPN at n = 2^22, 2^23) and the NTT mod
+469762049 -- against the oracle and against each other: every supported FFT
+size, plane counts that leave a partial transform, the maximum-magnitude
+inputs (all-ones `a` and planes: every convolution coefficient equals its
+bound n), the rate-1/2 form with odd batches, the full 128-plane dual LPN at
+n = 2^20 and 2^21, the Karatsuba sizes, and the one- and two-stream FFT group
+schedules."""
 import numpy as np
 import pytest
 
@@ -35,7 +36,7 @@ def gen_a(ctx, key, n):
 
 
 @pytest.mark.parametrize("e,nplanes", [(10, 1), (11, 3), (12, 4), (13, 5), (14, 6), (15, 9), (16, 2),
-                                       (17, 3), (18, 4), (19, 5), (20, 7)])
+                                       (17, 3), (18, 4), (19, 5), (20, 7), (21, 6)])
 def test_encode_every_size(bctx, e, nplanes):
     n = 1 << e
     rng = np.random.default_rng(500 + e)
@@ -48,7 +49,7 @@ def test_encode_every_size(bctx, e, nplanes):
     assert np.array_equal(to_host(d).view(np.uint64), exp)
 
 
-@pytest.mark.parametrize("e", [10, 16, 20])
+@pytest.mark.parametrize("e", [10, 16, 20, 21])
 def test_maximum_magnitude_inputs(bctx, e):
     """a = all ones: coefficient k of a*e is the weight of e (the same for
     every k); with e all ones every coefficient equals n, the bound the
@@ -122,11 +123,12 @@ def _ctx(backend):
     return c
 
 
-@pytest.mark.parametrize("e", [21, 22])
-def test_karatsuba_sizes_match_ntt_and_oracle(e):
-    """n = 2^21 / 2^22 dual LPN: the default backend (GF(2) Karatsuba over
-    2^20 FFTs: one / two levels) gives the NTT's blocks, one-shot and
-    through a plan, and sampled planes match the oracle's product."""
+@pytest.mark.parametrize("e", [21, 22, 23])
+def test_large_sizes_match_ntt_and_oracle(e):
+    """n = 2^21 / 2^22 / 2^23 dual LPN: the default backend (the direct FFT;
+    GF(2) Karatsuba over 2^21 FFTs, one / two levels) gives the NTT's
+    blocks, one-shot and through a plan, and sampled planes match the
+    oracle's product."""
     n = 1 << e
     rng = np.random.default_rng(900 + e)
     x = rng_blocks(rng, n)
@@ -143,7 +145,8 @@ def test_karatsuba_sizes_match_ntt_and_oracle(e):
             d2 = to_dev(x)
             plan.dual_lpn(d2)
             outs["plan"] = to_host(d2)
-            # plane encodes through the same plan (NTT A_hat kept beside the leaves)
+            # plane encodes through the same plan (FFT at 2^21; above, the NTT
+            # A_hat kept beside the Karatsuba leaves)
             pl = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)[:2].copy()
             dp = to_dev(pl.view(np.int64))
             plan.encode(dp, 2)
@@ -162,11 +165,12 @@ def test_karatsuba_sizes_match_ntt_and_oracle(e):
         assert np.array_equal(outs["plan_planes"][r], outp[r])
 
 
-def test_karatsuba_rate_half():
-    """Rate-1/2 form at n = 2^21 through the Karatsuba path: out = e0 ^ a*e1,
-    also with out aliasing the first n input blocks."""
-    n = 1 << 21
-    rng = np.random.default_rng(2121)
+@pytest.mark.parametrize("e", [21, 22])
+def test_rate_half_large(e):
+    """Rate-1/2 form at n = 2^21 (direct FFT) and 2^22 (Karatsuba): out =
+    e0 ^ a*e1, also with out aliasing the first n input blocks."""
+    n = 1 << e
+    rng = np.random.default_rng(2100 + e)
     x = rng_blocks(rng, 2 * n)
     c = _ctx(0)
     a = gen_a(c, rng_blocks(rng, 1)[0], n)
@@ -188,7 +192,7 @@ def test_karatsuba_rate_half():
         assert np.array_equal(po[r], p0[r] ^ oracle.gf2_cyclic_mul(a_np, p1[r], n))
 
 
-@pytest.mark.parametrize("e", [17, 20])
+@pytest.mark.parametrize("e", [17, 20, 21])
 def test_one_and_two_stream_encodes_agree(e):
     """CUOT_TUNE_QC_STREAMS = 1 (every group on the caller's stream) and 2
     (groups alternate with the context's second stream) give the oracle's
