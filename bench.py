@@ -266,12 +266,12 @@ NCU_TRAFFIC_PER_STEP = {
     "sot_n20_ntt:dual_lpn": 3990.2e6,
 }
 
-QC_FFT_MAX_LOG_N = 21  # the fp64 FFT encodes n <= 2^21 (exactness bound)
-QC_KARA_MAX_LOG_N = 23  # dual LPNs up to 2^23: GF(2) Karatsuba over 2^21 FFTs; the NTT above
+QC_FFT_MAX_LOG_N = 22  # the fp64 FFT encodes n <= 2^22 (exactness bound)
+QC_KARA_MAX_LOG_N = 24  # dual LPNs up to 2^24: GF(2) Karatsuba over 2^22 FFTs; the NTT above
 
 
 def qc_leaves(lg: int) -> int:
-    """FFT dual LPNs (of at most 2^21 points) behind one dual LPN of n = 2^lg
+    """FFT dual LPNs (of at most 2^22 points) behind one dual LPN of n = 2^lg
     (0: NTT)."""
     if lg <= QC_FFT_MAX_LOG_N:
         return 1
@@ -310,9 +310,9 @@ def qc_transform_work(ns) -> dict:
 
 def qc_transform_report(ns, ms: float) -> dict:
     w = qc_transform_work(ns)
-    out = {"backend": "fft (n <= 2^21) / karatsuba over 2^21 ffts (2^22, 2^23) / ntt (larger n)", "stage_ms": ms, **w,
+    out = {"backend": "fft (n <= 2^22) / karatsuba over 2^22 ffts (2^23, 2^24) / ntt (larger n)", "stage_ms": ms, **w,
            "model": "fft: 5 m log2 m flops per complex m-point transform + 6m per product, 3^L leaves of "
-                    "m = 2^21 for the Karatsuba sizes; ntt: n/2 log2 n butterflies"}
+                    "m = 2^22 for the Karatsuba sizes; ntt: n/2 log2 n butterflies"}
     if w["fft_fp64_flops"] and not w["ntt_butterflies"]:
         out["fp64_tflops"] = w["fft_fp64_flops"] / (ms / 1e3) / 1e12
         out["fp64_peak_nominal_tflops"] = 37.0
@@ -718,8 +718,8 @@ def run_batch(args):
     peaks, peak_kind = measured_peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
     # traffic: the batch is too large for a multi-metric ncu capture; the SOT
-    # encode runs the same kernels as sot_n20 (FFT up to 2^21, Karatsuba over
-    # it at 2^22 and 2^23, NTT above),
+    # encode runs the same kernels as sot_n20 (FFT up to 2^22, Karatsuba over
+    # it at 2^23 and 2^24, NTT above),
     # whose captured DRAM bytes per COT (both roles) scale it; other stages
     # have no capture (null)
     traffic = None
@@ -762,7 +762,7 @@ def run_batch(args):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": alg[dom],
                      "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu captures: "
-                              "3,863 DRAM bytes per COT for FFT sizes, 3^L times a 2^21 FFT dual LPN for the "
+                              "3,863 DRAM bytes per COT for FFT sizes, 3^L times a 2^22 FFT dual LPN for the "
                               "Karatsuba sizes, 3,805 per COT for NTT sizes (cold cache per kernel)"},
         "aes_roofline": aes,
         "qc_transform": qc_transform_report([i.n for i in insts if i.kind != KIND_FERRET], stages["sot_encode"]),
@@ -1093,8 +1093,8 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--qc-backend", default="auto", choices=sorted(QC_BACKENDS),
-                    help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^21, Karatsuba over it for "
-                         "dual LPNs at 2^22 and 2^23, NTT above)")
+                    help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^22, Karatsuba over it for "
+                         "dual LPNs at 2^23 and 2^24, NTT above)")
     args = ap.parse_args()
     global _qc_backend
     _qc_backend = QC_BACKENDS[args.qc_backend]

@@ -55,7 +55,11 @@ int qc_job_to_layout(const cuot_ctx *ctx, int e, const cuot_block *in, void *job
 int qc_job_from_layout(const cuot_ctx *ctx, int e, const void *job, cuot_block *out, cudaStream_t st);
 int qc_default_batch(uint64_t n, int nplanes);
 // FP64 FFT backend of the QC encode (qc_fft.cu): n = 2^e, 10 <= e <= kQcfMaxE.
-constexpr int kQcfMaxE = 21;
+constexpr int kQcfMaxE = 22;
+// n = 2^22 packs centred planes against `a` or its complement (whichever is
+// lighter); A_hat then carries a 256-byte trailer (the weight of `a`).
+constexpr bool qcf_center(int e) { return e >= 22; }
+constexpr uint64_t qcf_ahat_bytes(int e) { return (16ull << e) + (qcf_center(e) ? 256 : 0); }
 // A_hat of each transform y of a launch: p[(first + y) / per] (4 planes per transform).
 struct QcfAhatTab {
   const void *p[16];

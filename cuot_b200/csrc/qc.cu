@@ -748,7 +748,7 @@ static int leaf_batch(const cuot_ctx *ctx) {
 // Bytes of A_hat: NTT n Shoup pairs; FFT n complex doubles; Karatsuba the
 // 3^L leaf transforms, followed (with_planes) by the NTT's for plane encodes.
 static uint64_t ahat_bytes(QcKind k, int e, bool with_planes) {
-  if (k == kQcFft) return 16ull << e;
+  if (k == kQcFft) return qcf_ahat_bytes(e);
   if (k == kQcKara) return qck_ahat_bytes(e) + (with_planes ? 8ull << e : 0);
   return 8ull << e;
 }

@@ -1,32 +1,42 @@
 // qc_fft.cu -- exact quasi-cyclic encode through a double-precision complex
-// FFT (the default backend for n = 2^e, 10 <= e <= 21).
+// FFT (the default backend for n = 2^e, 10 <= e <= 22).
 //
 // out_r = a * e_r mod (x^n - 1) over GF(2) is the parity of the integer
-// cyclic convolution, whose coefficients lie in [0, n].  Four planes share
-// one complex transform, with base B = 2^21 for n <= 2^20 and B = 2^21 + 1
-// for n = 2^21 (B > n either way):
+// cyclic convolution, whose coefficients lie in [0, w(a)] (w: weight).  Four
+// planes share one complex transform, with base B = 2^21 for n <= 2^20 and
+// B = 2^21 + 1 for n >= 2^21:
 //   x_j = (e0_j + B e1_j) + i (e2_j + B e3_j),
 // and since `a` is real, IFFT(FFT(x) . FFT(a)) = (a*e0 + B a*e1) + i (a*e2
 // + B a*e3): every product coefficient is an integer V = c0 + B c1 below
-// 2^43 with c0, c1 in [0, n], so c1 = floor(V / B) and c0 = V - B c1.  For
-// B = 2^21 the two planes' bits are bits 0 and 21 of V; for B = 2^21 + 1,
+// 2^43 with c0, c1 in [0, W] (W < B), so c1 = floor(V / B) and c0 = V - B c1.
+// For B = 2^21 the two planes' bits are bits 0 and 21 of V; for B = 2^21 + 1,
 // with hi = V >> 21, lo = V mod 2^21 and d = hi - lo, c1 = hi - [d > 0] -
-// [d > B] and c0 has the parity of lo ^ c1 (B odd).  The computed values
-// differ from the integers by less than 1/2, so rounding recovers them
-// exactly: by the error bound for FFT-based convolution (Percival,
-// "Rapid multiplication modulo the sum and difference of highly composite
-// numbers", Math. Comp. 72 (2003), Thm. 5.1) the error is at most
+// [d > B] and c0 has the parity of lo ^ c1 (B odd).
+// At n = 2^22 two exact changes keep the rounding error small:
+//  * `a` is replaced by its complement when w(a) > n/2 (the weight is
+//    counted on the device when A_hat is built and kept in A_hat's trailer);
+//    a * e = w(e) - ~a * e coefficientwise, so each plane's result is XORed
+//    with the parity of the plane's weight (XOR-reduced by the forward pass).
+//    The coefficients then lie in [0, W] with W = min(w(a), n - w(a)) <= 2^21.
+//  * the planes are centred, x_j = (e0_j - 1/2) + B (e1_j - 1/2) + i (...),
+//    which moves every product coefficient by -(1 + B) W / 2 = -(2^20 + 1) W,
+//    an integer added back after rounding.
+// The computed values differ from the integers by less than 1/2, so rounding
+// recovers them exactly: by the error bound for FFT-based convolution
+// (Percival, "Rapid multiplication modulo the sum and difference of highly
+// composite numbers", Math. Comp. 72 (2003), Thm. 5.1) the error is at most
 // ||x||_2 ||a||_2 ((1+eps)^{3m} (1+eps sqrt5)^{3m+1} (1+beta)^{3m} - 1) with
-// m = log2 n, eps = 2^-53 and twiddle error beta <= 4 eps, and ||x||_2
-// ||a||_2 <= sqrt(2n) (1 + B) sqrt(n): below 2^41.5 * 436.4 * 2^-53 < 0.16
-// for n = 2^20 and 2^42.5 * 458.2 * 2^-53 < 0.32 for n = 2^21 (smaller n:
-// smaller bound).
+// m = log2 n, eps = 2^-53 and twiddle error beta <= 4 eps, where ||x||_2
+// ||a||_2 <= sqrt(2n) (1 + B) sqrt(n) (centred: sqrt(2n) (1 + B) / 2
+// sqrt(W)): below 2^41.5 * 436.4 * 2^-53 < 0.16 for n = 2^20, 2^42.5 *
+// 458.2 * 2^-53 < 0.32 for n = 2^21 and 2^42 * 479.9 * 2^-53 < 0.24 for
+// n = 2^22 (smaller n: smaller bound).
 //
 // Work per plane and radix-2 stage is one fp64 operation (a complex
 // butterfly shared by four planes), against several integer instructions
 // per plane in the number-theoretic transform of qc.cu.
 //
-// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= 512, N1 <= N2 <= 4096), input
+// Four-step transform, n = N1 * N2 (N1 = 2^e1 <= 1024, N1 <= N2 <= 4096), input
 // index j = N2*j1 + j2, frequency k = k1 + N1*k2:
 //   A (columns): 8 columns j2 of one transform per CTA: load the plane bits,
 //     N1-point DIF FFT over j1 (frequencies land in bit-reversed row order r),
@@ -70,6 +80,9 @@ __host__ __device__ constexpr int qcf_tw_off(int L, int p) {
   return p == 0 ? 0 : qcf_tw_off(L, p - 1) + ((1 << qcf_k(L, p - 1)) - 1) * ((1 << qcf_ls(L, p - 1)) >> qcf_k(L, p - 1));
 }
 __host__ __device__ constexpr int qcf_threads(int L) { return L >= 10 ? 512 : L == 9 ? 256 : L == 8 ? 128 : 64; }
+// Column CTAs per SM: three up to 512 points, one at 1024 (143 KB of shared
+// memory).
+__host__ __device__ constexpr int qcf_col_ctas(int L) { return L >= 10 ? 1 : 3; }
 // four-step factor tables per column: 2^lo + 2^(e1 - lo) entries (global
 // row stride), staged with an odd row stride so the 8 columns of a
 // quarter-warp hit distinct banks
@@ -86,12 +99,15 @@ __host__ __device__ constexpr bool qcf_row_tg0(int L) { return L >= 12; }
 __host__ __device__ constexpr int qcf_row_threads(int L) {
   return L >= 11 ? 256 : qcf_threads(L) / 2 < 32 ? 32 : qcf_threads(L) / 2;
 }
-// Packing base 2^21 + qcf_wide(e) (2^21 + 1 for n = 2^21, where a product
+// Packing base 2^21 + qcf_wide(e) (2^21 + 1 from n = 2^21, where a product
 // coefficient can equal 2^21).
 __host__ __device__ constexpr int qcf_wide(int e) { return e >= 21 ? 1 : 0; }
-// Split of n = 2^e into N1 = 2^e1 column points (at most 512, so three column
-// CTAs fit an SM) and N2 = 2^(e - e1) row points.
-__host__ __device__ constexpr int qcf_e1(int e) { return e / 2 < 9 ? e / 2 : 9; }
+// Split of n = 2^e into N1 = 2^e1 column points (at most 512 up to 2^21, so
+// three column CTAs fit an SM; 1024 at 2^22) and N2 = 2^(e - e1) row points
+// (at most 4096).
+__host__ __device__ constexpr int qcf_e1(int e) { return e >= 22 ? e - 12 : e / 2 < 9 ? e / 2 : 9; }
+// Centring offset (1 + B) / 2 of the n = 2^22 packing (B = 2^21 + 1).
+constexpr int64_t kCenter = (1 << 20) + 1;
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
@@ -264,16 +280,21 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 
 // Pass A.  grid (N2 / 8, transforms).  in: plane p at in + p * stride_bytes;
 // transform y holds planes 4y .. 4y+3 (< nplanes) with base 2^21 + wide;
-// one_plane: `a` (real part only).  With tiles != nullptr the input is in the tile layout
+// one_plane: `a` (real part only; centred mode: its complement if wa[0] >
+// n / 2).  With tiles != nullptr the input is in the tile layout
 // instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
-// columns of the CTA's tile in row j1 (qcf_gather).
+// columns of the CTA's tile in row j1 (qcf_gather).  centred mode (par !=
+// nullptr): planes centred, and par[y] ^= the XOR of the CTA's words (byte q:
+// column parities of plane 4y + q).
 template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_fwd(
+__global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_fwd(
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2, int wide,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
-    double2 *__restrict__ Y) {
+    double2 *__restrict__ Y, const unsigned long long *__restrict__ wa, uint32_t *__restrict__ par) {
   constexpr int N1 = 1 << E1, ld = N1 + 1, W = qcf_fs_ld(E1);
   const uint32_t base = (1u << 21) + uint32_t(wide);
+  const double center = par ? double(kCenter) : 0.0;
+  const uint32_t comp = wa && *wa > (1ull << (E1 + e2 - 1)) ? 1u : 0u;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
   double2 *xs = sm, *fss = xs + kCols * ld;
@@ -296,6 +317,12 @@ __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_fwd(
     }
   }
   __syncthreads();
+  if (par) {  // plane weight parities (XOR of the CTA's words)
+    uint32_t x = 0;
+    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) x ^= bits[j1];
+    x = __reduce_xor_sync(0xffffffffu, x);
+    if ((threadIdx.x & 31) == 0 && x) atomicXor(par + blockIdx.y, x);
+  }
   {  // pass 0 from the bits
     using Q = Pass<E1, 0>;
     for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
@@ -306,9 +333,10 @@ __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_fwd(
       for (int m = 0; m < Q::R; m++) {
         const uint32_t b = bits[i0 + Q::M * m] >> c;
         if (one_plane) {
-          x[m] = make_double2(double(b & 1u), 0.0);
+          x[m] = make_double2(double((b ^ comp) & 1u), 0.0);
         } else {
-          x[m] = make_double2(double((b & 1u) + ((b >> 8) & 1u) * base), double(((b >> 16) & 1u) + ((b >> 24) & 1u) * base));
+          x[m] = make_double2(double((b & 1u) + ((b >> 8) & 1u) * base) - center,
+                              double(((b >> 16) & 1u) + ((b >> 24) & 1u) * base) - center);
         }
       }
       dif_regs<Q::K>(x);
@@ -428,19 +456,21 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
   }
 }
 
-// The two planes' bits (c0 & 1, c1 & 1) of a rounded product coefficient
-// V = c0 + B c1, B = 2^21 + wide, c0 and c1 in [0, 2^21] (see the top of the
-// file); v + 1.5 * 2^52 holds round(v) in the low 51 bits of its mantissa.
-__device__ __forceinline__ void plane_bits(double v, int wide, uint32_t &p0, uint32_t &p1) {
+// The two planes' bits (c0 & 1, c1 & 1) of a product coefficient v ~ V -
+// shift, V = c0 + B c1, B = 2^21 + wide, c0 and c1 in [0, 2^21] (see the top
+// of the file).  For |v| < 2^51, v + 1.5 * 2^52 lies in [2^52, 2^53), where
+// doubles are the integers: its bit pattern minus that of 1.5 * 2^52 is
+// round(v).
+__device__ __forceinline__ void plane_bits(double v, int wide, int64_t shift, uint32_t &p0, uint32_t &p1) {
   const double r = v + kRoundMagic;
-  const uint32_t lw = uint32_t(__double2loint(r));
   if (!wide) {
+    const uint32_t lw = uint32_t(__double2loint(r));
     p0 = lw & 1u;
     p1 = (lw >> 21) & 1u;
     return;
   }
-  const uint32_t hw = uint32_t(__double2hiint(r)) & 0x7FFFFu;  // bits 32..50 of round(v)
-  const uint32_t lo = lw & 0x1FFFFFu, hi = (lw >> 21) | (hw << 11);
+  const uint64_t V = uint64_t(__double_as_longlong(r) - __double_as_longlong(kRoundMagic) + shift);
+  const uint32_t lo = uint32_t(V) & 0x1FFFFFu, hi = uint32_t(V >> 21);
   const int d = int(hi) - int(lo);
   const uint32_t c1 = hi - uint32_t(d > 0) - uint32_t(d > (1 << 21) + 1);
   p0 = (lo ^ c1) & 1u;
@@ -450,10 +480,14 @@ __device__ __forceinline__ void plane_bits(double v, int wide, uint32_t &p0, uin
 // Pass C.  grid (N2 / 8, transforms).  out: plane p at out + p * stride_bytes,
 // written (accumulate == 0) or XORed into (accumulate == 1); with tiles !=
 // nullptr the result goes to the tile layout instead (one word per row).
+// centred mode (par != nullptr): the transform's A_hat trailer (ahat) gives
+// w(a); the centring shift is added back and, for a complemented `a`, each
+// plane's weight parity (par[y]) is XORed in.
 template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_inv(
+__global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_inv(
     const double2 *__restrict__ Y, int e2, int wide, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
-    uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles) {
+    uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles,
+    QcfAhatTab ahat, const uint32_t *__restrict__ par) {
   constexpr int N1 = 1 << E1, ld = N1 + 1;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
@@ -461,6 +495,20 @@ __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_inv(
   const double2 *Ts = T1;  // pass twiddles read through L1
   const int c0 = blockIdx.x * kCols;
   const int p0 = 4 * blockIdx.y;
+  int64_t shift = 0;
+  uint32_t flip = 0;  // bit q: XOR into plane 4y + q
+  if (par) {
+    const uint64_t n = 1ull << (E1 + e2);
+    const uint64_t w = *reinterpret_cast<const unsigned long long *>(
+        static_cast<const uint8_t *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) + 16 * n);
+    const bool comp = w > n / 2;
+    shift = kCenter * int64_t(comp ? n - w : w);
+    if (comp) {
+      const uint32_t pw = par[blockIdx.y];
+#pragma unroll
+      for (int q = 0; q < 4; q++) flip |= (uint32_t(__popc((pw >> (8 * q)) & 0xffu)) & 1u) << q;
+    }
+  }
   stage_fs<E1>(fss, fs, c0);
   __syncthreads();
   {  // inverse of the last pass, from global
@@ -496,8 +544,10 @@ __global__ void __launch_bounds__(qcf_threads(E1), 3) qcf_col_inv(
 #pragma unroll
       for (int m = 0; m < Q::R; m++) {
         uint32_t pl[4];
-        plane_bits(x[m].x, wide, pl[0], pl[1]);
-        plane_bits(x[m].y, wide, pl[2], pl[3]);
+        plane_bits(x[m].x, wide, shift, pl[0], pl[1]);
+        plane_bits(x[m].y, wide, shift, pl[2], pl[3]);
+#pragma unroll
+        for (int q = 0; q < 4; q++) pl[q] ^= (flip >> q) & 1u;
         const int j1 = i0 + Q::M * m;
         uint32_t word = 0;
 #pragma unroll
@@ -601,6 +651,17 @@ __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ 
   }
 }
 
+// Adds the weight of a (`words` 64-bit words) to *w.
+__global__ void __launch_bounds__(256) qcf_weight(const uint64_t *__restrict__ a, uint64_t words,
+                                                  unsigned long long *w) {
+  unsigned long long c = 0;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < words; i += uint64_t(gridDim.x) * blockDim.x)
+    c += __popcll(__ldg(&a[i]));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(w, c);
+}
+
 // Table generation (one-time per n).  T: the pass-ordered twiddles of an
 // N = 2^L point transform (entries past the last pass's offset unused).
 __global__ void qcf_gen_roots(int L, double2 *T) {
@@ -631,9 +692,13 @@ __global__ void qcf_gen_fourstep(int e1, int e2, double2 *fs) {
   }
 }
 
+// Plane parity words per encode call in centred mode (one per transform).
+constexpr int kQcfParCap = 4096;
+
 struct QcfTables {
   int e, e1, e2;
   double2 *T1, *T2, *fs;
+  uint32_t *par;          // centred mode: kQcfParCap plane-parity words
   const cuot_ctx *owner;  // context that caches the tables (its qc_streams)
   cudaStream_t aux;    // second stream of the two-stream group schedule
   cudaEvent_t ev[2];   // fork / join
@@ -655,6 +720,7 @@ void qcf_free(QcfTables *t) {
   cudaFree(t->T1);
   cudaFree(t->T2);
   cudaFree(t->fs);
+  cudaFree(t->par);
   if (t->aux) cudaStreamDestroy(t->aux);
   for (cudaEvent_t e : t->ev)
     if (e) cudaEventDestroy(e);
@@ -673,7 +739,7 @@ int row_smem(int e2) {
   return (rows * ld + tw) * 16;
 }
 
-#define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9)
+#define QCF_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10)
 #define QCF_ROW_CASES(X) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12)
 
 int set_attrs() {
@@ -701,14 +767,18 @@ int set_attrs() {
   return CUOT_OK;
 }
 
+// par: plane-parity words of the launch's transforms (centred encodes), wa:
+// the weight of `a` (centred A_hat builds), else null.
 void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t *in, uint64_t stride_bytes,
-                    int nplanes, int one_plane, const uint32_t *tiles, double2 *Y) {
+                    int nplanes, int one_plane, const uint32_t *tiles, double2 *Y,
+                    const unsigned long long *wa = nullptr, uint32_t *par = nullptr) {
   const dim3 grid((1u << t->e2) / kCols, ntr);
   switch (t->e1) {
 #define QCF_L(E)                                                                                            \
   case E:                                                                                                   \
     qcf_col_fwd<E><<<grid, qcf_threads(E), col_smem(E), st>>>(in, stride_bytes, nplanes, one_plane, t->e2, \
-                                                               qcf_wide(t->e), tiles, t->T1, t->fs, Y);     \
+                                                               qcf_wide(t->e), tiles, t->T1, t->fs, Y, wa,  \
+                                                               par);                                        \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
@@ -727,13 +797,15 @@ void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const 
   }
 }
 void launch_col_inv(const QcfTables *t, int ntr, cudaStream_t st, const double2 *Y, uint8_t *out,
-                    uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *tiles) {
+                    uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *tiles, const QcfAhatTab &ahat,
+                    const uint32_t *par) {
   const dim3 grid((1u << t->e2) / kCols, ntr);
   switch (t->e1) {
 #define QCF_L(E)                                                                                          \
   case E:                                                                                                 \
     qcf_col_inv<E><<<grid, qcf_threads(E), col_smem(E), st>>>(Y, t->e2, qcf_wide(t->e), t->T1, t->fs, out, \
-                                                               stride_bytes, nplanes, accumulate, tiles); \
+                                                               stride_bytes, nplanes, accumulate, tiles,  \
+                                                               ahat, par);                                \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
@@ -759,7 +831,8 @@ int qcf_get_tables(cuot_ctx *ctx, int e, QcfTables **out) {
   const uint64_t N1 = 1ull << t->e1, N2 = 1ull << t->e2;
   int st = CUOT_OK;
   if ((st = qcf_alloc((void **)&t->T1, N1 * 16)) || (st = qcf_alloc((void **)&t->T2, N2 * 16)) ||
-      (st = qcf_alloc((void **)&t->fs, N2 * qcf_fs_width(t->e1) * 16))) {
+      (st = qcf_alloc((void **)&t->fs, N2 * qcf_fs_width(t->e1) * 16)) ||
+      (qcf_center(e) && (st = qcf_alloc((void **)&t->par, kQcfParCap * 4)))) {
     qcf_free(t);
     return st;
   }
@@ -791,9 +864,25 @@ void qcf_free_ctx_tables(cuot_ctx *ctx) {
 
 int qcf_build_ahat(const QcfTables *t, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st) {
   const uint64_t n = 1ull << t->e;
-  launch_col_fwd(t, 1, st, reinterpret_cast<const uint8_t *>(a_d), n / 8, 1, 1, nullptr, static_cast<double2 *>(Y));
+  unsigned long long *wa = nullptr;
+  int launches = 2;
+  if (qcf_center(t->e)) {  // w(a) into the trailer; the transform is of the lighter of a, ~a
+    wa = reinterpret_cast<unsigned long long *>(static_cast<uint8_t *>(ahat) + 16 * n);
+    if (cudaMemsetAsync(wa, 0, 8, st) != cudaSuccess) return launch_status(0);
+    qcf_weight<<<148, 256, 0, st>>>(a_d, n / 64, wa);
+    launches++;
+  }
+  launch_col_fwd(t, 1, st, reinterpret_cast<const uint8_t *>(a_d), n / 8, 1, 1, nullptr, static_cast<double2 *>(Y),
+                 wa);
   launch_row(t, 1, st, static_cast<double2 *>(Y), QcfAhatTab{}, 1, static_cast<double2 *>(ahat), 1.0 / double(n));
-  return launch_status(2);
+  return launch_status(launches);
+}
+
+// Zeroes the plane-parity words of `ntr` transforms (centred mode).
+static int clear_par(const QcfTables *t, int ntr, cudaStream_t st) {
+  if (!t->par) return CUOT_OK;
+  if (ntr > kQcfParCap) return fail(CUOT_EINVAL, "QC FFT: %d transforms in one call (at most %d)", ntr, kQcfParCap);
+  return cudaMemsetAsync(t->par, 0, size_t(ntr) * 4, st) == cudaSuccess ? CUOT_OK : launch_status(0);
 }
 
 int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, uint64_t *out, uint64_t stride,
@@ -805,11 +894,12 @@ int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, u
     const int ntr = (nb + 3) / 4;
     QcfAhatTab tab = ahat;
     tab.first += p0 / 4;
+    CUOT_TRY(clear_par(t, ntr, st));
     launch_col_fwd(t, ntr, st, reinterpret_cast<const uint8_t *>(in + uint64_t(p0) * stride), stride * 8, nb, 0,
-                   nullptr, static_cast<double2 *>(Y));
+                   nullptr, static_cast<double2 *>(Y), nullptr, t->par);
     launch_row(t, ntr, st, static_cast<double2 *>(Y), tab, 0, nullptr, 0.0);
     launch_col_inv(t, ntr, st, static_cast<const double2 *>(Y), reinterpret_cast<uint8_t *>(out + uint64_t(p0) * stride),
-                   stride * 8, nb, accumulate, nullptr);
+                   stride * 8, nb, accumulate, nullptr, tab, t->par);
     launches += 3;
   }
   return launch_status(launches);
@@ -832,6 +922,8 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
   // (callers that already run several encodes at once, such as the server).
   uint64_t g64 = (32ull << 20) / ybytes;
   const int G = g64 < 1 ? 1 : int(g64);
+  CUOT_TRY(clear_par(t, ntransforms, st));
+  uint32_t *par = t->par;
   if (t->owner->qc_streams == 2 && 2 * G <= bt && ntransforms > G) {
     cudaEventRecord(t->ev[0], st);
     cudaStreamWaitEvent(t->aux, t->ev[0], 0);
@@ -843,9 +935,10 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
       QcfAhatTab tab = ahat;
       tab.first += t0;
       uint32_t *tp = tiles + uint64_t(t0) * words;
-      launch_col_fwd(t, ntr, s, nullptr, 0, 4 * ntr, 0, tp, Yg);
+      uint32_t *pp = par ? par + t0 : nullptr;
+      launch_col_fwd(t, ntr, s, nullptr, 0, 4 * ntr, 0, tp, Yg, nullptr, pp);
       launch_row(t, ntr, s, Yg, tab, 0, nullptr, 0.0);
-      launch_col_inv(t, ntr, s, Yg, nullptr, 0, 4 * ntr, 0, tp);
+      launch_col_inv(t, ntr, s, Yg, nullptr, 0, 4 * ntr, 0, tp, tab, pp);
       launches += 3;
     }
     cudaEventRecord(t->ev[1], t->aux);
@@ -857,9 +950,10 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
     QcfAhatTab tab = ahat;
     tab.first += t0;
     uint32_t *tp = tiles + uint64_t(t0) * words;
-    launch_col_fwd(t, ntr, st, nullptr, 0, 4 * ntr, 0, tp, static_cast<double2 *>(Y));
+    uint32_t *pp = par ? par + t0 : nullptr;
+    launch_col_fwd(t, ntr, st, nullptr, 0, 4 * ntr, 0, tp, static_cast<double2 *>(Y), nullptr, pp);
     launch_row(t, ntr, st, static_cast<double2 *>(Y), tab, 0, nullptr, 0.0);
-    launch_col_inv(t, ntr, st, static_cast<const double2 *>(Y), nullptr, 0, 4 * ntr, 0, tp);
+    launch_col_inv(t, ntr, st, static_cast<const double2 *>(Y), nullptr, 0, 4 * ntr, 0, tp, tab, pp);
     launches += 3;
   }
   return launch_status(launches);

@@ -82,7 +82,7 @@ uint64_t pow3(int l) {
 }
 
 constexpr uint64_t kLeafN = 1ull << kQcfMaxE;
-constexpr uint64_t kLeafAhat = 16 * kLeafN;  // bytes of one leaf's transform
+constexpr uint64_t kLeafAhat = qcf_ahat_bytes(kQcfMaxE);  // bytes of one leaf's transform
 
 int ahat_tree(const QcfTables *leaf, int e, const uint64_t *a, uint8_t *bits, void *Y, uint8_t *ahat, cudaStream_t st) {
   if (e == kQcfMaxE) return qcf_build_ahat(leaf, a, Y, ahat, st);

@@ -5,9 +5,9 @@ import bench
 
 
 def test_qc_leaves_follow_the_backend_split():
-    assert [bench.qc_leaves(e) for e in (10, 16, 20, 21)] == [1, 1, 1, 1]
-    assert bench.qc_leaves(22) == 3 and bench.qc_leaves(23) == 9
-    assert bench.qc_leaves(24) == 0 and bench.qc_leaves(25) == 0
+    assert [bench.qc_leaves(e) for e in (10, 16, 20, 21, 22)] == [1, 1, 1, 1, 1]
+    assert bench.qc_leaves(23) == 3 and bench.qc_leaves(24) == 9
+    assert bench.qc_leaves(25) == 0
 
 
 def test_qc_work_counts():
@@ -15,18 +15,18 @@ def test_qc_work_counts():
     w = bench.qc_transform_work([n])
     # both roles, 32 four-plane transforms forward and inverse, 5 n log n each, + 6n products
     assert w == {"fft_fp64_flops": 2 * 32 * (2 * 5 * n * 20 + 6 * n), "ntt_butterflies": 0}
-    m = 1 << 21
-    w21 = bench.qc_transform_work([m])
-    assert w21["fft_fp64_flops"] == 2 * 32 * (2 * 5 * m * 21 + 6 * m)
-    assert bench.qc_transform_work([1 << 22])["fft_fp64_flops"] == 3 * w21["fft_fp64_flops"]
-    w24 = bench.qc_transform_work([1 << 24])
-    assert w24 == {"fft_fp64_flops": 0, "ntt_butterflies": 2 * 128 * 2 * (1 << 23) * 24}
+    m = 1 << 22
+    w22 = bench.qc_transform_work([m])
+    assert w22["fft_fp64_flops"] == 2 * 32 * (2 * 5 * m * 22 + 6 * m)
+    assert bench.qc_transform_work([1 << 23])["fft_fp64_flops"] == 3 * w22["fft_fp64_flops"]
+    w25 = bench.qc_transform_work([1 << 25])
+    assert w25 == {"fft_fp64_flops": 0, "ntt_butterflies": 2 * 128 * 2 * (1 << 24) * 25}
 
 
 def test_qc_report_rate_only_for_pure_fft():
     r = bench.qc_transform_report([1 << 20], 1.0)
     assert abs(r["fp64_tflops"] - r["fft_fp64_flops"] / 1e-3 / 1e12) < 1e-9
-    assert "fp64_tflops" not in bench.qc_transform_report([1 << 20, 1 << 24], 1.0)
+    assert "fp64_tflops" not in bench.qc_transform_report([1 << 20, 1 << 25], 1.0)
 
 
 def test_lpn_l1_roofline_model():

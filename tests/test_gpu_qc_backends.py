@@ -1,11 +1,13 @@
 """The transforms of the exact QC encode -- the fp64 FFT (four planes per
-complex transform, default for n <= 2^21; packing base 2^21 + 1 at 2^21),
-GF(2) Karatsuba over it (dual LPN at n = 2^22, 2^23) and the NTT mod
+complex transform, default for n <= 2^22; packing base 2^21 + 1 from 2^21;
+at 2^22 centred planes against the lighter of `a` and its complement),
+GF(2) Karatsuba over it (dual LPN at n = 2^23, 2^24) and the NTT mod
 469762049 -- against the oracle and against each other: every supported FFT
 size, plane counts that leave a partial transform, the maximum-magnitude
 inputs (all-ones `a` and planes: every convolution coefficient equals its
-bound n), the rate-1/2 form with odd batches, the full 128-plane dual LPN at
-n = 2^20 and 2^21, the Karatsuba sizes, and the one- and two-stream FFT group
+bound n), both sides of the complement at 2^22 (a and ~a, light and heavy
+`a`), the rate-1/2 form with odd batches, the full 128-plane dual LPN at
+n = 2^20 .. 2^22, the Karatsuba sizes, and the one- and two-stream FFT group
 schedules."""
 import numpy as np
 import pytest
@@ -36,7 +38,7 @@ def gen_a(ctx, key, n):
 
 
 @pytest.mark.parametrize("e,nplanes", [(10, 1), (11, 3), (12, 4), (13, 5), (14, 6), (15, 9), (16, 2),
-                                       (17, 3), (18, 4), (19, 5), (20, 7), (21, 6)])
+                                       (17, 3), (18, 4), (19, 5), (20, 7), (21, 6), (22, 5)])
 def test_encode_every_size(bctx, e, nplanes):
     n = 1 << e
     rng = np.random.default_rng(500 + e)
@@ -49,7 +51,7 @@ def test_encode_every_size(bctx, e, nplanes):
     assert np.array_equal(to_host(d).view(np.uint64), exp)
 
 
-@pytest.mark.parametrize("e", [10, 16, 20, 21])
+@pytest.mark.parametrize("e", [10, 16, 20, 21, 22])
 def test_maximum_magnitude_inputs(bctx, e):
     """a = all ones: coefficient k of a*e is the weight of e (the same for
     every k); with e all ones every coefficient equals n, the bound the
@@ -123,11 +125,11 @@ def _ctx(backend):
     return c
 
 
-@pytest.mark.parametrize("e", [21, 22, 23])
+@pytest.mark.parametrize("e", [21, 22, 23, 24])
 def test_large_sizes_match_ntt_and_oracle(e):
-    """n = 2^21 / 2^22 / 2^23 dual LPN: the default backend (the direct FFT;
-    GF(2) Karatsuba over 2^21 FFTs, one / two levels) gives the NTT's
-    blocks, one-shot and through a plan, and sampled planes match the
+    """n = 2^21 .. 2^24 dual LPN: the default backend (the direct FFT up to
+    2^22; GF(2) Karatsuba over 2^22 FFTs, one / two levels, above) gives the
+    NTT's blocks, one-shot and through a plan, and sampled planes match the
     oracle's product."""
     n = 1 << e
     rng = np.random.default_rng(900 + e)
@@ -145,8 +147,8 @@ def test_large_sizes_match_ntt_and_oracle(e):
             d2 = to_dev(x)
             plan.dual_lpn(d2)
             outs["plan"] = to_host(d2)
-            # plane encodes through the same plan (FFT at 2^21; above, the NTT
-            # A_hat kept beside the Karatsuba leaves)
+            # plane encodes through the same plan (FFT up to 2^22; above, the
+            # NTT A_hat kept beside the Karatsuba leaves)
             pl = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)[:2].copy()
             dp = to_dev(pl.view(np.int64))
             plan.encode(dp, 2)
@@ -165,10 +167,10 @@ def test_large_sizes_match_ntt_and_oracle(e):
         assert np.array_equal(outs["plan_planes"][r], outp[r])
 
 
-@pytest.mark.parametrize("e", [21, 22])
+@pytest.mark.parametrize("e", [21, 22, 23])
 def test_rate_half_large(e):
-    """Rate-1/2 form at n = 2^21 (direct FFT) and 2^22 (Karatsuba): out =
-    e0 ^ a*e1, also with out aliasing the first n input blocks."""
+    """Rate-1/2 form at n = 2^21, 2^22 (direct FFT) and 2^23 (Karatsuba):
+    out = e0 ^ a*e1, also with out aliasing the first n input blocks."""
     n = 1 << e
     rng = np.random.default_rng(2100 + e)
     x = rng_blocks(rng, 2 * n)
@@ -192,7 +194,7 @@ def test_rate_half_large(e):
         assert np.array_equal(po[r], p0[r] ^ oracle.gf2_cyclic_mul(a_np, p1[r], n))
 
 
-@pytest.mark.parametrize("e", [17, 20, 21])
+@pytest.mark.parametrize("e", [17, 20, 21, 22])
 def test_one_and_two_stream_encodes_agree(e):
     """CUOT_TUNE_QC_STREAMS = 1 (every group on the caller's stream) and 2
     (groups alternate with the context's second stream) give the oracle's
@@ -222,4 +224,41 @@ def test_one_and_two_stream_encodes_agree(e):
     planes = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
     outp = oracle.bit_transpose(outs[0], n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
     for r in (0, 90):
+        assert np.array_equal(outp[r], oracle.gf2_cyclic_mul(a_np, planes[r], n))
+
+
+@pytest.mark.parametrize("kind", ["a", "not_a", "light", "heavy"])
+def test_complement_sides_at_2_22(kind):
+    """n = 2^22: the FFT packs centred planes against the lighter of `a` and
+    ~a.  `a` from the PRG and its complement land on opposite sides of n/2;
+    a light (weight ~ n/8) and a heavy (~ 7n/8) `a` exercise each side far
+    from the edge.  The full 128-plane dual LPN equals the NTT's, and
+    sampled planes equal the oracle's product."""
+    e = 22
+    n = 1 << e
+    rng = np.random.default_rng(2222)
+    x = rng_blocks(rng, n)
+    c0 = _ctx(0)
+    a = gen_a(c0, rng_blocks(rng, 1)[0], n)
+    a_np = to_host(a).view(np.uint64)
+    if kind == "not_a":
+        a_np = ~a_np
+    elif kind in ("light", "heavy"):
+        r = rng.integers(0, 2**63, (3, n // 64), dtype=np.uint64)
+        a_np = r[0] & r[1] & r[2]
+        if kind == "heavy":
+            a_np = ~a_np
+    c0.close()
+    outs = []
+    for b in (NTT, 0):
+        c = _ctx(b)
+        d = to_dev(x)
+        c.sot_dual_lpn(to_dev(a_np.view(np.int64)), d, n)
+        outs.append(to_host(d))
+        torch.cuda.synchronize()
+        c.close()
+    assert np.array_equal(outs[0], outs[1])
+    planes = oracle.bit_transpose(x, n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    outp = oracle.bit_transpose(outs[1], n, 16, 0, 128).view(np.uint64).reshape(128, n // 64)
+    for r in (5, 127):
         assert np.array_equal(outp[r], oracle.gf2_cyclic_mul(a_np, planes[r], n))
