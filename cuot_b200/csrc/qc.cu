@@ -1,7 +1,7 @@
 // qc.cu -- exact quasi-cyclic encode over GF(2)[x]/(x^n - 1) (SOT dual LPN):
 // the entry points, the choice of transform per size (the fp64 FFT of
-// qc_fft.cu up to 2^21, GF(2) Karatsuba over it in qc_kara.cu for dual LPNs
-// at 2^22 and 2^23, the number-theoretic transform below otherwise), the
+// qc_fft.cu up to 2^22, GF(2) Karatsuba over it in qc_kara.cu for dual LPNs
+// at 2^23 and 2^24, the number-theoretic transform below otherwise), the
 // sparse encode and the AES-CTR helpers.
 //
 // The reference multiplies with float32 cuFFT and recovers bits by truncating
@@ -716,8 +716,8 @@ static int default_batch(uint64_t n, int nplanes) {
 }
 
 // ---- backend selection -------------------------------------------------------
-// Transform of the dual LPN of n = 2^e: the fp64 FFT (qc_fft.cu) up to 2^21,
-// GF(2) Karatsuba over it (qc_kara.cu) for 2^22 and 2^23, the NTT above and
+// Transform of the dual LPN of n = 2^e: the fp64 FFT (qc_fft.cu) up to 2^22,
+// GF(2) Karatsuba over it (qc_kara.cu) for 2^23 and 2^24, the NTT above and
 // whenever the context asks for it.  Plane encodes (cuot_qc_encode and
 // cuot_qc_plan_encode) take the FFT or the NTT.
 enum QcKind { kQcNtt = 0, kQcFft = 1, kQcKara = 2 };
@@ -740,7 +740,7 @@ static uint64_t y_bytes(bool fft, int e, int batch) {
   return (b < 4 ? 4 : b) << (e + 2);
 }
 
-// Planes per pass of the Karatsuba leaves (2^21-point FFTs).
+// Planes per pass of the Karatsuba leaves (2^22-point FFTs).
 static int leaf_batch(const cuot_ctx *ctx) {
   return ctx->qc_planes_per_pass > 0 ? ctx->qc_planes_per_pass : default_batch(1ull << kQcfMaxE, 128);
 }
@@ -778,7 +778,7 @@ static uint64_t dual_y_offset(QcKind k, int e, bool r2) {
 struct QcEngine {
   QcKind kind;
   QcTables *t;   // NTT tables (NTT, and Karatsuba plans' plane encodes)
-  QcfTables *f;  // FFT tables (FFT: of n; Karatsuba: of the 2^21 leaves)
+  QcfTables *f;  // FFT tables (FFT: of n; Karatsuba: of the 2^22 leaves)
 };
 
 static int engine(cuot_ctx *ctx, int e, QcKind kind, QcEngine *g) {

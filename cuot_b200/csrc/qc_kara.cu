@@ -1,5 +1,5 @@
-// qc_kara.cu -- exact QC dual LPN for n = 2^22 and 2^23 as GF(2) Karatsuba
-// over the fp64 FFT of qc_fft.cu (which is exact up to 2^21).
+// qc_kara.cu -- exact QC dual LPN for n = 2^23 and 2^24 as GF(2) Karatsuba
+// over the fp64 FFT of qc_fft.cu (which is exact up to 2^22).
 //
 // Block j of the dual LPN holds coefficient j of all 128 bit planes, so with
 // y = x^2, a(x) = a0(y) + x a1(y) (a0 / a1: even / odd bits of a) and
@@ -9,7 +9,7 @@
 // a1 e1.  Three products of half size per level:
 //   P1 = a0 e0, P2 = a1 e1, P3 = (a0 ^ a1)(e0 ^ e1),
 //   out[2k] = P1[k] ^ P2[k-1 mod n/2],  out[2k+1] = P3[k] ^ P1[k] ^ P2[k].
-// One level turns 2^22 into three 2^21 FFT dual LPNs, two levels turn 2^23
+// One level turns 2^23 into three 2^22 FFT dual LPNs, two levels turn 2^24
 // into nine; each leaf is the exact FFT path, so the result is exact.  The
 // transforms of the 3^L leaf polynomials are computed once (the plan's
 // A_hat, leaves in the order P1, P2, P3 per level, depth first).

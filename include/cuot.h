@@ -55,8 +55,8 @@ uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
  *   CUOT_TUNE_QC_PLANES     planes per QC pass, 0 = automatic (512 MiB of
  *                           intermediate)
  *   CUOT_TUNE_QC_BACKEND    transform of the exact QC encode: 0 automatic
- *                           (fp64 FFT for n <= 2^21; dual LPNs at 2^22 and
- *                           2^23 as GF(2) Karatsuba over 2^21 FFTs; the NTT
+ *                           (fp64 FFT for n <= 2^22; dual LPNs at 2^23 and
+ *                           2^24 as GF(2) Karatsuba over 2^22 FFTs; the NTT
  *                           mod 469762049 above), 1 the NTT everywhere, 2 as
  *                           0.  Plans and batches keep the backend they were
  *                           created with; set it before creating them.
@@ -251,9 +251,9 @@ int cuot_ferret_chi_sum(cuot_ctx *ctx, const cuot_block *leaves_d, uint64_t t,
  * consecutive) becomes a * plane_r mod (x^n - 1) over GF(2), exactly
  * (replaces the float cuFFT path of QuasiCyclic::encode_dense,
  * quasi_cyclic.cu:118-128).  n a power of two in [2^10, 2^25].  The
- * product is an fp64 FFT carrying four planes per transform for n <= 2^21
+ * product is an fp64 FFT carrying four planes per transform for n <= 2^22
  * (exact: the rounding error of the convolution stays below 1/2), GF(2)
- * Karatsuba over that FFT for dual LPNs at 2^22 and 2^23, and a number-
+ * Karatsuba over that FFT for dual LPNs at 2^23 and 2^24, and a number-
  * theoretic transform mod 469762049 otherwise (CUOT_TUNE_QC_BACKEND).
  * encode_sparse: out = a * e mod (x^n - 1), e = indicator of pos_d[0..w)
  * (QuasiCyclic::encode_sparse, quasi_cyclic.cu:130-161).
