@@ -80,16 +80,21 @@ __host__ __device__ constexpr int qcf_tw_off(int L, int p) {
   return p == 0 ? 0 : qcf_tw_off(L, p - 1) + ((1 << qcf_k(L, p - 1)) - 1) * ((1 << qcf_ls(L, p - 1)) >> qcf_k(L, p - 1));
 }
 __host__ __device__ constexpr int qcf_threads(int L) { return L >= 10 ? 512 : L == 9 ? 256 : L == 8 ? 128 : 64; }
-// Column CTAs per SM: three up to 512 points, one at 1024 (143 KB of shared
-// memory).
-__host__ __device__ constexpr int qcf_col_ctas(int L) { return L >= 10 ? 1 : 3; }
+// Column CTAs per SM: three up to 512 points and for 4-column CTAs, one for
+// 8 columns of 1024 points (143 KB of shared memory).
+__host__ __device__ constexpr int qcf_col_ctas(int L, int KC) { return L >= 10 ? (KC == 8 ? 1 : 2) : 3; }
 // four-step factor tables per column: 2^lo + 2^(e1 - lo) entries (global
 // row stride), staged with an odd row stride so the 8 columns of a
 // quarter-warp hit distinct banks
 __host__ __device__ constexpr int qcf_fs_lo(int e1) { return (e1 + 1) / 2; }
 __host__ __device__ constexpr int qcf_fs_width(int e1) { return (1 << qcf_fs_lo(e1)) + (1 << (e1 - qcf_fs_lo(e1))); }
 __host__ __device__ constexpr int qcf_fs_ld(int e1) { return qcf_fs_width(e1) + 1; }
-constexpr int kCols = 8;  // columns per CTA of the column passes
+// Columns per CTA of the column passes: 8 (one tile byte per plane and row),
+// or 4 for the 1024-point columns of the tile layout, whose 8-column CTAs
+// (143 KB) would run one per SM; two CTAs then share each tile byte and
+// write one 16-bit half of its word each (see qcf_col_inv).
+constexpr int kCols = 8;
+__host__ __device__ constexpr int qcf_col_threads(int L, int KC) { return KC == 8 ? qcf_threads(L) : qcf_threads(L) / 2; }
 // Rows per CTA of the row pass, so that two CTAs fit an SM: 4 up to 1024
 // points, 2 for 2048, 1 for 4096 (its first pass's twiddles are read
 // through L1, only the middle pass's are staged).
@@ -106,6 +111,8 @@ __host__ __device__ constexpr int qcf_wide(int e) { return e >= 21 ? 1 : 0; }
 // three column CTAs fit an SM; 1024 at 2^22) and N2 = 2^(e - e1) row points
 // (at most 4096).
 __host__ __device__ constexpr int qcf_e1(int e) { return e >= 22 ? e - 12 : e / 2 < 9 ? e / 2 : 9; }
+// Columns per CTA of the tile-layout column passes of n = 2^e.
+__host__ __device__ constexpr int qcf_tile_kc(int e) { return qcf_e1(e) >= 10 ? 4 : 8; }
 // Centring offset (1 + B) / 2 of the n = 2^22 packing (B = 2^21 + 1).
 constexpr int64_t kCenter = (1 << 20) + 1;
 
@@ -270,41 +277,41 @@ __device__ __forceinline__ double2 fourstep_w(const double2 *fs, int c, int r) {
 __device__ __forceinline__ void stage(double2 *dst, const double2 *src, int cnt) {
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = __ldg(&src[i]);
 }
-// The 8 columns' four-step factor rows (global stride W) into rows of W + 1.
-template <int E1>
+// The KC columns' four-step factor rows (global stride W) into rows of W + 1.
+template <int E1, int KC>
 __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0) {
   constexpr int W = qcf_fs_width(E1);
   const double2 *src = fs + uint64_t(c0) * W;
-  for (int i = threadIdx.x; i < kCols * W; i += blockDim.x) dst[(i / W) * (W + 1) + i % W] = __ldg(&src[i]);
+  for (int i = threadIdx.x; i < KC * W; i += blockDim.x) dst[(i / W) * (W + 1) + i % W] = __ldg(&src[i]);
 }
 
-// Pass A.  grid (N2 / 8, transforms).  in: plane p at in + p * stride_bytes;
+// Pass A.  grid (N2 / KC, transforms).  in: plane p at in + p * stride_bytes;
 // transform y holds planes 4y .. 4y+3 (< nplanes) with base 2^21 + wide;
 // one_plane: `a` (real part only; centred mode: its complement if wa[0] >
 // n / 2).  With tiles != nullptr the input is in the tile layout
 // instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
 // columns of the CTA's tile in row j1 (qcf_gather).  centred mode (par !=
 // nullptr): planes centred, and par[y] ^= the XOR of the CTA's words (byte q:
-// column parities of plane 4y + q).
-template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_fwd(
+// column parities of plane 4y + q; only the CTA's KC columns).
+template <int E1, int KC>
+__global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC)) qcf_col_fwd(
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2, int wide,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     double2 *__restrict__ Y, const unsigned long long *__restrict__ wa, uint32_t *__restrict__ par) {
-  constexpr int N1 = 1 << E1, ld = N1 + 1, W = qcf_fs_ld(E1);
+  constexpr int N1 = 1 << E1, ld = sld<KC>(N1), W = qcf_fs_ld(E1);
   const uint32_t base = (1u << 21) + uint32_t(wide);
   const double center = par ? double(kCenter) : 0.0;
   const uint32_t comp = wa && *wa > (1ull << (E1 + e2 - 1)) ? 1u : 0u;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
-  double2 *xs = sm, *fss = xs + kCols * ld;
-  uint32_t *bits = reinterpret_cast<uint32_t *>(fss + kCols * W);
+  double2 *xs = sm, *fss = xs + KC * ld;
+  uint32_t *bits = reinterpret_cast<uint32_t *>(fss + KC * W);
   const double2 *Ts = T1;  // pass twiddles read through L1
-  const int c0 = blockIdx.x * kCols;
+  const int c0 = blockIdx.x * KC, sub = c0 & 7;  // sub: the CTA's first bit in each tile byte
   const int p0 = 4 * blockIdx.y;
-  stage_fs<E1>(fss, fs, c0);
+  stage_fs<E1, KC>(fss, fs, c0);
   if (tiles) {
-    const uint32_t *tp = tiles + (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + blockIdx.x;
+    const uint32_t *tp = tiles + (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (c0 >> 3);
     for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) bits[j1] = __ldg(tp + (uint64_t(j1) << (e2 - 3)));
   } else {
     for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
@@ -318,20 +325,21 @@ __global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_fwd
   }
   __syncthreads();
   if (par) {  // plane weight parities (XOR of the CTA's words)
+    constexpr uint32_t mask = KC == 8 ? 0xffffffffu : 0x0f0f0f0fu;
     uint32_t x = 0;
-    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) x ^= bits[j1];
+    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) x ^= bits[j1] & (mask << sub);
     x = __reduce_xor_sync(0xffffffffu, x);
     if ((threadIdx.x & 31) == 0 && x) atomicXor(par + blockIdx.y, x);
   }
   {  // pass 0 from the bits
     using Q = Pass<E1, 0>;
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < KC * Q::items; it += blockDim.x) {
+      const int c = it & (KC - 1), w = it / KC;
       const int i0 = Q::first(w);
       double2 x[Q::R];
 #pragma unroll
       for (int m = 0; m < Q::R; m++) {
-        const uint32_t b = bits[i0 + Q::M * m] >> c;
+        const uint32_t b = bits[i0 + Q::M * m] >> (sub + c);
         if (one_plane) {
           x[m] = make_double2(double((b ^ comp) & 1u), 0.0);
         } else {
@@ -341,22 +349,22 @@ __global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_fwd
       }
       dif_regs<Q::K>(x);
       pass_twiddle<E1, 0, false, true>(x, Q::base(w), Ts);
-      double2 *row = xs + c * ld + i0;
+      double2 *row = xs + c * ld;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) row[Q::M * m] = x[m];
+      for (int m = 0; m < Q::R; m++) row[spos<E1, KC>(i0 + Q::M * m)] = x[m];
     }
   }
-  middle_passes<E1, false, kCols, true>(xs, Ts);
+  middle_passes<E1, false, KC, true>(xs, Ts);
   {  // last pass (M = 1), then the four-step twiddle, to global
     using Q = Pass<E1, NP - 1>;
     static_assert(Q::M == 1, "last pass");
     double2 *Yp = Y + (uint64_t(blockIdx.y) << (E1 + e2));
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < KC * Q::items; it += blockDim.x) {
+      const int c = it & (KC - 1), w = it / KC;
       const int i0 = Q::first(w);
       double2 x[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + i0 + m];
+      for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + spos<E1, KC>(i0 + m)];
       dif_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) {
@@ -477,23 +485,26 @@ __device__ __forceinline__ void plane_bits(double v, int wide, int64_t shift, ui
   p1 = c1 & 1u;
 }
 
-// Pass C.  grid (N2 / 8, transforms).  out: plane p at out + p * stride_bytes,
+// Pass C.  grid (N2 / KC, transforms).  out: plane p at out + p * stride_bytes,
 // written (accumulate == 0) or XORed into (accumulate == 1); with tiles !=
-// nullptr the result goes to the tile layout instead (one word per row).
+// nullptr the result goes to the tile layout instead (one word per row; for
+// KC = 4, the CTA writes 16-bit half sub / 4 of the word, nibble q = plane
+// 4y + q's bits of its 4 columns, which qcf_scatter puts back in byte
+// order).  KC = 4 writes tiles only.
 // centred mode (par != nullptr): the transform's A_hat trailer (ahat) gives
 // w(a); the centring shift is added back and, for a complemented `a`, each
 // plane's weight parity (par[y]) is XORed in.
-template <int E1>
-__global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_inv(
+template <int E1, int KC>
+__global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC)) qcf_col_inv(
     const double2 *__restrict__ Y, int e2, int wide, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles,
     QcfAhatTab ahat, const uint32_t *__restrict__ par) {
-  constexpr int N1 = 1 << E1, ld = N1 + 1;
+  constexpr int N1 = 1 << E1, ld = sld<KC>(N1);
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
-  double2 *xs = sm, *fss = xs + kCols * ld;
+  double2 *xs = sm, *fss = xs + KC * ld;
   const double2 *Ts = T1;  // pass twiddles read through L1
-  const int c0 = blockIdx.x * kCols;
+  const int c0 = blockIdx.x * KC;
   const int p0 = 4 * blockIdx.y;
   int64_t shift = 0;
   uint32_t flip = 0;  // bit q: XOR into plane 4y + q
@@ -509,13 +520,13 @@ __global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_inv
       for (int q = 0; q < 4; q++) flip |= (uint32_t(__popc((pw >> (8 * q)) & 0xffu)) & 1u) << q;
     }
   }
-  stage_fs<E1>(fss, fs, c0);
+  stage_fs<E1, KC>(fss, fs, c0);
   __syncthreads();
   {  // inverse of the last pass, from global
     using Q = Pass<E1, NP - 1>;
     const double2 *Yp = Y + (uint64_t(blockIdx.y) << (E1 + e2));
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < KC * Q::items; it += blockDim.x) {
+      const int c = it & (KC - 1), w = it / KC;
       const int i0 = Q::first(w);
       double2 x[Q::R];
 #pragma unroll
@@ -525,20 +536,21 @@ __global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_inv
       }
       dit_regs<Q::K>(x);
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) xs[c * ld + i0 + m] = x[m];
+      for (int m = 0; m < Q::R; m++) xs[c * ld + spos<E1, KC>(i0 + m)] = x[m];
     }
   }
-  middle_passes<E1, true, kCols, true>(xs, Ts);
-  {  // inverse of pass 0; round; the 8 columns' bits of each plane form a byte
+  middle_passes<E1, true, KC, true>(xs, Ts);
+  {  // inverse of pass 0; round; the KC columns' bits of each plane form a byte (nibble)
     using Q = Pass<E1, 0>;
+    static_assert((KC * Q::items) % 32 == 0, "whole warps at the ballots");
     const int lane = threadIdx.x & 31;
-    for (int it = threadIdx.x; it < kCols * Q::items; it += blockDim.x) {
-      const int c = it & (kCols - 1), w = it / kCols;
+    for (int it = threadIdx.x; it < KC * Q::items; it += blockDim.x) {
+      const int c = it & (KC - 1), w = it / KC;
       const int i0 = Q::first(w);
-      const double2 *row = xs + c * ld + i0;
+      const double2 *row = xs + c * ld;
       double2 x[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = row[Q::M * m];
+      for (int m = 0; m < Q::R; m++) x[m] = row[spos<E1, KC>(i0 + Q::M * m)];
       pass_twiddle<E1, 0, true, true>(x, Q::base(w), Ts);
       dit_regs<Q::K>(x);
 #pragma unroll
@@ -549,12 +561,18 @@ __global__ void __launch_bounds__(qcf_threads(E1), qcf_col_ctas(E1)) qcf_col_inv
 #pragma unroll
         for (int q = 0; q < 4; q++) pl[q] ^= (flip >> q) & 1u;
         const int j1 = i0 + Q::M * m;
+        constexpr uint32_t cm = (1u << KC) - 1;
         uint32_t word = 0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) word |= ((__ballot_sync(0xffffffffu, pl[q]) >> (lane & ~7)) & 0xffu) << (8 * q);
+        for (int q = 0; q < 4; q++) word |= ((__ballot_sync(0xffffffffu, pl[q]) >> (lane & ~(KC - 1))) & cm) << (KC * q);
         if (c != 0) continue;
+        const uint64_t wi = (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (uint64_t(j1) << (e2 - 3)) + (c0 >> 3);
+        if constexpr (KC == 4) {
+          reinterpret_cast<uint16_t *>(tiles)[2 * wi + ((c0 & 7) >> 2)] = uint16_t(word);
+          continue;
+        }
         if (tiles) {
-          tiles[(uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (uint64_t(j1) << (e2 - 3)) + blockIdx.x] = word;
+          tiles[wi] = word;
           continue;
         }
         const uint64_t byte = ((uint64_t(j1) << e2) | uint64_t(c0)) >> 3;
@@ -617,9 +635,18 @@ __global__ void __launch_bounds__(256) qcf_gather(const uint4 *__restrict__ in, 
   }
 }
 
+// Nibbles 0..3 of x at bits 0, 8, 16, 24.
+__device__ __forceinline__ uint32_t spread_nibbles(uint32_t x) {
+  x = (x | (x << 8)) & 0x00FF00FFu;
+  return (x | (x << 4)) & 0x0F0F0F0Fu;
+}
+
 // The inverse of qcf_gather; out[j] = (xor_in ? xor_in[j] : 0) ^ block j.
+// halves: the words hold two 16-bit halves from 4-column CTAs (low: columns
+// 0-3, high: 4-7; nibble q of each: plane q), put back in byte order first.
 __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ tiles, uint64_t ngroups,
-                                                   const uint4 *__restrict__ xor_in, uint4 *__restrict__ out) {
+                                                   const uint4 *__restrict__ xor_in, uint4 *__restrict__ out,
+                                                   int halves) {
   for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups;
        g += uint64_t(gridDim.x) * blockDim.x) {
     uint32_t w[8][4];
@@ -632,8 +659,12 @@ __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ 
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         const int t = 8 * wd + 2 * k;
-        uint64_t x = uint64_t(__ldg(&tiles[uint64_t(t) * ngroups + g])) |
-                     uint64_t(__ldg(&tiles[uint64_t(t + 1) * ngroups + g])) << 32;
+        uint32_t lo = __ldg(&tiles[uint64_t(t) * ngroups + g]), hi = __ldg(&tiles[uint64_t(t + 1) * ngroups + g]);
+        if (halves) {
+          lo = spread_nibbles(lo & 0xffffu) | (spread_nibbles(lo >> 16) << 4);
+          hi = spread_nibbles(hi & 0xffffu) | (spread_nibbles(hi >> 16) << 4);
+        }
+        uint64_t x = uint64_t(lo) | uint64_t(hi) << 32;
         x = transpose8(x);
 #pragma unroll
         for (int c = 0; c < 8; c++) w[c][wd] |= uint32_t((x >> (8 * c)) & 0xffu) << (8 * k);
@@ -727,9 +758,9 @@ void qcf_free(QcfTables *t) {
   delete t;
 }
 
-int col_smem(int e1) {
+int col_smem(int e1, int kc) {
   const int N1 = 1 << e1;
-  return (kCols * (N1 + 1) + kCols * qcf_fs_ld(e1)) * 16 + N1 * 4;
+  return (kc * (kc == 8 ? sld<8>(N1) : sld<4>(N1)) + kc * qcf_fs_ld(e1)) * 16 + N1 * 4;
 }
 int row_smem(int e2) {
   const int N2 = 1 << e2;
@@ -748,15 +779,18 @@ int set_attrs() {
   cudaGetDevice(&dev);
   if (dev < 64 && done[dev]) return CUOT_OK;
   bool ok = true;
-#define QCF_SET(E)                                                                                     \
-  ok &= cudaFuncSetAttribute(qcf_col_fwd<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E)) == \
-        cudaSuccess;                                                                                   \
-  ok &= cudaFuncSetAttribute(qcf_col_inv<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E)) == \
+#define QCF_SETK(E, K)                                                                                   \
+  ok &= cudaFuncSetAttribute(qcf_col_fwd<E, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E, K)) == \
+        cudaSuccess;                                                                                         \
+  ok &= cudaFuncSetAttribute(qcf_col_inv<E, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E, K)) == \
         cudaSuccess;
+#define QCF_SET(E) QCF_SETK(E, 8)
 #define QCF_SETR(E) \
   ok &= cudaFuncSetAttribute(qcf_row<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem(E)) == cudaSuccess;
   QCF_CASES(QCF_SET)
+  QCF_SETK(10, 4)
   QCF_ROW_CASES(QCF_SETR)
+#undef QCF_SETK
 #undef QCF_SET
 #undef QCF_SETR
   if (!ok) {
@@ -772,16 +806,23 @@ int set_attrs() {
 void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t *in, uint64_t stride_bytes,
                     int nplanes, int one_plane, const uint32_t *tiles, double2 *Y,
                     const unsigned long long *wa = nullptr, uint32_t *par = nullptr) {
-  const dim3 grid((1u << t->e2) / kCols, ntr);
+  const int kc = tiles ? qcf_tile_kc(t->e) : 8;
+  const dim3 grid((1u << t->e2) / kc, ntr);
+#define QCF_LK(E, K)                                                                                           \
+  qcf_col_fwd<E, K><<<grid, qcf_col_threads(E, K), col_smem(E, K), st>>>(                                     \
+      in, stride_bytes, nplanes, one_plane, t->e2, qcf_wide(t->e), tiles, t->T1, t->fs, Y, wa, par);
+  if (kc == 4) {
+    QCF_LK(10, 4)
+    return;
+  }
   switch (t->e1) {
-#define QCF_L(E)                                                                                            \
-  case E:                                                                                                   \
-    qcf_col_fwd<E><<<grid, qcf_threads(E), col_smem(E), st>>>(in, stride_bytes, nplanes, one_plane, t->e2, \
-                                                               qcf_wide(t->e), tiles, t->T1, t->fs, Y, wa,  \
-                                                               par);                                        \
+#define QCF_L(E) \
+  case E:        \
+    QCF_LK(E, 8) \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
+#undef QCF_LK
   }
 }
 void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const QcfAhatTab &ahat, int mode,
@@ -799,16 +840,23 @@ void launch_row(const QcfTables *t, int ntr, cudaStream_t st, double2 *Y, const 
 void launch_col_inv(const QcfTables *t, int ntr, cudaStream_t st, const double2 *Y, uint8_t *out,
                     uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *tiles, const QcfAhatTab &ahat,
                     const uint32_t *par) {
-  const dim3 grid((1u << t->e2) / kCols, ntr);
+  const int kc = tiles ? qcf_tile_kc(t->e) : 8;
+  const dim3 grid((1u << t->e2) / kc, ntr);
+#define QCF_LK(E, K)                                                                                         \
+  qcf_col_inv<E, K><<<grid, qcf_col_threads(E, K), col_smem(E, K), st>>>(                                   \
+      Y, t->e2, qcf_wide(t->e), t->T1, t->fs, out, stride_bytes, nplanes, accumulate, tiles, ahat, par);
+  if (kc == 4) {
+    QCF_LK(10, 4)
+    return;
+  }
   switch (t->e1) {
-#define QCF_L(E)                                                                                          \
-  case E:                                                                                                 \
-    qcf_col_inv<E><<<grid, qcf_threads(E), col_smem(E), st>>>(Y, t->e2, qcf_wide(t->e), t->T1, t->fs, out, \
-                                                               stride_bytes, nplanes, accumulate, tiles,  \
-                                                               ahat, par);                                \
+#define QCF_L(E) \
+  case E:        \
+    QCF_LK(E, 8) \
     break;
     QCF_CASES(QCF_L)
 #undef QCF_L
+#undef QCF_LK
   }
 }
 
@@ -968,7 +1016,7 @@ int qcf_gather(int e, const cuot_block *in, uint32_t *tiles, cudaStream_t st) {
 int qcf_scatter(int e, const uint32_t *tiles, const cuot_block *xor_in, cuot_block *out, cudaStream_t st) {
   const uint64_t ng = 1ull << (e - 3);
   qcf_scatter<<<unsigned((ng + 255) / 256), 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
-                                                           reinterpret_cast<uint4 *>(out));
+                                                           reinterpret_cast<uint4 *>(out), qcf_tile_kc(e) == 4);
   return launch_status();
 }
 
