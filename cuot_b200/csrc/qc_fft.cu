@@ -111,6 +111,10 @@ __host__ __device__ constexpr int qcf_wide(int e) { return e >= 21 ? 1 : 0; }
 // three column CTAs fit an SM; 1024 at 2^22) and N2 = 2^(e - e1) row points
 // (at most 4096).
 __host__ __device__ constexpr int qcf_e1(int e) { return e >= 22 ? e - 12 : e / 2 < 9 ? e / 2 : 9; }
+// The centred mode is n = 2^22, the only size with 1024-point columns.
+__host__ __device__ constexpr bool qcf_col_center(int e1) { return e1 >= 10; }
+static_assert(qcf_col_center(qcf_e1(22)) && !qcf_col_center(qcf_e1(21)) && qcf_center(22) && !qcf_center(21),
+              "centred mode <=> 1024-point columns");
 // Columns per CTA of the tile-layout column passes of n = 2^e.
 __host__ __device__ constexpr int qcf_tile_kc(int e) { return qcf_e1(e) >= 10 ? 4 : 8; }
 // Centring offset (1 + B) / 2 of the n = 2^22 packing (B = 2^21 + 1).
@@ -292,16 +296,18 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 // instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
 // columns of the CTA's tile in row j1 (qcf_gather).  centred mode (par !=
 // nullptr): planes centred, and par[y] ^= the XOR of the CTA's words (byte q:
-// column parities of plane 4y + q; only the CTA's KC columns).
-template <int E1, int KC>
+// column parities of plane 4y + q; only the CTA's KC columns).  CEN: the
+// kernel has the centred mode (compiled in for the 1024-point columns of
+// n = 2^22 only).
+template <int E1, int KC, bool CEN>
 __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC)) qcf_col_fwd(
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2, int wide,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     double2 *__restrict__ Y, const unsigned long long *__restrict__ wa, uint32_t *__restrict__ par) {
   constexpr int N1 = 1 << E1, ld = sld<KC>(N1), W = qcf_fs_ld(E1);
   const uint32_t base = (1u << 21) + uint32_t(wide);
-  const double center = par ? double(kCenter) : 0.0;
-  const uint32_t comp = wa && *wa > (1ull << (E1 + e2 - 1)) ? 1u : 0u;
+  const double center = CEN && par ? double(kCenter) : 0.0;
+  const uint32_t comp = CEN && wa && *wa > (1ull << (E1 + e2 - 1)) ? 1u : 0u;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
   double2 *xs = sm, *fss = xs + KC * ld;
@@ -324,7 +330,7 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
     }
   }
   __syncthreads();
-  if (par) {  // plane weight parities (XOR of the CTA's words)
+  if (CEN && par) {  // plane weight parities (XOR of the CTA's words)
     constexpr uint32_t mask = KC == 8 ? 0xffffffffu : 0x0f0f0f0fu;
     uint32_t x = 0;
     for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) x ^= bits[j1] & (mask << sub);
@@ -493,8 +499,8 @@ __device__ __forceinline__ void plane_bits(double v, int wide, int64_t shift, ui
 // order).  KC = 4 writes tiles only.
 // centred mode (par != nullptr): the transform's A_hat trailer (ahat) gives
 // w(a); the centring shift is added back and, for a complemented `a`, each
-// plane's weight parity (par[y]) is XORed in.
-template <int E1, int KC>
+// plane's weight parity (par[y]) is XORed in (CEN: as for qcf_col_fwd).
+template <int E1, int KC, bool CEN>
 __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC)) qcf_col_inv(
     const double2 *__restrict__ Y, int e2, int wide, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     uint8_t *__restrict__ out, uint64_t stride_bytes, int nplanes, int accumulate, uint32_t *__restrict__ tiles,
@@ -508,7 +514,7 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
   const int p0 = 4 * blockIdx.y;
   int64_t shift = 0;
   uint32_t flip = 0;  // bit q: XOR into plane 4y + q
-  if (par) {
+  if (CEN && par) {
     const uint64_t n = 1ull << (E1 + e2);
     const uint64_t w = *reinterpret_cast<const unsigned long long *>(
         static_cast<const uint8_t *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) + 16 * n);
@@ -558,8 +564,10 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
         uint32_t pl[4];
         plane_bits(x[m].x, wide, shift, pl[0], pl[1]);
         plane_bits(x[m].y, wide, shift, pl[2], pl[3]);
+        if constexpr (CEN) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) pl[q] ^= (flip >> q) & 1u;
+          for (int q = 0; q < 4; q++) pl[q] ^= (flip >> q) & 1u;
+        }
         const int j1 = i0 + Q::M * m;
         constexpr uint32_t cm = (1u << KC) - 1;
         uint32_t word = 0;
@@ -642,11 +650,13 @@ __device__ __forceinline__ uint32_t spread_nibbles(uint32_t x) {
 }
 
 // The inverse of qcf_gather; out[j] = (xor_in ? xor_in[j] : 0) ^ block j.
-// halves: the words hold two 16-bit halves from 4-column CTAs (low: columns
-// 0-3, high: 4-7; nibble q of each: plane q), put back in byte order first.
+// HALVES: the words hold two 16-bit halves from 4-column CTAs (low: columns
+// 0-3, high: 4-7; nibble q of each: plane q), put back in byte order first
+// (a template parameter: a runtime branch in the unrolled loop cost the
+// loads' overlap, 2-7 % of the small dual LPNs).
+template <bool HALVES>
 __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ tiles, uint64_t ngroups,
-                                                   const uint4 *__restrict__ xor_in, uint4 *__restrict__ out,
-                                                   int halves) {
+                                                   const uint4 *__restrict__ xor_in, uint4 *__restrict__ out) {
   for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups;
        g += uint64_t(gridDim.x) * blockDim.x) {
     uint32_t w[8][4];
@@ -660,7 +670,7 @@ __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ 
       for (int k = 0; k < 4; k++) {
         const int t = 8 * wd + 2 * k;
         uint32_t lo = __ldg(&tiles[uint64_t(t) * ngroups + g]), hi = __ldg(&tiles[uint64_t(t + 1) * ngroups + g]);
-        if (halves) {
+        if constexpr (HALVES) {
           lo = spread_nibbles(lo & 0xffffu) | (spread_nibbles(lo >> 16) << 4);
           hi = spread_nibbles(hi & 0xffffu) | (spread_nibbles(hi >> 16) << 4);
         }
@@ -779,11 +789,11 @@ int set_attrs() {
   cudaGetDevice(&dev);
   if (dev < 64 && done[dev]) return CUOT_OK;
   bool ok = true;
-#define QCF_SETK(E, K)                                                                                   \
-  ok &= cudaFuncSetAttribute(qcf_col_fwd<E, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E, K)) == \
-        cudaSuccess;                                                                                         \
-  ok &= cudaFuncSetAttribute(qcf_col_inv<E, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, col_smem(E, K)) == \
-        cudaSuccess;
+#define QCF_SETK(E, K)                                                                                  \
+  ok &= cudaFuncSetAttribute(qcf_col_fwd<E, K, qcf_col_center(E)>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             col_smem(E, K)) == cudaSuccess;                                                \
+  ok &= cudaFuncSetAttribute(qcf_col_inv<E, K, qcf_col_center(E)>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             col_smem(E, K)) == cudaSuccess;
 #define QCF_SET(E) QCF_SETK(E, 8)
 #define QCF_SETR(E) \
   ok &= cudaFuncSetAttribute(qcf_row<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, row_smem(E)) == cudaSuccess;
@@ -809,7 +819,7 @@ void launch_col_fwd(const QcfTables *t, int ntr, cudaStream_t st, const uint8_t 
   const int kc = tiles ? qcf_tile_kc(t->e) : 8;
   const dim3 grid((1u << t->e2) / kc, ntr);
 #define QCF_LK(E, K)                                                                                           \
-  qcf_col_fwd<E, K><<<grid, qcf_col_threads(E, K), col_smem(E, K), st>>>(                                     \
+  qcf_col_fwd<E, K, qcf_col_center(E)><<<grid, qcf_col_threads(E, K), col_smem(E, K), st>>>(                  \
       in, stride_bytes, nplanes, one_plane, t->e2, qcf_wide(t->e), tiles, t->T1, t->fs, Y, wa, par);
   if (kc == 4) {
     QCF_LK(10, 4)
@@ -843,7 +853,7 @@ void launch_col_inv(const QcfTables *t, int ntr, cudaStream_t st, const double2 
   const int kc = tiles ? qcf_tile_kc(t->e) : 8;
   const dim3 grid((1u << t->e2) / kc, ntr);
 #define QCF_LK(E, K)                                                                                         \
-  qcf_col_inv<E, K><<<grid, qcf_col_threads(E, K), col_smem(E, K), st>>>(                                   \
+  qcf_col_inv<E, K, qcf_col_center(E)><<<grid, qcf_col_threads(E, K), col_smem(E, K), st>>>(                \
       Y, t->e2, qcf_wide(t->e), t->T1, t->fs, out, stride_bytes, nplanes, accumulate, tiles, ahat, par);
   if (kc == 4) {
     QCF_LK(10, 4)
@@ -1015,8 +1025,13 @@ int qcf_gather(int e, const cuot_block *in, uint32_t *tiles, cudaStream_t st) {
 
 int qcf_scatter(int e, const uint32_t *tiles, const cuot_block *xor_in, cuot_block *out, cudaStream_t st) {
   const uint64_t ng = 1ull << (e - 3);
-  qcf_scatter<<<unsigned((ng + 255) / 256), 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
-                                                           reinterpret_cast<uint4 *>(out), qcf_tile_kc(e) == 4);
+  const dim3 grid(unsigned((ng + 255) / 256));
+  if (qcf_tile_kc(e) == 4)
+    qcf_scatter<true><<<grid, 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
+                                            reinterpret_cast<uint4 *>(out));
+  else
+    qcf_scatter<false><<<grid, 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
+                                             reinterpret_cast<uint4 *>(out));
   return launch_status();
 }
 
