@@ -38,20 +38,23 @@
 //
 // Four-step transform, n = N1 * N2 (N1 = 2^e1 <= 1024, N1 <= N2 <= 4096), input
 // index j = N2*j1 + j2, frequency k = k1 + N1*k2:
-//   A (columns): 8 columns j2 of one transform per CTA: load the plane bits,
-//     N1-point DIF FFT over j1 (frequencies land in bit-reversed row order r),
-//     multiply by w_n^(j2 * rev(r)), store Y[r][j2].
+//   A (columns): 8 columns j2 of one transform per CTA (4 for the 1024-point
+//     columns of the tile layout): load the plane bits, N1-point DIF FFT over
+//     j1 (frequencies land in bit-reversed row order r), multiply by
+//     w_n^(j2 * rev(r)), store Y[r][j2].
 //   B (rows): 4 rows (2 at N2 = 2048, 1 at 4096) per CTA: N2-point DIF FFT, multiply by A_hat (the
 //     transform of `a` in the same layout, scaled by 1/n), N2-point DIT
 //     inverse, store.
 //   C (columns): multiply by w_n^-(j2 * rev(r)), N1-point DIT inverse over r,
-//     round, extract the four planes' bits, store (or XOR) 8 columns per byte.
+//     round, extract the four planes' bits, store (or XOR) 8 columns per byte
+//     (4-column CTAs: one 16-bit half of the tile word).
 // An N-point transform runs in shared memory as 2-3 passes of 2^K-point
 // butterflies in registers (K <= 4, constant internal twiddles), each pass
 // followed by one multiplication with w_S^(base * q) from a table.  The 8
-// transforms of a CTA sit in rows of N + 1 complex values and the 8 lanes of
-// each quarter-warp work on the same item of the 8 transforms, so every
-// shared-memory access is conflict-free.
+// transforms (columns) of a CTA sit in rows of N + 1 complex values and the 8
+// lanes of each quarter-warp work on the same item of the 8 transforms; with
+// 4 (2, 1) per CTA, rows of N + 2 (N + 4, N) and an XOR swizzle (spos), so
+// every shared-memory access is conflict-free.
 #include "ctx.cuh"
 
 namespace cuot {
