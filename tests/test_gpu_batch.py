@@ -68,3 +68,32 @@ def test_configs3_shaped_mix_is_a_cot_everywhere(ctx):
         ev, ew, ec = oracle_outputs(inst)
         assert np.array_equal(v, ev) and np.array_equal(w, ew)
     b.close()
+
+
+def test_large_sot_batch_equals_plain_and_is_a_cot(ctx):
+    """SOT instances at n = 2^21 and 2^22 (the direct FFT: 512 x 4096, and
+    1024 x 4096 with centred planes against the lighter of a and ~a in
+    4-column CTAs) beside a small Ferret instance: the graph-captured batched
+    program gives the plain path's outputs (the one-shot entry points, checked
+    against the oracle by the QC tests), and each SOT instance's outputs form
+    a COT, w_j = v_j ^ c_j * delta."""
+    specs = [(KIND_SOT, 512, 12, 0), (KIND_SOT, 1024, 12, 0), (KIND_FERRET, 8, 10, 1000)]
+    insts = [Instance(ctx, kd, t, h, 300 + i, k=k) for i, (kd, t, h, k) in enumerate(specs)]
+    stream = torch.cuda.Stream()
+    b = Batch(ctx, insts, use_graph=True)
+    b.run(stream)
+    got = snapshot(insts)
+    for inst in insts:
+        inst.v.zero_(); inst.w.zero_()
+    b.run_plain(stream)
+    plain = snapshot(insts)
+    for inst, g, p in zip(insts, got, plain):
+        assert np.array_equal(g[0], p[0]) and np.array_equal(g[1], p[1])
+        if inst.kind == KIND_SOT:
+            assert np.array_equal(g[2], p[2])
+            cbits = np.unpackbits(g[2].view(np.uint8), bitorder="little").astype(bool)
+            diff = g[0] ^ g[1]
+            assert not diff[~cbits].any()
+            assert (diff[cbits] == inst.delta).all()
+            assert 0.4 < cbits.mean() < 0.6
+    b.close()
