@@ -165,6 +165,12 @@ void cuda_mpcot_recver(Mat *expanded, Mat *buffer, Mat *sep, blk *cSum_h, blk *s
   });
 }
 
+// `key` is emp's PRP(seed).aes.rd_key (lpn_f2.h:82-86): the expanded AES-128
+// schedule, whose round key 0 is the cipher key itself (FIPS-197 5.2: the
+// first Nk words of the schedule are the key), so its first 16 bytes are the
+// LPN seed that the index AES is keyed with.  Each n[g] must be a multiple of
+// 4 except the last GPU's: the row-range LPN starts every range on a 4-row
+// group, and FerretCOT's n[g] = trees x 2^h always is (ferret_cot.hpp:55-63).
 void cuda_primal_lpn(Role role, Mat *pubMats, int64_t d, int64_t *n, int k, uint32_t *key,
                      Mat *expanded, blk *nn, Mat *kk_d, blk *kk, int ngpu) {
   (void)role;

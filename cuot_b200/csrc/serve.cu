@@ -221,8 +221,8 @@ int enqueue_request(Slot &s, cudaStream_t st, const cuot_request &r, std::vector
 
 // Starts request r on slot s: its work, then the stream-ordered frees of its
 // buffers (also after a failed enqueue) and the slot's completion event.
-int start_request(cuot_server *sv, Slot &s, const cuot_request &r) {
-  const bool hi = sv->cfg.high_priority_below_n && req_n(r) < sv->cfg.high_priority_below_n;
+int start_request(const cuot_server_config &cfg, Slot &s, const cuot_request &r) {
+  const bool hi = cfg.high_priority_below_n && req_n(r) < cfg.high_priority_below_n;
   cudaStream_t st = hi ? s.hi : s.lo;
   s.cur = st;
   std::vector<void *> bufs;
@@ -357,10 +357,17 @@ int cuot_server_cancel(cuot_server *sv, int index) {
 
 int cuot_server_run(cuot_server *sv, cuot_request *reqs, int count, cuot_server_stats *stats) {
   if (!sv || (count > 0 && !reqs) || count < 0) return fail(CUOT_EINVAL, "bad argument");
-  const bool dry = sv->cfg.dry_run_service_s > 0;
+  // cuot_server_configure may change the scheduling fields from another
+  // thread while this loop runs: every iteration works on a copy taken under
+  // the server's mutex.
+  cuot_server_config cfg;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    cfg = sv->cfg;
+  }
+  const bool dry = cfg.dry_run_service_s > 0;
   if (!dry) cudaSetDevice(sv->device);
-  const double budget = sv->cfg.budget_bytes - double(sv->reserved);
-  const int max_log_n = sv->cfg.max_log_n > 0 ? sv->cfg.max_log_n : 24;
+  const int max_log_n = cfg.max_log_n > 0 ? cfg.max_log_n : 24;
   std::vector<int> order(count);
   for (int i = 0; i < count; i++) {
     order[i] = i;
@@ -376,9 +383,14 @@ int cuot_server_run(cuot_server *sv, cuot_request *reqs, int count, cuot_server_
   int nbusy = 0;
   size_t next = 0;
   const double t0 = now_s();
-  auto is_big = [&](const cuot_request &r) { return sv->cfg.big_n && req_n(r) >= sv->cfg.big_n; };
+  auto is_big = [&](const cuot_request &r) { return cfg.big_n && req_n(r) >= cfg.big_n; };
   int rc = CUOT_OK;
   while (next < order.size() || !queue.empty() || nbusy) {
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      cfg = sv->cfg;
+    }
+    const double budget = cfg.budget_bytes - double(sv->reserved);
     const double now = now_s() - t0;
     while (next < order.size() && reqs[order[next]].arrival <= now) {
       const int i = order[next++];
@@ -417,11 +429,11 @@ int cuot_server_run(cuot_server *sv, cuot_request *reqs, int count, cuot_server_
     // cancellations and queue timeouts
     {
       std::lock_guard<std::mutex> lk(sv->mu);
-      if (!sv->cancelled.empty() || sv->cfg.max_queue_wait > 0) {
+      if (!sv->cancelled.empty() || cfg.max_queue_wait > 0) {
         std::deque<int> keep;
         for (int i : queue) {
           if (sv->cancelled.count(i)) reqs[i].status = CUOT_REQ_CANCELLED;
-          else if (sv->cfg.max_queue_wait > 0 && now - reqs[i].arrival > sv->cfg.max_queue_wait)
+          else if (cfg.max_queue_wait > 0 && now - reqs[i].arrival > cfg.max_queue_wait)
             reqs[i].status = CUOT_REQ_TIMEOUT;
           else keep.push_back(i);
         }
@@ -437,7 +449,7 @@ int cuot_server_run(cuot_server *sv, cuot_request *reqs, int count, cuot_server_
       for (size_t j = 0; j < queue.size(); j++) {
         const cuot_request &r = reqs[queue[j]];
         if (used + double(footprint(r)) > budget) break;  // memory is head-of-line
-        if (is_big(r) && nbig >= std::max(1, sv->cfg.max_big)) continue;
+        if (is_big(r) && nbig >= std::max(1, cfg.max_big)) continue;
         pick = int(j);
         break;
       }
@@ -453,8 +465,8 @@ int cuot_server_run(cuot_server *sv, cuot_request *reqs, int count, cuot_server_
       busy[s] = i;
       nbusy++;
       if (dry) {
-        sv->slots[s].dry_end = now_s() + sv->cfg.dry_run_service_s;
-      } else if ((rc = start_request(sv, sv->slots[s], reqs[i]))) {
+        sv->slots[s].dry_end = now_s() + cfg.dry_run_service_s;
+      } else if ((rc = start_request(cfg, sv->slots[s], reqs[i]))) {
         break;
       }
     }

@@ -29,7 +29,28 @@ of the process group's device (NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
+from contextlib import contextmanager
 from dataclasses import dataclass
+
+
+@contextmanager
+def _on_stream(stream, device):
+    """Runs the body with `stream` (default: the current stream) as torch's
+    current stream, after it has waited for the work already queued on the
+    caller's current stream (which produced the inputs).  Everything in a
+    shard function -- the library calls, torch's own kernels and NCCL's
+    collectives, which order themselves after the current stream -- then
+    runs in one order on one stream.  Yields None for CPU tensors."""
+    import torch
+    if device.type != "cuda":
+        yield None
+        return
+    cur = torch.cuda.current_stream(device)
+    s = cur if stream is None else stream
+    if s != cur:
+        s.wait_stream(cur)
+    with torch.cuda.stream(s):
+        yield s
 
 
 @dataclass(frozen=True)
@@ -68,20 +89,21 @@ def ferret_extend_rank(ctx, plan: ShardPlan, rank: int, roots, delta, choice, se
     sender MPCOT -> (ideal OT of the sums) -> receiver MPCOT -> LPN of this
     rank's rows on both roles (kk_s / kk_r: the two roles' LPN inputs).
     Returns (v, w): this rank's rows of the sender's and the receiver's
-    outputs."""
+    outputs, written in order on `stream` (default: the current stream)."""
     import torch
     t, h = plan.trees(rank), plan.h
     n_r = t << h
     dev = roots.device
-    emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device=dev)
-    v, w = emp(n_r), emp(n_r)
-    lsum, rsum, ss, mc = emp(t * h), emp(t * h), emp(t), emp(t * h)
-    ctx.ferret_pprf_sender(roots, h, delta, v, lsum, rsum, ss, stream=stream)
-    torch.where(choice.view(-1, 1).bool(), rsum, lsum, out=mc)
-    ctx.ferret_pprf_recver(mc, choice, ss, h, w, stream=stream)
-    lo, hi = plan.rows(rank)
-    ctx.lpn_primal_range(seed, kk_s, v, lo, hi, plan.n, stream=stream)
-    ctx.lpn_primal_range(seed, kk_r, w, lo, hi, plan.n, stream=stream)
+    with _on_stream(stream, dev) as s:
+        emp = lambda m: torch.empty((m, 16), dtype=torch.uint8, device=dev)
+        v, w = emp(n_r), emp(n_r)
+        lsum, rsum, ss, mc = emp(t * h), emp(t * h), emp(t), emp(t * h)
+        ctx.ferret_pprf_sender(roots, h, delta, v, lsum, rsum, ss, stream=s)
+        torch.where(choice.view(-1, 1).bool(), rsum, lsum, out=mc)
+        ctx.ferret_pprf_recver(mc, choice, ss, h, w, stream=s)
+        lo, hi = plan.rows(rank)
+        ctx.lpn_primal_range(seed, kk_s, v, lo, hi, plan.n, stream=s)
+        ctx.lpn_primal_range(seed, kk_r, w, lo, hi, plan.n, stream=s)
     return v, w
 
 
@@ -151,21 +173,20 @@ def sot_dual_lpn_rank(ctx, plan: ShardPlan, rank: int, a, rows, stream=None):
     """Rate-1 dual LPN of one SOT instance split over the ranks: `rows` holds
     this rank's noise blocks (rows_r x 16 bytes, the expansion of its own
     trees); returns its rows of out = a * e mod (x^n - 1) per bit plane,
-    bit-identical to the unsplit cuot_sot_dual_lpn."""
+    bit-identical to the unsplit cuot_sot_dual_lpn, written in order on
+    `stream` (default: the current stream; the all-to-alls wait for it)."""
     import torch
     lo, hi = plan.rows(rank)
     nr = hi - lo
     dev = rows.device
-    local = torch.empty((128, nr // 8), dtype=torch.uint8, device=dev)
-    ctx.bit_transpose(rows, nr, 16, 0, 128, local, stream=stream)
-    s = torch.cuda.current_stream() if stream is None else stream
-    s.synchronize()
-    mine = planes_to_owners(local, plan, rank)
-    p_lo, p_hi = plane_range(plan.world, rank)
-    if p_hi > p_lo:
-        ctx.qc_encode(a, mine.view(torch.int64), plan.n, p_hi - p_lo, stream=stream)
-        s.synchronize()
-    back = owners_to_rows(mine, plan, rank)
-    out = torch.empty((nr, 16), dtype=torch.uint8, device=dev)
-    ctx.bit_transpose(back, 128, nr // 8, 0, nr, out, stream=stream)
+    with _on_stream(stream, dev) as s:
+        local = torch.empty((128, nr // 8), dtype=torch.uint8, device=dev)
+        ctx.bit_transpose(rows, nr, 16, 0, 128, local, stream=s)
+        mine = planes_to_owners(local, plan, rank)
+        p_lo, p_hi = plane_range(plan.world, rank)
+        if p_hi > p_lo:
+            ctx.qc_encode(a, mine.view(torch.int64), plan.n, p_hi - p_lo, stream=s)
+        back = owners_to_rows(mine, plan, rank)
+        out = torch.empty((nr, 16), dtype=torch.uint8, device=dev)
+        ctx.bit_transpose(back, 128, nr // 8, 0, nr, out, stream=s)
     return out

@@ -40,6 +40,90 @@ def ref_lib():
     return _REF
 
 
+_EMP = None
+
+
+def emp_lib():
+    """oracle/_ref/libempref.so: the reference's own emp-ot Ferret headers
+    (twokeyprp.h, spcot_sender.h, spcot_recver.h, lpn_f2.h) compiled from the
+    reference tree over the emp-tool shim (oracle/emp_shim), or None when it
+    was not built."""
+    global _EMP
+    if _EMP is None:
+        path = os.path.join(_HERE, "_ref", "libempref.so")
+        if not os.path.exists(path):
+            return None
+        _EMP = ctypes.CDLL(path)
+        _EMP.ref_lpn_task.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_int64, C.c_int64, C.c_int64]
+    return _EMP
+
+
+def emp_aes_ecb(key, blocks: np.ndarray):
+    """AES-128 ECB through the emp-tool shim (AES_set_encrypt_key +
+    AES_ecb_encrypt_blks)."""
+    inp = np.ascontiguousarray(blocks, np.uint8).reshape(-1, 16)
+    out = np.empty_like(inp)
+    emp_lib().ref_emp_aes_ecb(_p(_u8(key)), _p(inp), _p(out), C.c_uint64(inp.shape[0]))
+    return out
+
+
+def emp_spcot_sender(roots, h: int, delta):
+    """SPCOT_Sender::compute (spcot_sender.h:40-86) per tree, seed = root:
+    (leaves [t*2^h], ot_msg_0 [t*h], ot_msg_1 [t*h], secret_sum [t]) in the
+    MPCOT layout (tree-major leaves, [tree][level] messages).  h >= 2."""
+    roots = np.ascontiguousarray(roots, np.uint8).reshape(-1, 16)
+    t = roots.shape[0]
+    leaves = np.empty((t << h, 16), np.uint8)
+    m0 = np.empty((t * h, 16), np.uint8)
+    m1 = np.empty((t * h, 16), np.uint8)
+    ss = np.empty((t, 16), np.uint8)
+    d = _u8(delta)
+    L = emp_lib()
+    for i in range(t):
+        rc = L.ref_spcot_sender(_p(roots[i]), INT(h), _p(d), _p(leaves[i << h:(i + 1) << h]),
+                                _p(m0[i * h:(i + 1) * h]), _p(m1[i * h:(i + 1) * h]), _p(ss[i]))
+        assert rc == 0, f"ref_spcot_sender rejected h={h}"
+    return leaves, m0, m1, ss
+
+
+def emp_spcot_recver(mc, choice, secret_sum, h: int):
+    """SPCOT_Recver::get_index + compute (spcot_recver.h:33-95) per tree:
+    (leaves [t*2^h], punctured index [t])."""
+    ss = np.ascontiguousarray(secret_sum, np.uint8).reshape(-1, 16)
+    t = ss.shape[0]
+    mc = np.ascontiguousarray(mc, np.uint8).reshape(t * h, 16)
+    ch = np.ascontiguousarray(choice, np.uint8).reshape(t * h)
+    leaves = np.empty((t << h, 16), np.uint8)
+    pos = np.empty(t, np.int32)
+    L = emp_lib()
+    for i in range(t):
+        p = C.c_int(0)
+        rc = L.ref_spcot_recver(INT(h), _p(ch[i * h:(i + 1) * h]), _p(mc[i * h:(i + 1) * h]), _p(ss[i]),
+                                _p(leaves[i << h:(i + 1) << h]), C.byref(p))
+        assert rc == 0
+        pos[i] = p.value
+    return leaves, pos
+
+
+def emp_lpn_task(seed, kk, nn, d: int = 10, start: int = 0, end: int | None = None,
+                 inplace: bool = False) -> np.ndarray:
+    """LpnF2<IO, d>::task(nn, kk, start, end) (lpn_f2.h:46-79): one task
+    over rows [start, end), default [0, n), on a copy of nn (or on nn itself,
+    a C-contiguous (n, 16) uint8 array, with inplace=True)."""
+    kk = np.ascontiguousarray(kk, np.uint8).reshape(-1, 16)
+    if inplace:
+        assert nn.dtype == np.uint8 and nn.flags["C_CONTIGUOUS"] and nn.shape[-1] == 16
+        out = nn.reshape(-1, 16)
+    else:
+        out = np.array(nn, dtype=np.uint8, copy=True).reshape(-1, 16)
+    n = out.shape[0]
+    end = n if end is None else end
+    rc = emp_lib().ref_lpn_task(_p(_u8(seed)), _p(kk), kk.shape[0], d, _p(out), n, start, end)
+    assert rc == 0, "ref_lpn_task rejected its arguments"
+    return out
+
+
 def _p(a: np.ndarray):
     assert a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(ctypes.c_void_p)

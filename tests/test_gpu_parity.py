@@ -407,10 +407,14 @@ def test_lpn_row_ranges_equal_unsplit(ctx, n, k, cuts):
         assert np.array_equal(to_host(part), exp[lo:hi])
 
 
-def test_sharded_ferret_extend_equals_unsplit(ctx):
+@pytest.mark.parametrize("side_stream", [False, True])
+def test_sharded_ferret_extend_equals_unsplit(ctx, side_stream):
     """The per-rank share computation of cuot_b200.shard, run for each of 3
-    ranks in turn on this GPU, concatenates to the unsplit extension."""
+    ranks in turn on this GPU, concatenates to the unsplit extension, also
+    when the caller passes a stream other than the current one (its torch
+    ops must then run on that stream too)."""
     from cuot_b200.shard import ShardPlan, ferret_extend_rank
+    side = torch.cuda.Stream() if side_stream else None
     t, h, k = 10, 8, 999
     rng = np.random.default_rng(31)
     roots, delta = rng_blocks(rng, t), delta_ferret(rng)
@@ -421,7 +425,10 @@ def test_sharded_ferret_extend_equals_unsplit(ctx):
     for r in range(3):
         f, tr = plan.first_tree(r), plan.trees(r)
         v, w = ferret_extend_rank(ctx, plan, r, to_dev(roots[f:f + tr]), delta,
-                                  to_dev(choice[f * h:(f + tr) * h]), seed, to_dev(kk_s), to_dev(kk_r))
+                                  to_dev(choice[f * h:(f + tr) * h]), seed, to_dev(kk_s), to_dev(kk_r),
+                                  stream=side)
+        if side is not None:
+            side.synchronize()
         vs.append(to_host(v))
         ws.append(to_host(w))
     leaves, lsum, rsum, ss = oracle.ferret_pprf_sender(roots, h, delta, threads=4)
@@ -431,11 +438,13 @@ def test_sharded_ferret_extend_equals_unsplit(ctx):
     assert np.array_equal(np.concatenate(ws), oracle.lpn_primal(seed, kk_r, rleaves))
 
 
-def test_sharded_sot_dual_lpn_one_rank_nccl(ctx):
+@pytest.mark.parametrize("side_stream", [False, True])
+def test_sharded_sot_dual_lpn_one_rank_nccl(ctx, side_stream):
     """cuot_b200.shard's SOT path (transpose -> all-to-all to plane owners ->
     encode -> reverse all-to-all -> transpose) through a one-rank NCCL group
-    on this GPU equals the unsplit dual LPN.  The multi-rank exchange itself
-    is covered by the gloo tests in test_shard.py."""
+    on this GPU equals the unsplit dual LPN, on the current stream and on a
+    side stream the caller passes.  The multi-rank exchange itself is covered
+    by the gloo tests in test_shard.py."""
     import datetime
     import socket
     import torch.distributed as dist
@@ -453,7 +462,10 @@ def test_sharded_sot_dual_lpn_one_rank_nccl(ctx):
         rows = rng_blocks(rng, n)
         a = torch.empty(n // 64, dtype=torch.int64, device="cuda")
         ctx.qc_gen_a(rng_blocks(rng, 1)[0], n, a)
-        out = sot_dual_lpn_rank(ctx, ShardPlan(t, h, 1), 0, a, to_dev(rows))
+        side = torch.cuda.Stream() if side_stream else None
+        out = sot_dual_lpn_rank(ctx, ShardPlan(t, h, 1), 0, a, to_dev(rows), stream=side)
+        if side is not None:
+            side.synchronize()
         exp = oracle.sot_dual_lpn(to_host(a).view(np.uint64), rows, n, threads=8)
         assert np.array_equal(to_host(out), exp)
     finally:

@@ -35,10 +35,17 @@ def _noalloc(lib, roots, t, h, delta, leaves, lsum, rsum, ss):
         C.c_void_p(torch.cuda.current_stream().cuda_stream))
 
 
-def test_noalloc_sender_equals_ordinary_sender_twice(ctx):
+@pytest.fixture(scope="module")
+def lib():
     lib = cuot_b200.load()
-    # two calls in a row with different shapes and inputs
-    for t, h, seed in [(64, 10, 11), (300, 9, 12)]:
+    lib.cuot_last_error.restype = C.c_char_p
+    return lib
+
+
+def test_noalloc_sender_equals_ordinary_sender_twice(ctx, lib):
+    # calls in a row with different shapes and inputs; the last one fills the
+    # scratch array to its limit, t * 2^h = 2^20 leaves
+    for t, h, seed in [(64, 10, 11), (300, 9, 12), (1024, 10, 13)]:
         rng = np.random.default_rng(seed)
         roots, delta = rng_blocks(rng, t), delta_ferret(rng)
         droots = to_dev(roots)
@@ -52,11 +59,12 @@ def test_noalloc_sender_equals_ordinary_sender_twice(ctx):
             assert np.array_equal(to_host(got), to_host(exp))
 
 
-def test_noalloc_rejects_sizes_beyond_its_scratch():
-    lib = cuot_b200.load()
-    lib.cuot_last_error.restype = C.c_char_p
+def test_noalloc_rejects_sizes_beyond_its_scratch(lib):
     small = torch.empty((16, 16), dtype=torch.uint8, device="cuda")
     delta = np.zeros(16, np.uint8)
-    st = _noalloc(lib, small, 2048, 10, delta, small, small, small, small)  # 2^21 leaves > 2^20
-    assert st == 1
-    assert b"no-alloc limit" in lib.cuot_last_error()
+    # one tree past the limit (2^20 + 2^10 leaves), and twice the limit; the
+    # arguments are rejected before anything is launched
+    for t, h in [(1025, 10), (2048, 10)]:
+        st = _noalloc(lib, small, t, h, delta, small, small, small, small)
+        assert st == 1
+        assert b"no-alloc limit" in lib.cuot_last_error()
