@@ -18,6 +18,8 @@ Workloads (--workload):
   sot_n20_r2  SOT rate-1/2 form with n = 2^20 outputs: 512 trees of depth
               12 give 2n noise blocks e = (e0, e1) per role, encoded as
               e0 ^ a * e1 (the flagged second SOT configuration).
+  sot_n21, sot_n22  plain SOT at n = 2^21 and 2^22 (512 / 1024 trees of
+              depth 12), the largest sizes of the batched mix.
   ferret_b13  plain Ferret at full size (ferret_b13): n = 10,485,760,
               t = 1280 trees of depth 13, k = 452,000, d = 10 (both roles:
               MPCOT + primal LPN).
@@ -32,9 +34,13 @@ Multi-GPU: one process per GPU (torchrun), each rank runs its own instance
 (the path shards by independent instances; no data-path collective):
 "scaling": "weak", value = COTs of all ranks / max-over-ranks time.
 
---impl reference: the reference's CPU implementation of the path (emp-ot /
-cryptoTools semantics restated in oracle/, since emp-tool is not buildable
-here) timed on all host threads on a bounded sample of the same workload.
+--impl reference: the reference's CPU implementation of the path timed on
+all host threads on a bounded sample of the same workload: the Ferret GGM
+and LPN by the reference's own emp-ot headers (compiled over an emp-tool shim
+into oracle/_ref/libempref.so, where the reference tree was present at build
+time), the SOT PPRF and QC encode by the oracle's restatement (the reference
+has no CPU SOT code).  For the batched mix every one of its 64 instances is
+sampled (CpuMix).
 """
 from __future__ import annotations
 
@@ -57,6 +63,8 @@ WORKLOADS = {
     "mixed64_small": dict(kind="batch", count=64, lo=12, hi=16),
     "sot_n20": dict(kind="sot", t=256, h=12),
     "sot_n20_r2": dict(kind="sot", t=512, h=12, r2=True),
+    "sot_n21": dict(kind="sot", t=512, h=12),
+    "sot_n22": dict(kind="sot", t=1024, h=12),
     "ferret_b13": dict(kind="ferret", t=1280, h=13, k=452000, d=10),
     "ferret_b13_mal": dict(kind="ferret", t=1280, h=13, k=452000, d=10, mal=True),
     "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
@@ -70,6 +78,9 @@ CONFIG_TEXT = {
     "sot_n20": "plain SOT n=2^20: 256 GGM trees depth 12, exact QC encode of 128 planes, transposes (both roles)",
     "sot_n20_r2": "plain SOT rate-1/2, n=2^20 outputs: 512 GGM trees depth 12 (2n noise blocks), "
                   "out = e0 ^ a*e1 exact on 128 planes, transposes (both roles)",
+    "sot_n21": "plain SOT n=2^21: 512 GGM trees depth 12, exact QC encode of 128 planes, transposes (both roles)",
+    "sot_n22": "plain SOT n=2^22 (the mix's largest size): 1024 GGM trees depth 12, exact QC encode of 128 "
+               "planes, transposes (both roles)",
     "ferret_b13": "plain Ferret ferret_b13: n=10485760, t=1280, h=13, k=452000, d=10 (both roles)",
     "ferret_b13_mal": "ferret_b13 plus the malicious consistency check's per-tree GF(2^128) sums of both roles "
                       "(seeds given; their SHA-256 derivation is host protocol)",
@@ -225,8 +236,8 @@ class Instance:
                 self.sctx.ferret_chi_sum(self.leaves_s, h, self.d_chiseed, self.chi_v)
                 self.rctx.ferret_chi_sum(self.leaves_r, h, self.d_chiseed, self.chi_w)
             mark("chi1")
-            self.sctx.lpn_primal(self.seed, self.d_kk_s, self.leaves_s, d=self.d)
-            self.rctx.lpn_primal(self.seed, self.d_kk_r, self.leaves_r, d=self.d)
+            # both roles' LPN share the public seed: one dual-role launch
+            self.sctx.lpn_primal_dual(self.seed, self.d_kk_s, self.d_kk_r, self.leaves_s, self.leaves_r, d=self.d)
             mark("lpn1")
         else:
             t, h, n = self.t, self.h, self.n
@@ -442,8 +453,8 @@ def e2e_compute(inst: Instance, host, stream, slot: int = 0) -> int:
             if inst.mal:
                 inst.sctx.ferret_chi_sum(inst.leaves_s, inst.h, inst.d_chiseed, inst.chi_v, stream=stream)
                 inst.rctx.ferret_chi_sum(inst.leaves_r, inst.h, inst.d_chiseed, inst.chi_w, stream=stream)
-            inst.sctx.lpn_primal(inst.seed, din["kk_s"], inst.leaves_s, d=inst.d, stream=stream)
-            inst.rctx.lpn_primal(inst.seed, din["kk_r"], inst.leaves_r, d=inst.d, stream=stream)
+            inst.sctx.lpn_primal_dual(inst.seed, din["kk_s"], din["kk_r"], inst.leaves_s, inst.leaves_r, d=inst.d,
+                                      stream=stream)
         else:
             inst.sctx.sot_pprf_sender(din["roots"], inst.h, inst.delta, din["b0"], din["b1"], inst.leaves_s,
                                       inst.m0, inst.m1, stream=stream)
@@ -479,9 +490,48 @@ def make_host(inst: Instance):
 
 
 # --------------------------------------------------------------------------
+def ref_ferret_available() -> bool:
+    """True when oracle/_ref/libempref.so (the reference's own emp-ot GGM and
+    LPN code) was built and travelled with the repository."""
+    import oracle
+    return oracle.emp_lib() is not None
+
+
+def _ref_ferret_step(roots, h, delta, ch, kk, seed_b, threads: int):
+    """Both roles of one Ferret MPCOT + LPN through the reference's own
+    emp-ot code, threaded as emp-ot threads it: trees split over `threads`
+    workers, the LPN rows over `threads` LpnF2::task ranges (each with its own
+    __compute1 tail, as emp-ot's threaded LPN does)."""
+    import concurrent.futures as cf
+    import oracle
+    t = roots.shape[0]
+    cuts = [t * i // threads for i in range(threads + 1)]
+    ls = np.empty((t << h, 16), np.uint8)
+    lr = np.empty((t << h, 16), np.uint8)
+
+    def trees(i):
+        a, b = cuts[i], cuts[i + 1]
+        if b > a:
+            ls[a << h:b << h], lr[a << h:b << h] = oracle.emp_mpcot_trees(roots[a:b], h, delta, ch[a * h:b * h])
+
+    n = t << h
+    rcuts = [n * i // threads // 4 * 4 for i in range(threads)] + [n]
+
+    def rows(i):
+        for out in (ls, lr):
+            oracle.emp_lpn_task(seed_b, kk, out, start=rcuts[i], end=rcuts[i + 1], inplace=True)
+
+    with cf.ThreadPoolExecutor(max_workers=threads) as pool:
+        list(pool.map(trees, range(threads)))
+        list(pool.map(rows, range(threads)))
+    return ls, lr
+
+
 def cpu_sample(name: str, threads: int, budget_s: float = 10.0):
-    """Times the oracle port (restated emp-ot / cryptoTools CPU path) on a
-    bounded sample of the workload; returns (COTs/s, sample description)."""
+    """Times the CPU path on a bounded sample of the workload; returns
+    (COTs/s, sample description).  Ferret: the reference's own emp-ot code
+    (oracle/_ref/libempref.so) when it is built, else the oracle's
+    restatement; SOT: the oracle's restatement."""
     import oracle
     spec = WORKLOADS[name]
     rng = np.random.default_rng(99)
@@ -494,19 +544,25 @@ def cpu_sample(name: str, threads: int, budget_s: float = 10.0):
         delta[0] |= 1
         kk = blk(spec["k"])
         ch = rng.integers(0, 2, t * h).astype(np.uint8)
+        use_ref = ref_ferret_available() and spec["d"] == 10
         t0 = time.perf_counter()
         reps = 0
         while True:
-            lv, ls, rs, ss = oracle.ferret_pprf_sender(roots, h, delta, threads=threads)
-            mc = np.where(ch[:, None] == 0, ls, rs)
-            rl = oracle.ferret_pprf_recver(mc, ch, ss, h, threads=threads)
-            oracle.lpn_primal(blk(1)[0], kk, lv, d=spec["d"], threads=threads)
-            oracle.lpn_primal(blk(1)[0], kk, rl, d=spec["d"], threads=threads)
+            if use_ref:
+                _ref_ferret_step(roots, h, delta, ch, kk, blk(1)[0], threads)
+            else:
+                lv, ls, rs, ss = oracle.ferret_pprf_sender(roots, h, delta, threads=threads)
+                mc = np.where(ch[:, None] == 0, ls, rs)
+                rl = oracle.ferret_pprf_recver(mc, ch, ss, h, threads=threads)
+                oracle.lpn_primal(blk(1)[0], kk, lv, d=spec["d"], threads=threads)
+                oracle.lpn_primal(blk(1)[0], kk, rl, d=spec["d"], threads=threads)
             reps += 1
             el = time.perf_counter() - t0
             if el > budget_s or reps >= 3:
                 break
-        return reps * n / el, f"{t} of {t_full} trees (n={n}), both roles, MPCOT + LPN (k={spec['k']}), {reps} reps"
+        code = "reference emp-ot code (SPCOT_Sender/Recver, LpnF2::task)" if use_ref else "oracle restatement"
+        return reps * n / el, (f"{t} of {t_full} trees (n={n}), both roles, MPCOT + LPN (k={spec['k']}), "
+                               f"{reps} reps, {code}")
     # SOT: PPRF both roles on all trees; QC encode on a subset of planes, scaled
     r2 = bool(spec.get("r2"))
     nl = t_full << h
@@ -531,6 +587,110 @@ def cpu_sample(name: str, threads: int, budget_s: float = 10.0):
     return n / el, f"both roles PPRF on all {t_full} trees; QC encode timed on {nplanes} of 128 planes (one role) and scaled x{128 / nplanes * 2:g}"
 
 
+class CpuMix:
+    """The CPU path on the batched mix's own instances (the shapes the GPU
+    arm runs, `mixed_shapes` with the same seed), every instance sampled and
+    scaled to its full size.  `time_step()` times one pass and returns the
+    estimated COTs/s of the whole mix on `threads` host threads.
+
+    Work units, run as independent jobs on a pool of `threads` host threads
+    (each job single-threaded, so all cores are busy while any job is timed):
+      * Ferret-style instance: both roles of min(t, sample_trees) trees and
+        the LPN of their rows on both roles, with the instance's own k;
+        scaled by t / trees.  The reference's own emp-ot code does this
+        (SPCOT_Sender / SPCOT_Recver::compute, LpnF2::task, compiled from
+        its headers into oracle/_ref/libempref.so); without that library the
+        oracle's restatement does.
+      * SOT instance: the PPRF of both roles on the same tree sample plus the
+        two transposes of its rows, scaled by t / trees; and the exact QC
+        product of one bit plane of the instance's own n, scaled by 256 (128
+        planes x 2 roles).  The reference has no CPU SOT code, so these run
+        on the oracle's restatement.
+    The step time is then sum(job time x scale) / threads: the mix spread
+    over every host thread, each unit costing what it cost with all threads
+    busy."""
+
+    def __init__(self, spec: dict, threads: int, seed: int = 2024, sample_trees: int = 8):
+        import oracle
+        from cuot_b200.batch import mixed_shapes  # the workload's shapes only; no device code
+        self.threads = threads
+        self.shapes = mixed_shapes(spec["count"], seed, spec["lo"], spec["hi"])
+        self.use_ref = oracle.emp_lib() is not None
+        self.jobs = self._jobs(seed, sample_trees)
+        fer_code = ("the reference's own emp-ot code (oracle/_ref/libempref.so)" if self.use_ref
+                    else "the oracle's restatement")
+        self.sample = (
+            f"all {len(self.shapes)} instances of the mix (seed {seed}), each sampled and scaled: Ferret-style: both "
+            f"roles of {sample_trees} trees (or all, if fewer) + LPN of their rows on both roles, by {fer_code}, "
+            f"x t/trees; SOT (oracle restatement; the reference has no CPU SOT code): PPRF both roles + "
+            f"transposes on the same tree sample x t/trees, one bit plane's exact QC product of the instance's "
+            f"own n x 256; step time = sum of job times / {threads} threads, jobs run {threads} at a time")
+        # "reference" only when every leg runs the reference's own code; the
+        # SOT legs never do
+        self.kind = "port"
+
+    def _jobs(self, seed: int, sample_trees: int):
+        import oracle
+        from cuot_b200.batch import KIND_FERRET
+        use_ref = self.use_ref
+        rng = np.random.default_rng(seed)
+        blk = lambda m: rng.integers(0, 256, (m, 16), dtype=np.uint8)
+        jobs = []  # (fn, scale)
+        for kind, t, h, k in self.shapes:
+            n, ts = t << h, min(t, sample_trees)
+            roots, delta = blk(ts), blk(1)[0]
+            delta[0] |= 1
+            ch = rng.integers(0, 2, ts * h).astype(np.uint8)
+            if kind == KIND_FERRET:
+                kk, seed_b = blk(k), blk(1)[0]
+
+                def fer(roots=roots, h=h, delta=delta, ch=ch, kk=kk, seed_b=seed_b):
+                    if use_ref:
+                        ls, lr = oracle.emp_mpcot_trees(roots, h, delta, ch)
+                        oracle.emp_lpn_task(seed_b, kk, ls, inplace=True)
+                        oracle.emp_lpn_task(seed_b, kk, lr, inplace=True)
+                    else:
+                        lv, lsum, rsum, ss = oracle.ferret_pprf_sender(roots, h, delta)
+                        rl = oracle.ferret_pprf_recver(np.where(ch[:, None] == 0, lsum, rsum), ch, ss, h)
+                        oracle.lpn_primal(seed_b, kk, lv)
+                        oracle.lpn_primal(seed_b, kk, rl)
+                jobs.append((fer, t / ts))
+            else:
+                b0, b1 = blk(h * ts), blk(h * ts)
+                chs = rng.integers(0, 2, h * ts).astype(np.uint8)
+                mc = np.where(chs[:, None] == 0, b0, b1)
+                a = oracle.qc_gen_a(blk(1)[0], n)
+                plane = rng.integers(0, 2**63, (1, n // 64), dtype=np.uint64)
+
+                def sot_pprf(roots=roots, h=h, delta=delta, b0=b0, b1=b1, mc=mc, chs=chs, ts=ts):
+                    lv, m0, m1 = oracle.sot_pprf_sender(roots, h, delta, b0, b1)
+                    rl = oracle.sot_pprf_recver(m0, m1, mc, chs, ts, h)
+                    rows = ts << h
+                    for lvs in (lv, rl):
+                        pl = oracle.bit_transpose(lvs, rows, 16, 0, 128)
+                        oracle.bit_transpose(pl, 128, rows // 8, 0, rows)
+
+                def sot_qc(a=a, plane=plane, n=n):
+                    oracle.qc_encode(a, plane, n)
+                jobs.append((sot_pprf, t / ts))
+                jobs.append((sot_qc, 256.0))
+        return jobs
+
+    def time_step(self) -> float:
+        import concurrent.futures as cf
+
+        def timed(job):
+            t0 = time.perf_counter()
+            job[0]()
+            return (time.perf_counter() - t0) * job[1]
+
+        with cf.ThreadPoolExecutor(max_workers=self.threads) as pool:
+            # the 256-scaled plane jobs (the longest) first, so the pool drains evenly
+            order = sorted(range(len(self.jobs)), key=lambda j: -self.jobs[j][1])
+            total = sum(pool.map(lambda j: timed(self.jobs[j]), order))
+        return sum(t << h for _, t, h, _ in self.shapes) / (total / self.threads)
+
+
 # --------------------------------------------------------------------------
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -541,23 +701,11 @@ def run_reference(args):
     vals = []
     sample = ""
     spec = WORKLOADS[name]
-    if spec["kind"] == "batch":
-        # the mix's COTs split by kind (same generator as the GPU arm, no device)
-        rng = np.random.default_rng(2024)
-        n_sot = n_fer = 0
-        for i in range(spec["count"]):
-            e = int(rng.integers(spec["lo"], spec["hi"] + 1))
-            rng.integers(10, min(14, e) + 1)
-            if i % 2 == 0:
-                n_sot += 1 << e
-            else:
-                n_fer += 1 << e
+    kind = "port"
+    mix = CpuMix(spec, threads) if spec["kind"] == "batch" else None
     for i in range(args.warmup + args.steps):
-        if spec["kind"] == "batch":
-            v1, s1 = cpu_sample("sot_n20", threads, budget_s=2.0)
-            v2, s2 = cpu_sample("ferret_b13", threads, budget_s=2.0)
-            v = (n_sot + n_fer) / (n_sot / v1 + n_fer / v2)
-            sample = f"SOT: {s1}; Ferret: {s2}; weighted by the mix's COTs"
+        if mix is not None:
+            v, sample, kind = mix.time_step(), mix.sample, mix.kind
         elif spec["kind"] == "session":
             v, sample = cpu_sample("ferret_b13", threads, budget_s=5.0)
             v *= (spec["t"] << spec["h"]) - (spec["k"] + spec["t"] * spec["h"] + 128)
@@ -565,6 +713,8 @@ def run_reference(args):
             sample += "; usable COTs (ot_limit / n of the outputs)"
         else:
             v, sample = cpu_sample(name, threads, budget_s=5.0)
+        if spec["kind"] in ("ferret", "session"):
+            kind = "reference" if ref_ferret_available() else "port"
         if i >= args.warmup:
             vals.append(v)
     v = statistics.median(vals)
@@ -574,10 +724,11 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
         "config": {"workload": name, "what": CONFIG_TEXT[name]},
-        "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference CPU path: emp-ot/cryptoTools semantics restated in oracle/ (emp-tool is not "
-                "vendored, so emp-ot cannot be built); all host threads",
+        "note": "reference CPU path on all host threads: Ferret GGM/LPN by the reference's own emp-ot headers "
+                "(spcot_sender.h, spcot_recver.h, lpn_f2.h) compiled over an emp-tool shim into "
+                "oracle/_ref/libempref.so; SOT by the oracle's restatement (the reference has no CPU SOT code)",
     }), flush=True)
     return 0
 
@@ -777,12 +928,10 @@ def run_batch(args):
         out["served"] = run_served(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, sample = cpu_sample("sot_n20", threads, budget_s=5.0)
-        v2, sample2 = cpu_sample("ferret_b13", threads, budget_s=5.0)
-        # per-COT CPU cost of each kind, weighted by the mix
-        cpu_ms = (n_sot / v + n_fer / v2) * 1e3
-        out["cpu_baseline"] = {"value": cots / (cpu_ms / 1e3), "unit": "COTs/s", "cores": threads, "kind": "port",
-                               "sample": f"SOT: {sample}; Ferret: {sample2}; weighted by the mix's COTs"}
+        mix = CpuMix(spec, threads, seed=2024 + rank)
+        vals = [mix.time_step() for _ in range(3)]
+        out["cpu_baseline"] = {"value": statistics.median(vals), "unit": "COTs/s", "cores": threads,
+                               "kind": mix.kind, "sample": mix.sample + "; median of 3 passes"}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:
@@ -913,7 +1062,8 @@ def run_session(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample("ferret_b13", threads)
-        out["cpu_baseline"] = {"value": v * p.ot_limit / p.n, "unit": "COTs/s", "cores": threads, "kind": "port",
+        out["cpu_baseline"] = {"value": v * p.ot_limit / p.n, "unit": "COTs/s", "cores": threads,
+                               "kind": "reference" if ref_ferret_available() else "port",
                                "sample": sample + "; scaled by ot_limit / n"}
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -1070,7 +1220,9 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample(args.workload, threads)
-        out["cpu_baseline"] = {"value": v, "unit": "COTs/s", "cores": threads, "kind": "port", "sample": sample}
+        ref = inst.spec["kind"] == "ferret" and inst.spec["d"] == 10 and ref_ferret_available()
+        out["cpu_baseline"] = {"value": v, "unit": "COTs/s", "cores": threads,
+                               "kind": "reference" if ref else "port", "sample": sample}
     if rank == 0:
         print(json.dumps(out), flush=True)
     del inst

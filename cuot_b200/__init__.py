@@ -134,9 +134,17 @@ class Context:
         return int(self.lib.cuot_ctx_scratch_bytes(self.h))
 
     TUNE_PPRF_THREADS, TUNE_QC_PLANES, TUNE_QC_BACKEND, TUNE_QC_STREAMS = 1, 2, 3, 4
+    TUNE_QC_RECORD_MARGIN = 5
 
     def set_tuning(self, key: int, value: int):
         _check(self.lib.cuot_ctx_set_tuning(self.h, C.c_int(key), C.c_int64(value)), "cuot_ctx_set_tuning")
+
+    def qc_fft_margin(self, reset: bool = True) -> float:
+        """Largest |v - round(v)| rounded by this context's fp64 FFT encodes
+        since recording was switched on (TUNE_QC_RECORD_MARGIN) or last reset."""
+        v = C.c_double()
+        _check(self.lib.cuot_qc_fft_margin(self.h, C.byref(v), C.c_int(int(reset))), "cuot_qc_fft_margin")
+        return v.value
 
     # ---- AES ---------------------------------------------------------------
     def aes128_ecb(self, key, io, stream=None):
@@ -173,6 +181,16 @@ class Context:
         _check(self.lib.cuot_lpn_primal(self.h, _host_block(seed), _ptr(kk), C.c_int64(_nblocks(kk)),
                                         C.c_int(d), _ptr(e_io), C.c_int64(_nblocks(e_io)), _stream(stream)),
                "cuot_lpn_primal")
+
+    def lpn_primal_dual(self, seed, kk_send, kk_recv, e_send, e_recv, d: int = 10, stream=None):
+        """Both roles' LPN of one extension (same seed) in one launch: the
+        public index matrix is generated once for the two."""
+        n = _nblocks(e_send)
+        if _nblocks(e_recv) != n or _nblocks(kk_recv) != _nblocks(kk_send):
+            raise ValueError("the two roles need equal row and kk counts")
+        _check(self.lib.cuot_lpn_primal_dual(self.h, _host_block(seed), _ptr(kk_send), _ptr(kk_recv),
+                                             C.c_int64(_nblocks(kk_send)), C.c_int(d), _ptr(e_send), _ptr(e_recv),
+                                             C.c_int64(n), _stream(stream)), "cuot_lpn_primal_dual")
 
     def lpn_primal_range(self, seed, kk, e_rows, row_lo: int, row_hi: int, n: int, d: int = 10, stream=None):
         _check(self.lib.cuot_lpn_primal_range(self.h, _host_block(seed), _ptr(kk), C.c_int64(_nblocks(kk)),

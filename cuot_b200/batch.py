@@ -29,7 +29,7 @@ class BatchItem(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("pprf_threads", C.c_int), ("ctas_per_sm", C.c_int), ("lpn_rows_per_task", C.c_int),
-                ("qc_planes_per_pass", C.c_int), ("use_graph", C.c_int)]
+                ("qc_planes_per_pass", C.c_int), ("use_graph", C.c_int), ("serial", C.c_int)]
 
 
 class Instance:
@@ -97,10 +97,11 @@ class Instance:
 
 class Batch:
     def __init__(self, ctx, instances, pprf_threads: int = 0, ctas_per_sm: int = 0, lpn_rows_per_task: int = 0,
-                 qc_planes_per_pass: int = 0, use_graph: bool = True):
+                 qc_planes_per_pass: int = 0, use_graph: bool = True, serial: bool = False):
         self.lib, self.ctx, self.instances = load(), ctx, list(instances)
         arr = (BatchItem * len(self.instances))(*[i.item() for i in self.instances])
-        cfg = BatchConfig(pprf_threads, ctas_per_sm, lpn_rows_per_task, qc_planes_per_pass, int(use_graph))
+        cfg = BatchConfig(pprf_threads, ctas_per_sm, lpn_rows_per_task, qc_planes_per_pass, int(use_graph),
+                          int(serial))
         h = C.c_void_p()
         _check(self.lib.cuot_batch_create(ctx.h, arr, C.c_int(len(self.instances)), C.byref(cfg), C.byref(h)),
                "cuot_batch_create")
@@ -134,10 +135,11 @@ class Batch:
             pass
 
 
-def mixed_workload(ctx, count: int = 64, seed: int = 2024, lo: int = 16, hi: int = 22):
-    """The mixed batch: `count` instances, half SOT and half
-    Ferret-style, log2(n) uniform over [lo, hi], depth in [10, 14] with t =
-    n / 2^h; Ferret k = ceil(n * 452000 / 10485760) (ferret_b13's ratio)."""
+def mixed_shapes(count: int = 64, seed: int = 2024, lo: int = 16, hi: int = 22):
+    """Shapes of the mixed batch: `count` (kind, t, h, k) tuples, half SOT
+    and half Ferret-style, log2(n) uniform over [lo, hi], depth in [10, 14]
+    with t = n / 2^h; Ferret k = ceil(n * 452000 / 10485760) (ferret_b13's
+    ratio).  Needs no device."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -146,5 +148,12 @@ def mixed_workload(ctx, count: int = 64, seed: int = 2024, lo: int = 16, hi: int
         h = int(rng.integers(10, min(14, e) + 1))
         t = (1 << e) >> h
         k = -(-(1 << e) * 452000 // 10485760) if kind == KIND_FERRET else 0
-        out.append(Instance(ctx, kind, t, h, seed * 1000 + i, k=k))
+        out.append((kind, t, h, k))
     return out
+
+
+def mixed_workload(ctx, count: int = 64, seed: int = 2024, lo: int = 16, hi: int = 22):
+    """The mixed batch of `mixed_shapes`, each instance seeded with
+    seed * 1000 + its index, with device buffers."""
+    return [Instance(ctx, kind, t, h, seed * 1000 + i, k=k)
+            for i, (kind, t, h, k) in enumerate(mixed_shapes(count, seed, lo, hi))]

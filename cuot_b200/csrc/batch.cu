@@ -1,23 +1,30 @@
 // batch.cu -- the batched engine: many OT-extension instances (Ferret and
 // SOT, uneven n and depth, both roles) as one device program.
 //
-//   1. persistent PPRF launch over every sender tree of every instance: each
-//      CTA pulls (instance, tree) tasks from an atomic work counter, deepest
-//      trees first, and expands one whole tree per task (pprf_tree), with a
-//      per-CTA scratch slot for the level ping-pong;
-//   2. one launch selecting the Ferret receivers' OT messages (ideal OT of
-//      the sender's level sums, as emp-ot's OTIdeal, ideal.h:7-31);
-//   3. the same persistent PPRF launch over every receiver tree;
-//   4. persistent LPN launch over chunks of rows of every Ferret instance,
-//      both roles (key schedule and arguments staged in shared memory per
-//      task);
-//   5. per SOT transform size: block->plane transposes, NTT passes that span
-//      the planes of every instance of that size (each with its own `a`),
-//      plane->block transposes, and the receivers' choice-bit encodes.
+// Two independent branches, forked from the caller's stream and joined back:
+//   Ferret branch: a persistent PPRF launch over every Ferret sender tree
+//     (each CTA pulls (instance, tree) tasks from an atomic work counter,
+//     deepest trees first, and expands one whole tree per task with
+//     pprf_tree, in a per-CTA scratch slot for the level ping-pong); one
+//     launch selecting the receivers' OT messages (ideal OT of the sender's
+//     level sums, as emp-ot's OTIdeal, ideal.h:7-31); the same persistent
+//     launch over the receiver trees; one persistent LPN launch over chunks
+//     of rows of every instance, both roles of a row from one index
+//     computation (the two roles share the public LPN seed).
+//   SOT branch: the persistent PPRF launches over the SOT sender and then
+//     receiver trees; then each transform size on its own stream (sizes that
+//     share per-size FFT state, qc_lane, on one): blocks into the encode's
+//     layout, transform passes that span every instance of that size (each
+//     with its own A_hat), back to blocks, and the receivers' choice-bit
+//     encodes.
+// Independent work thus shares the GPU: the Ferret chain and the small
+// sizes' passes fill the SMs that the large sizes' passes leave idle.
+// cfg.serial runs the same launches as one chain on the caller's stream.
 // The whole program is captured into a CUDA graph on the first run.
 // Spin-free: work queues are atomic counters, reset by a memset node.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -112,10 +119,15 @@ __global__ void __launch_bounds__(kLpnThreads, 3) lpn_batch_kernel(LpnBatchArgs 
       reinterpret_cast<uint32_t *>(&s_job)[i] = src[i];
     __syncthreads();
     const LpnArgs &a = s_job;
+    const bool dual = a.kk2 != nullptr;
     for (int64_t w = tk.w0 + threadIdx.x; w < tk.w1; w += blockDim.x) {
       if (w < a.ngroups) {
-        if (a.d == 10) lpn_group4<10>(a, T, a.g0 + w);
-        else lpn_group4_dyn(a, T, a.g0 + w);
+        if (a.d == 10) {
+          if (dual) lpn_group4<10, true>(a, T, a.g0 + w);
+          else lpn_group4<10>(a, T, a.g0 + w);
+        } else {
+          lpn_group4_dyn(a, T, a.g0 + w);
+        }
       } else {
         lpn_row1(a, T, a.j0 + (w - a.ngroups));
       }
@@ -146,11 +158,19 @@ int batch_setup_device() {
 
 struct SotClass {
   int e;
-  int batch = 1;                  // planes per NTT pass for this size (Y holds batch * 4n bytes)
+  int batch = 1;                  // planes per transform pass group of this size
   std::vector<int> items;         // item indices of this size
   uint8_t *planes = nullptr;      // 2 * items * 16n bytes (jobs: item x role)
+  void *Y = nullptr;              // this size's intermediate: qc_y_bytes(batch)
   std::vector<const void *> ahats;  // per job
 };
+
+// PPRF branches of the program.
+enum { kBrFerret = 0, kBrSot = 1 };
+// Work counters: PPRF sender and receiver per branch, LPN.
+constexpr int kCounters = 5;
+// Events: fork, Ferret branch done, SOT PPRF done, then one per lane.
+constexpr int kEvFork = 0, kEvFerret = 1, kEvSotPprf = 2, kEvLane0 = 3;
 
 }  // namespace
 }  // namespace cuot
@@ -162,25 +182,29 @@ struct cuot_batch {
   std::vector<cuot_batch_item> items;
   cuot_batch_config cfg{};
   std::vector<void *> allocs;  // every device allocation owned by the batch
-  // PPRF
-  PprfBatchArgs send{}, recv{};
-  int pprf_grid = 0;
+  // PPRF per branch (kBrFerret, kBrSot)
+  PprfBatchArgs send[2]{}, recv[2]{};
+  int pprf_grid[2] = {0, 0};
   int pprf_threads = 256;
   // Ferret selection
   SelItem *sel_d = nullptr;
   int nsel = 0;
   uint64_t sel_max = 0;
-  // LPN
+  // LPN: one job per Ferret instance, both roles
   LpnBatchArgs lpn{};
   int lpn_grid = 0;
-  unsigned int *counters = nullptr;  // [3]
-  // SOT
+  unsigned int *counters = nullptr;  // [kCounters]
+  // SOT: sizes, largest first, grouped into lanes (qc_lane) that run side by side
   std::vector<SotClass> classes;
-  void *Y = nullptr;  // QC intermediate, max over classes of qc_y_bytes(batch)
-  std::vector<void *> item_ahat;      // per item (SOT), nullptr otherwise
-  std::vector<cuot_qc_plan *> plans;  // plain path, per item (SOT)
+  std::vector<std::vector<int>> lanes;  // class indices per lane, in order
+  std::vector<void *> item_ahat;        // per item (SOT), nullptr otherwise
+  std::vector<cuot_qc_plan *> plans;    // plain path, per item (SOT)
   // Ferret per-item sums (batch-owned)
   std::vector<Blk *> lsum, rsum, ss, mc, m0, m1;
+  // concurrent schedule: streams[0] for the Ferret branch, streams[j] for
+  // lane j >= 1 (lane 0 runs on the caller's stream)
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
   int kernels_per_run = 0;  // kernels one batched run launches
   // graph
   cudaGraph_t graph = nullptr;
@@ -221,6 +245,7 @@ int check_item(const cuot_batch_item &it, int i) {
   if (it.kind == CUOT_KIND_FERRET) {
     if (it.k < 1 || it.k > 0x7fffffffll || it.d < 1 || it.d > 32 || !it.kk_send_d || !it.kk_recv_d)
       return fail(CUOT_EINVAL, "item %d: bad LPN arguments", i);
+    if (it.v_d == it.w_d) return fail(CUOT_EINVAL, "item %d: v and w must not alias", i);
   } else {
     if (n < 1024 || n > (1ull << 25) || (n & (n - 1)))
       return fail(CUOT_EINVAL, "item %d: SOT n=%llu must be a power of two in [2^10, 2^25]", i,
@@ -231,12 +256,16 @@ int check_item(const cuot_batch_item &it, int i) {
   return CUOT_OK;
 }
 
-LpnArgs make_lpn_job(const cuot_batch_item &it, Blk *e, const cuot_block *kk, const uint32_t *t0) {
+// The LPN of both roles of a Ferret item: rows v with kk_send, rows w with
+// kk_recv, one index matrix (the item's seed).
+LpnArgs make_lpn_job(const cuot_batch_item &it, const uint32_t *t0) {
   LpnArgs a{};
   host_aes_key_expand(it.lpn_seed, &a.key);
   a.t0 = t0;
-  a.kk = reinterpret_cast<const Blk *>(kk);
-  a.e = e;
+  a.kk = reinterpret_cast<const Blk *>(it.kk_send_d);
+  a.e = reinterpret_cast<Blk *>(it.v_d);
+  a.kk2 = reinterpret_cast<const Blk *>(it.kk_recv_d);
+  a.e2 = reinterpret_cast<Blk *>(it.w_d);
   const int64_t n = int64_t(it.t << it.h);
   a.n = n;
   a.k = it.k;
@@ -254,50 +283,37 @@ LpnArgs make_lpn_job(const cuot_batch_item &it, Blk *e, const cuot_block *kk, co
   return a;
 }
 
-// Enqueues the batched program on `st`.  ev (optional): 5 events recorded
-// before the sender PPRF, the receiver PPRF, the LPN, the SOT encodes, and
-// at the end.
-int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
+int pprf_launch(cuot_batch *b, const PprfBatchArgs &args, int br, cudaStream_t st) {
+  if (!args.ntasks) return 0;
+  pprf_batch_kernel<<<b->pprf_grid[br], b->pprf_threads, kTableBytes, st>>>(args);
+  return 1;
+}
+
+int select_launch(cuot_batch *b, cudaStream_t st) {
+  if (!b->nsel) return 0;
+  const unsigned gx = unsigned(std::min<uint64_t>((b->sel_max + 255) / 256, 1024));
+  ferret_select_kernel<<<dim3(gx, b->nsel), 256, 0, st>>>(b->sel_d);
+  return 1;
+}
+
+int lpn_launch(cuot_batch *b, cudaStream_t st) {
+  if (!b->lpn.ntasks) return 0;
+  lpn_batch_kernel<<<b->lpn_grid, kLpnThreads, kTableBytes, st>>>(b->lpn);
+  return 1;
+}
+
+// The SOT sizes of one lane, in order, on `st`.
+int enqueue_lane(cuot_batch *b, const std::vector<int> &lane, cudaStream_t st) {
   cuot_ctx *ctx = b->ctx;
-  const unsigned long long k0 = cuot_launch_count();
-  auto mark = [&](int i) {
-    if (ev) cudaEventRecord(ev[i], st);
-  };
-  if (cudaMemsetAsync(b->counters, 0, 3 * sizeof(unsigned int), st) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(CUOT_ECUDA, "counter reset failed");
-  }
-  int launches = 0;
-  mark(0);
-  if (b->send.ntasks) {
-    pprf_batch_kernel<<<b->pprf_grid, b->pprf_threads, kTableBytes, st>>>(b->send);
-    launches++;
-  }
-  if (b->nsel) {
-    unsigned gx = unsigned(std::min<uint64_t>((b->sel_max + 255) / 256, 1024));
-    ferret_select_kernel<<<dim3(gx, b->nsel), 256, 0, st>>>(b->sel_d);
-    launches++;
-  }
-  mark(1);
-  if (b->recv.ntasks) {
-    pprf_batch_kernel<<<b->pprf_grid, b->pprf_threads, kTableBytes, st>>>(b->recv);
-    launches++;
-  }
-  mark(2);
-  if (b->lpn.ntasks) {
-    lpn_batch_kernel<<<b->lpn_grid, kLpnThreads, kTableBytes, st>>>(b->lpn);
-    launches++;
-  }
-  CUOT_TRY(launch_status(launches));
-  mark(3);
-  for (auto &c : b->classes) {
+  for (int ci : lane) {
+    SotClass &c = b->classes[ci];
     const uint64_t n = 1ull << c.e;
     const int njobs = int(c.items.size()) * 2;
     for (int j = 0; j < njobs; j++) {
       const cuot_batch_item &it = b->items[c.items[j / 2]];
       CUOT_TRY(qc_job_to_layout(ctx, c.e, j % 2 ? it.w_d : it.v_d, c.planes + uint64_t(j) * n * 16, st));
     }
-    CUOT_TRY(qc_encode_jobs(ctx, c.e, reinterpret_cast<uint64_t *>(c.planes), njobs, c.ahats.data(), b->Y,
+    CUOT_TRY(qc_encode_jobs(ctx, c.e, reinterpret_cast<uint64_t *>(c.planes), njobs, c.ahats.data(), c.Y,
                             c.batch, st));
     for (int j = 0; j < njobs; j++) {
       const cuot_batch_item &it = b->items[c.items[j / 2]];
@@ -308,7 +324,71 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
       CUOT_TRY(cuot_qc_encode_sparse(ctx, it.a_d, it.punct_d, int(it.t), n, it.cbits_d, st));
     }
   }
-  mark(4);
+  return CUOT_OK;
+}
+
+int ev_fail() {
+  cudaGetLastError();
+  return fail(CUOT_ECUDA, "batch stream fork / join failed");
+}
+
+// Enqueues the batched program on `st`.  ev (optional, diagnostic): 5 events
+// recorded before the sender PPRF, the receiver PPRF, the LPN, the SOT
+// encodes, and at the end; with ev the program runs as one chain (phases in
+// order), as it does with cfg.serial.
+int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
+  const unsigned long long k0 = cuot_launch_count();
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], st);
+  };
+  if (cudaMemsetAsync(b->counters, 0, kCounters * sizeof(unsigned int), st) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "counter reset failed");
+  }
+  if (ev || b->cfg.serial) {
+    int launches = 0;
+    mark(0);
+    launches += pprf_launch(b, b->send[kBrSot], kBrSot, st);
+    launches += pprf_launch(b, b->send[kBrFerret], kBrFerret, st);
+    launches += select_launch(b, st);
+    mark(1);
+    launches += pprf_launch(b, b->recv[kBrSot], kBrSot, st);
+    launches += pprf_launch(b, b->recv[kBrFerret], kBrFerret, st);
+    mark(2);
+    launches += lpn_launch(b, st);
+    CUOT_TRY(launch_status(launches));
+    mark(3);
+    for (const auto &lane : b->lanes) CUOT_TRY(enqueue_lane(b, lane, st));
+    mark(4);
+  } else {
+    cudaEvent_t *E = b->events.data();
+    if (cudaEventRecord(E[kEvFork], st) != cudaSuccess) return ev_fail();
+    const bool fer = b->send[kBrFerret].ntasks > 0;
+    if (fer) {  // Ferret branch on streams[0]
+      cudaStream_t sf = b->streams[0];
+      if (cudaStreamWaitEvent(sf, E[kEvFork], 0) != cudaSuccess) return ev_fail();
+      int launches = pprf_launch(b, b->send[kBrFerret], kBrFerret, sf);
+      launches += select_launch(b, sf);
+      launches += pprf_launch(b, b->recv[kBrFerret], kBrFerret, sf);
+      launches += lpn_launch(b, sf);
+      CUOT_TRY(launch_status(launches));
+      if (cudaEventRecord(E[kEvFerret], sf) != cudaSuccess) return ev_fail();
+    }
+    // SOT branch: PPRFs on the caller's stream, then the lanes side by side
+    CUOT_TRY(launch_status(pprf_launch(b, b->send[kBrSot], kBrSot, st) +
+                           pprf_launch(b, b->recv[kBrSot], kBrSot, st)));
+    if (cudaEventRecord(E[kEvSotPprf], st) != cudaSuccess) return ev_fail();
+    for (size_t j = 1; j < b->lanes.size(); j++) {
+      cudaStream_t sl = b->streams[j];
+      if (cudaStreamWaitEvent(sl, E[kEvSotPprf], 0) != cudaSuccess) return ev_fail();
+      CUOT_TRY(enqueue_lane(b, b->lanes[j], sl));
+      if (cudaEventRecord(E[kEvLane0 + j], sl) != cudaSuccess) return ev_fail();
+    }
+    if (!b->lanes.empty()) CUOT_TRY(enqueue_lane(b, b->lanes[0], st));
+    if (fer && cudaStreamWaitEvent(st, E[kEvFerret], 0) != cudaSuccess) return ev_fail();
+    for (size_t j = 1; j < b->lanes.size(); j++)
+      if (cudaStreamWaitEvent(st, E[kEvLane0 + j], 0) != cudaSuccess) return ev_fail();
+  }
   b->kernels_per_run = int(cuot_launch_count() - k0);
   return CUOT_OK;
 }
@@ -348,12 +428,13 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
   std::vector<PprfArgs> sargs(count), rargs(count);
   std::vector<int> smodes(count), rmodes(count);
   std::vector<SelItem> sel;
-  int hmax = 1;
+  int hmax[2] = {1, 1};
   for (int i = 0; i < count; i++) {
     const cuot_batch_item &it = items[i];
     const uint64_t t = it.t;
     const int h = it.h;
-    hmax = std::max(hmax, h);
+    const int br = it.kind == CUOT_KIND_FERRET ? kBrFerret : kBrSot;
+    hmax[br] = std::max(hmax[br], h);
     PprfArgs s{}, r{};
     s.t = r.t = t;
     s.h = r.h = h;
@@ -385,55 +466,57 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
     sargs[i] = s;
     rargs[i] = r;
   }
-  // ---- PPRF tasks: every tree, deepest first
-  std::vector<PprfTask> tasks;
+  PprfArgs *sd = nullptr, *rd = nullptr;
+  int *smd = nullptr, *rmd = nullptr;
+  if ((st = upload(b, &sd, sargs)) || (st = upload(b, &rd, rargs)) || (st = upload(b, &smd, smodes)) ||
+      (st = upload(b, &rmd, rmodes)) || (st = balloc(b, &b->counters, kCounters * sizeof(unsigned int))))
+    return cleanup(st);
+  // ---- PPRF tasks per branch: every tree, deepest first; each branch has
+  // its own per-CTA scratch slots (the branches run at the same time)
   std::vector<int> order(count);
   for (int i = 0; i < count; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return items[x].h > items[y].h; });
-  for (int i : order)
-    for (uint64_t tr = 0; tr < items[i].t; tr++) tasks.push_back(PprfTask{uint32_t(i), uint32_t(tr)});
-  const uint64_t ntasks = tasks.size();
-  b->pprf_grid = int(std::min<uint64_t>(uint64_t(sms) * per_sm, ntasks));
-  PprfArgs *sd = nullptr, *rd = nullptr;
-  int *smd = nullptr, *rmd = nullptr;
-  PprfTask *td = nullptr;
-  Blk *pscr = nullptr;
-  if ((st = upload(b, &sd, sargs)) || (st = upload(b, &rd, rargs)) || (st = upload(b, &smd, smodes)) ||
-      (st = upload(b, &rmd, rmodes)) || (st = upload(b, &td, tasks)) ||
-      (st = balloc(b, &pscr, (uint64_t(b->pprf_grid) << hmax) * 16)) ||
-      (st = balloc(b, &b->counters, 4 * sizeof(unsigned int))))
-    return cleanup(st);
-  b->send = PprfBatchArgs{sd, smd, td, uint32_t(ntasks), b->counters + 0, pscr, hmax, ctx->t0_d};
-  b->recv = PprfBatchArgs{rd, rmd, td, uint32_t(ntasks), b->counters + 1, pscr, hmax, ctx->t0_d};
+  for (int br = 0; br < 2; br++) {
+    std::vector<PprfTask> tasks;
+    for (int i : order)
+      if ((items[i].kind == CUOT_KIND_FERRET) == (br == kBrFerret))
+        for (uint64_t tr = 0; tr < items[i].t; tr++) tasks.push_back(PprfTask{uint32_t(i), uint32_t(tr)});
+    if (tasks.empty()) continue;
+    b->pprf_grid[br] = int(std::min<uint64_t>(uint64_t(sms) * per_sm, tasks.size()));
+    PprfTask *td = nullptr;
+    Blk *pscr = nullptr;
+    if ((st = upload(b, &td, tasks)) || (st = balloc(b, &pscr, (uint64_t(b->pprf_grid[br]) << hmax[br]) * 16)))
+      return cleanup(st);
+    b->send[br] = PprfBatchArgs{sd, smd, td, uint32_t(tasks.size()), b->counters + 2 * br, pscr, hmax[br],
+                                ctx->t0_d};
+    b->recv[br] = PprfBatchArgs{rd, rmd, td, uint32_t(tasks.size()), b->counters + 2 * br + 1, pscr, hmax[br],
+                                ctx->t0_d};
+  }
   b->nsel = int(sel.size());
   if (b->nsel && (st = upload(b, &b->sel_d, sel))) return cleanup(st);
 
-  // ---- LPN jobs and tasks (both roles of every Ferret item)
+  // ---- LPN: one job per Ferret item (both roles), tasks of rows_per_task rows
   const int64_t rows_per_task = b->cfg.lpn_rows_per_task > 0 ? (b->cfg.lpn_rows_per_task + 3) / 4 * 4 : 65536;
   std::vector<LpnArgs> jobs;
   std::vector<LpnTask> ltasks;
   for (int i = 0; i < count; i++) {
     const cuot_batch_item &it = items[i];
     if (it.kind != CUOT_KIND_FERRET) continue;
-    for (int role = 0; role < 2; role++) {
-      LpnArgs a = make_lpn_job(it, reinterpret_cast<Blk *>(role ? it.w_d : it.v_d),
-                               role ? it.kk_recv_d : it.kk_send_d, ctx->t0_d);
-      const uint32_t j = uint32_t(jobs.size());
-      jobs.push_back(a);
-      const int64_t total = a.ngroups + a.ntail, chunk = rows_per_task / 4;
-      for (int64_t w0 = 0; w0 < total; w0 += chunk) ltasks.push_back(LpnTask{j, 0, w0, std::min(total, w0 + chunk)});
-    }
+    const LpnArgs a = make_lpn_job(it, ctx->t0_d);
+    const uint32_t j = uint32_t(jobs.size());
+    jobs.push_back(a);
+    const int64_t total = a.ngroups + a.ntail, chunk = rows_per_task / 4;
+    for (int64_t w0 = 0; w0 < total; w0 += chunk) ltasks.push_back(LpnTask{j, 0, w0, std::min(total, w0 + chunk)});
   }
   if (!jobs.empty()) {
     LpnArgs *jd = nullptr;
     LpnTask *ltd = nullptr;
     if ((st = upload(b, &jd, jobs)) || (st = upload(b, &ltd, ltasks))) return cleanup(st);
-    b->lpn = LpnBatchArgs{jd, ltd, uint32_t(ltasks.size()), b->counters + 2, ctx->t0_d};
+    b->lpn = LpnBatchArgs{jd, ltd, uint32_t(ltasks.size()), b->counters + 4, ctx->t0_d};
     b->lpn_grid = int(std::min<uint64_t>(uint64_t(sms) * per_sm, ltasks.size()));
   }
 
-  // ---- SOT size classes, transforms of every `a`
-  uint64_t ybytes = 0;
+  // ---- SOT size classes (largest first), their lanes, transforms of every `a`
   for (int i = 0; i < count; i++) {
     const cuot_batch_item &it = items[i];
     if (it.kind != CUOT_KIND_SOT) continue;
@@ -446,28 +529,52 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
     }
     c->items.push_back(i);
   }
-  for (auto &c : b->classes) {
+  std::stable_sort(b->classes.begin(), b->classes.end(),
+                   [](const SotClass &x, const SotClass &y) { return x.e > y.e; });
+  std::map<int, int> lane_of;  // qc_lane -> index into b->lanes
+  for (size_t ci = 0; ci < b->classes.size(); ci++) {
+    SotClass &c = b->classes[ci];
     const uint64_t n = 1ull << c.e;
     if ((st = qc_prepare(ctx, c.e))) return cleanup(st);
     if ((st = balloc(b, &c.planes, 2 * c.items.size() * n * 16))) return cleanup(st);
     int pb = b->cfg.qc_planes_per_pass > 0 ? b->cfg.qc_planes_per_pass
                                            : qc_default_batch(n, int(256 * c.items.size()));
     pb = std::min(pb, int(256 * c.items.size()));
-    c.batch = pb;  // this class's passes use exactly the Y size reserved for them
-    ybytes = std::max(ybytes, qc_y_bytes(ctx, c.e, pb));
-  }
-  if (!b->classes.empty()) {
-    if ((st = balloc(b, &b->Y, ybytes))) return cleanup(st);
-    for (auto &c : b->classes) {
-      for (int i : c.items) {
-        const uint64_t n = 1ull << c.e;
-        if ((st = balloc(b, &b->item_ahat[i], qc_ahat_bytes(ctx, c.e)))) return cleanup(st);
-        if ((st = qc_build_ahat(ctx, c.e, items[i].a_d, b->Y, b->item_ahat[i], nullptr))) return cleanup(st);
-        c.ahats.push_back(b->item_ahat[i]);  // sender job
-        c.ahats.push_back(b->item_ahat[i]);  // receiver job
-        if ((st = cuot_qc_plan_create(ctx, items[i].a_d, n, nullptr, &b->plans[i]))) return cleanup(st);
-      }
+    c.batch = pb;
+    if ((st = balloc(b, &c.Y, qc_y_bytes(ctx, c.e, pb)))) return cleanup(st);
+    const int key = qc_lane(ctx, c.e);
+    auto l = lane_of.find(key);
+    if (l == lane_of.end()) {
+      lane_of[key] = int(b->lanes.size());
+      b->lanes.push_back({int(ci)});
+    } else {
+      b->lanes[l->second].push_back(int(ci));
     }
+    for (int i : c.items) {
+      if ((st = balloc(b, &b->item_ahat[i], qc_ahat_bytes(ctx, c.e)))) return cleanup(st);
+      if ((st = qc_build_ahat(ctx, c.e, items[i].a_d, c.Y, b->item_ahat[i], nullptr))) return cleanup(st);
+      c.ahats.push_back(b->item_ahat[i]);  // sender job
+      c.ahats.push_back(b->item_ahat[i]);  // receiver job
+      if ((st = cuot_qc_plan_create(ctx, items[i].a_d, n, nullptr, &b->plans[i]))) return cleanup(st);
+    }
+  }
+  // ---- streams and events of the concurrent schedule
+  const size_t nstreams = std::max<size_t>(1, b->lanes.size());
+  for (size_t j = 0; j < nstreams; j++) {
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return cleanup(fail(CUOT_ECUDA, "batch stream creation failed"));
+    }
+    b->streams.push_back(s);
+  }
+  for (size_t j = 0; j < kEvLane0 + b->lanes.size(); j++) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return cleanup(fail(CUOT_ECUDA, "batch event creation failed"));
+    }
+    b->events.push_back(e);
   }
   if (cudaDeviceSynchronize() != cudaSuccess) {
     cudaGetLastError();
@@ -532,8 +639,8 @@ int cuot_batch_run_plain(cuot_batch *b, void *stream) {
       CUOT_TRY(launch_status());
       CUOT_TRY(cuot_ferret_pprf_recver(ctx, reinterpret_cast<cuot_block *>(b->mc[i]), it.choice_d,
                                        reinterpret_cast<cuot_block *>(b->ss[i]), t, h, it.w_d, st));
-      CUOT_TRY(cuot_lpn_primal(ctx, it.lpn_seed, it.kk_send_d, it.k, it.d, it.v_d, int64_t(n), st));
-      CUOT_TRY(cuot_lpn_primal(ctx, it.lpn_seed, it.kk_recv_d, it.k, it.d, it.w_d, int64_t(n), st));
+      CUOT_TRY(cuot_lpn_primal_dual(ctx, it.lpn_seed, it.kk_send_d, it.kk_recv_d, it.k, it.d, it.v_d, it.w_d,
+                                    int64_t(n), st));
     } else {
       CUOT_TRY(cuot_sot_pprf_sender(ctx, it.roots_d, t, h, &it.delta, it.base0_d, it.base1_d, it.v_d,
                                     reinterpret_cast<cuot_block *>(b->m0[i]),
@@ -571,6 +678,9 @@ int cuot_batch_destroy(cuot_batch *b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     for (auto *p : b->plans)
       if (p) cuot_qc_plan_destroy(p);
+    for (auto s : b->streams) cudaStreamSynchronize(s);
+    for (auto s : b->streams) cudaStreamDestroy(s);
+    for (auto e : b->events) cudaEventDestroy(e);
     for (void *p : b->allocs) cudaFree(p);
   }
   delete b;

@@ -1,4 +1,5 @@
 // capi.cu -- context lifetime, status strings, error reporting, scratch.
+#include <cstring>
 #include <cstdarg>
 #include <cstdio>
 #include <atomic>
@@ -116,6 +117,7 @@ int cuot_ctx_destroy(cuot_ctx *c) {
   {
     DeviceGuard g(c);
     qc_free_ctx_tables(c);
+    if (c->qcf_margin) cudaFree(c->qcf_margin);
     if (c->scratch) cudaFree(c->scratch);
     if (c->t0_d) cudaFree(c->t0_d);
   }
@@ -131,6 +133,22 @@ int cuot_ctx_reserve(cuot_ctx *c, uint64_t bytes) {
 }
 
 uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *c) { return c ? c->scratch_bytes : 0; }
+
+int cuot_qc_fft_margin(cuot_ctx *c, double *out, int reset) {
+  if (!c || !out) return fail(CUOT_EINVAL, "null argument");
+  if (!c->qcf_margin) return fail(CUOT_EINVAL, "margin recording is off (CUOT_TUNE_QC_RECORD_MARGIN)");
+  DeviceGuard g(c);
+  uint32_t bits = 0;
+  if (cudaMemcpy(&bits, c->qcf_margin, sizeof(bits), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      (reset && cudaMemset(c->qcf_margin, 0, sizeof(bits)) != cudaSuccess)) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "margin read failed");
+  }
+  float f;
+  std::memcpy(&f, &bits, sizeof(f));
+  *out = double(f);
+  return CUOT_OK;
+}
 
 int cuot_ctx_set_tuning(cuot_ctx *c, int key, int64_t value) {
   if (!c) return fail(CUOT_EINVAL, "ctx is null");
@@ -151,6 +169,27 @@ int cuot_ctx_set_tuning(cuot_ctx *c, int key, int64_t value) {
       if (value != 1 && value != 2) return fail(CUOT_EINVAL, "QC streams must be 1 or 2");
       c->qc_streams = int(value);
       return CUOT_OK;
+    case CUOT_TUNE_QC_RECORD_MARGIN: {
+      if (value != 0 && value != 1) return fail(CUOT_EINVAL, "QC margin recording must be 0 or 1");
+      DeviceGuard g(c);
+      if (value == 0) {
+        if (c->qcf_margin) cudaFree(c->qcf_margin);
+        c->qcf_margin = nullptr;
+        return CUOT_OK;
+      }
+      if (!c->qcf_margin) {
+        if (cudaMalloc(&c->qcf_margin, sizeof(uint32_t)) != cudaSuccess) {
+          cudaGetLastError();
+          c->qcf_margin = nullptr;
+          return fail(CUOT_ENOMEM, "margin word allocation failed");
+        }
+      }
+      if (cudaMemset(c->qcf_margin, 0, sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CUOT_ECUDA, "margin word reset failed");
+      }
+      return CUOT_OK;
+    }
     default:
       return fail(CUOT_EINVAL, "unknown tuning key %d", key);
   }

@@ -13,6 +13,7 @@ struct cuot_ctx {
   int qc_planes_per_pass;  // 0: automatic
   int qc_backend;          // CUOT_TUNE_QC_BACKEND value: 0 automatic, 1 NTT, 2 FFT
   int qc_streams;          // CUOT_TUNE_QC_STREAMS value: 1 or 2 (FFT group schedule)
+  uint32_t *qcf_margin;    // CUOT_TUNE_QC_RECORD_MARGIN: device word, max |v - round(v)| as float bits
 };
 
 namespace cuot {
@@ -46,6 +47,10 @@ uint64_t qc_one_shot_dual_bytes(const cuot_ctx *ctx, int e, bool r2);
 // and intermediate sizes depend on it.
 int qc_prepare(cuot_ctx *ctx, int e);
 uint64_t qc_ahat_bytes(const cuot_ctx *ctx, int e);
+// Encodes of two sizes with the same lane share per-size FFT state (the
+// tables' second stream, events and plane-parity words) and must not run at
+// the same time; different lanes may.
+int qc_lane(const cuot_ctx *ctx, int e);
 uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch);
 int qc_build_ahat(cuot_ctx *ctx, int e, const uint64_t *a_d, void *Y, void *ahat, cudaStream_t st);
 int qc_encode_jobs(cuot_ctx *ctx, int e, uint64_t *planes, int njobs, const void *const *ahats,
@@ -65,6 +70,10 @@ struct QcfAhatTab {
   const void *p[16];
   int first;
   int per;
+  // When non-null (the context records rounding margins), the last inverse
+  // pass atomically raises *margin to the largest |v - round(v)| it rounds,
+  // as the bit pattern of a non-negative float.
+  uint32_t *margin;
 };
 struct QcfTables;
 bool qcf_supported(int e);

@@ -107,8 +107,8 @@ int extend_once(cuot_ferret_session *s, int64_t t, int h, int64_t k, const cuot_
   CUOT_TRY(launch_status());
   CUOT_TRY(cuot_ferret_pprf_recver(s->ctx, s->mc, s->choice, s->ss, uint64_t(t), h, out_r, s->st));
   const uint8_t *ls = reinterpret_cast<const uint8_t *>(&lpn_seed);
-  CUOT_TRY(cuot_lpn_primal(s->ctx, ls, kk_s, k, s->d, out_s, t << h, s->st));
-  CUOT_TRY(cuot_lpn_primal(s->ctx, ls, kk_r, k, s->d, out_r, t << h, s->st));
+  // both parties' LpnF2::compute with the seed ALICE sent BOB, in one launch
+  CUOT_TRY(cuot_lpn_primal_dual(s->ctx, ls, kk_s, kk_r, k, s->d, out_s, out_r, t << h, s->st));
   s->extensions++;
   return CUOT_OK;
 }

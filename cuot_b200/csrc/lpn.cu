@@ -14,7 +14,8 @@
 
 namespace cuot {
 
-template <int D>
+// D = 0: any d (a.d); D > 0: d = D.  DUAL: both roles (a.kk2 / a.e2 set).
+template <int D, bool DUAL>
 __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(LpnArgs a) {
   extern __shared__ __align__(16) uint32_t smem_tab[];
   stage_table(smem_tab, a.t0);
@@ -24,7 +25,7 @@ __global__ void __launch_bounds__(kLpnThreads) lpn_kernel(LpnArgs a) {
   for (int64_t w = int64_t(blockIdx.x) * kLpnThreads + threadIdx.x; w < total;
        w += int64_t(gridDim.x) * kLpnThreads) {
     if (w < a.ngroups) {
-      if (D > 0) lpn_group4<(D > 0 ? D : 1)>(a, T, a.g0 + w);
+      if (D > 0) lpn_group4<(D > 0 ? D : 1), DUAL>(a, T, a.g0 + w);
       else lpn_group4_dyn(a, T, a.g0 + w);
     } else {
       lpn_row1(a, T, a.j0 + (w - a.ngroups));
@@ -78,16 +79,20 @@ static int set_smem(F fn) {
   return CUOT_OK;
 }
 
-}  // namespace cuot
+template <int D, bool DUAL>
+int launch_lpn(cuot_ctx *ctx, const LpnArgs &a, cudaStream_t st) {
+  CUOT_TRY(set_smem(lpn_kernel<D, DUAL>));
+  int grid = 1;
+  grid_for(ctx, (const void *)lpn_kernel<D, DUAL>, a.ngroups + a.ntail, &grid);
+  lpn_kernel<D, DUAL><<<grid, kLpnThreads, kTableBytes, st>>>(a);
+  return launch_status();
+}
 
-using namespace cuot;
-
-extern "C" {
-
-int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
-                          int64_t k, int d, cuot_block *e_rows_d, int64_t row_lo, int64_t row_hi,
-                          int64_t n, void *stream) {
-  if (!ctx || !seed || !kk_d || !e_rows_d) return fail(CUOT_EINVAL, "null argument");
+// Rows [row_lo, row_hi) of one task over [0, n) (lpn_f2.h:72-79), for one
+// role (kk2 == e2 == nullptr) or for both roles of one extension.
+int lpn_rows(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d, const cuot_block *kk2_d,
+             int64_t k, int d, cuot_block *e_rows_d, cuot_block *e2_rows_d, int64_t row_lo, int64_t row_hi,
+             int64_t n, void *stream) {
   if (k < 1 || k > 0x7fffffffll) return fail(CUOT_EINVAL, "k=%lld out of range", (long long)k);
   if (d < 1 || d > 32) return fail(CUOT_EINVAL, "d=%d out of range [1,32]", d);
   if (n < 0 || row_lo < 0 || row_hi < row_lo || row_hi > n)
@@ -102,6 +107,8 @@ int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16], const cuot_bloc
   a.t0 = ctx->t0_d;
   a.kk = reinterpret_cast<const Blk *>(kk_d);
   a.e = reinterpret_cast<Blk *>(e_rows_d);
+  a.kk2 = reinterpret_cast<const Blk *>(kk2_d);
+  a.e2 = reinterpret_cast<Blk *>(e2_rows_d);
   a.n = n; a.k = k; a.d = d; a.row_lo = row_lo;
   uint32_t mask = 1;
   while (int64_t(mask) < k) mask = (mask << 1) | 1u;  // lpn_f2.h:27-31
@@ -115,17 +122,31 @@ int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16], const cuot_bloc
   a.j0 = row_lo > tail ? row_lo : tail;
   a.ntail = row_hi > a.j0 ? row_hi - a.j0 : 0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int grid = 1;
-  if (d == 10) {
-    CUOT_TRY(set_smem(lpn_kernel<10>));
-    grid_for(ctx, (const void *)lpn_kernel<10>, a.ngroups + a.ntail, &grid);
-    lpn_kernel<10><<<grid, kLpnThreads, kTableBytes, st>>>(a);
-  } else {
-    CUOT_TRY(set_smem(lpn_kernel<0>));
-    grid_for(ctx, (const void *)lpn_kernel<0>, a.ngroups + a.ntail, &grid);
-    lpn_kernel<0><<<grid, kLpnThreads, kTableBytes, st>>>(a);
-  }
-  return launch_status();
+  const bool dual = kk2_d != nullptr;
+  if (d == 10) return dual ? launch_lpn<10, true>(ctx, a, st) : launch_lpn<10, false>(ctx, a, st);
+  return launch_lpn<0, false>(ctx, a, st);  // lpn_group4_dyn / lpn_row1 read a.kk2 themselves
+}
+
+}  // namespace cuot
+
+using namespace cuot;
+
+extern "C" {
+
+int cuot_lpn_primal_dual(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_send_d,
+                         const cuot_block *kk_recv_d, int64_t k, int d, cuot_block *e_send_io_d,
+                         cuot_block *e_recv_io_d, int64_t n, void *stream) {
+  if (!ctx || !seed || !kk_send_d || !kk_recv_d || !e_send_io_d || !e_recv_io_d)
+    return fail(CUOT_EINVAL, "null argument");
+  if (e_send_io_d == e_recv_io_d) return fail(CUOT_EINVAL, "the two roles' rows must not alias");
+  return lpn_rows(ctx, seed, kk_send_d, kk_recv_d, k, d, e_send_io_d, e_recv_io_d, 0, n, n, stream);
+}
+
+int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
+                          int64_t k, int d, cuot_block *e_rows_d, int64_t row_lo, int64_t row_hi,
+                          int64_t n, void *stream) {
+  if (!ctx || !seed || !kk_d || !e_rows_d) return fail(CUOT_EINVAL, "null argument");
+  return lpn_rows(ctx, seed, kk_d, nullptr, k, d, e_rows_d, nullptr, row_lo, row_hi, n, stream);
 }
 
 int cuot_lpn_primal(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,

@@ -859,6 +859,13 @@ int qc_prepare(cuot_ctx *ctx, int e) {
 
 uint64_t qc_ahat_bytes(const cuot_ctx *ctx, int e) { return ahat_bytes(dual_kind(ctx, e), e, false); }
 
+int qc_lane(const cuot_ctx *ctx, int e) {
+  const QcKind k = dual_kind(ctx, e);
+  if (k == kQcFft) return e;
+  if (k == kQcKara) return kQcfMaxE;  // its leaves run on the 2^22 FFT tables
+  return 64 + e;                      // NTT tables hold no per-call state
+}
+
 uint64_t qc_y_bytes(const cuot_ctx *ctx, int e, int batch) {
   const QcKind k = dual_kind(ctx, e);
   const uint64_t y = k == kQcKara ? dual_scratch_bytes(ctx, k, e, batch, false) : y_bytes(k == kQcFft, e, batch);

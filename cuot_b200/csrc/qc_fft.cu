@@ -562,6 +562,14 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
       for (int m = 0; m < Q::R; m++) x[m] = row[spos<E1, KC>(i0 + Q::M * m)];
       pass_twiddle<E1, 0, true, true>(x, Q::base(w), Ts);
       dit_regs<Q::K>(x);
+      if (ahat.margin) {  // rounding-margin record (diagnostic mode only)
+        double mx = 0.0;
+#pragma unroll
+        for (int m = 0; m < Q::R; m++)
+          mx = fmax(mx, fmax(fabs(x[m].x - rint(x[m].x)), fabs(x[m].y - rint(x[m].y))));
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) atomicMax(ahat.margin, __float_as_uint(float(mx)));
+      }
 #pragma unroll
       for (int m = 0; m < Q::R; m++) {
         uint32_t pl[4];
@@ -955,6 +963,7 @@ int qcf_encode(const QcfTables *t, const QcfAhatTab &ahat, const uint64_t *in, u
     const int ntr = (nb + 3) / 4;
     QcfAhatTab tab = ahat;
     tab.first += p0 / 4;
+    tab.margin = t->owner->qcf_margin;
     CUOT_TRY(clear_par(t, ntr, st));
     launch_col_fwd(t, ntr, st, reinterpret_cast<const uint8_t *>(in + uint64_t(p0) * stride), stride * 8, nb, 0,
                    nullptr, static_cast<double2 *>(Y), nullptr, t->par);
@@ -996,6 +1005,7 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
       double2 *Yg = reinterpret_cast<double2 *>(static_cast<uint8_t *>(Y) + uint64_t(g & 1) * G * ybytes);
       QcfAhatTab tab = ahat;
       tab.first += t0;
+      tab.margin = t->owner->qcf_margin;
       uint32_t *tp = tiles + uint64_t(t0) * words;
       uint32_t *pp = par ? par + t0 : nullptr;
       launch_col_fwd(t, ntr, s, nullptr, 0, 4 * ntr, 0, tp, Yg, nullptr, pp);
@@ -1011,6 +1021,7 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
     const int ntr = ntransforms - t0 < bt ? ntransforms - t0 : bt;
     QcfAhatTab tab = ahat;
     tab.first += t0;
+    tab.margin = t->owner->qcf_margin;
     uint32_t *tp = tiles + uint64_t(t0) * words;
     uint32_t *pp = par ? par + t0 : nullptr;
     launch_col_fwd(t, ntr, st, nullptr, 0, 4 * ntr, 0, tp, static_cast<double2 *>(Y), nullptr, pp);

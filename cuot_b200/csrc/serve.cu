@@ -185,8 +185,8 @@ int enqueue_request(Slot &s, cudaStream_t st, const cuot_request &r, std::vector
     CUOT_TRY(launch_status());
     CUOT_TRY(cuot_ferret_pprf_recver(s.ctx, mc, choice, ss, t, h, w, st));
     const uint8_t *ls = reinterpret_cast<const uint8_t *>(&lpn_seed);
-    CUOT_TRY(cuot_lpn_primal(s.ctx, ls, kk_s, r.k, 10, v, int64_t(n), st));
-    CUOT_TRY(cuot_lpn_primal(s.ctx, ls, kk_r, r.k, 10, w, int64_t(n), st));
+    // both roles' LPN in one launch: they share the request's public seed
+    CUOT_TRY(cuot_lpn_primal_dual(s.ctx, ls, kk_s, kk_r, r.k, 10, v, w, int64_t(n), st));
   } else {
     cuot_block *b0, *b1, *m0, *m1, *mc;
     uint64_t *a, *pos;

@@ -68,12 +68,28 @@ uint64_t cuot_ctx_scratch_bytes(const cuot_ctx *ctx);
  *                           stream, for callers that already overlap several
  *                           encodes (the server's slots).  Applies to later
  *                           calls and plans; a graph batch keeps the value
- *                           of its first run (the graph is captured then). */
+ *                           of its first run (the graph is captured then).
+ *   CUOT_TUNE_QC_RECORD_MARGIN  diagnostic, 0 (default) or 1: the fp64 FFT
+ *                           encodes of this context record the largest
+ *                           distance |v - round(v)| between a computed
+ *                           product coefficient and the integer it rounds to
+ *                           (exactness needs < 1/2), read by
+ *                           cuot_qc_fft_margin.  Setting 1 allocates and
+ *                           zeroes one device word (synchronous: not during
+ *                           stream capture); plans and batches made later
+ *                           record too. */
 #define CUOT_TUNE_PPRF_THREADS 1
 #define CUOT_TUNE_QC_PLANES 2
 #define CUOT_TUNE_QC_BACKEND 3
 #define CUOT_TUNE_QC_STREAMS 4
+#define CUOT_TUNE_QC_RECORD_MARGIN 5
 int cuot_ctx_set_tuning(cuot_ctx *ctx, int key, int64_t value);
+/* The largest |v - round(v)| the context's fp64 FFT encodes have rounded
+ * since recording was switched on or last reset (reset != 0 zeroes it after
+ * the read).  Synchronous.  CUOT_EINVAL when recording is off.  No
+ * counterpart in the reference (its float cuFFT encode truncates without a
+ * bound, silent/quasi_cyclic.cu:34-49). */
+int cuot_qc_fft_margin(cuot_ctx *ctx, double *out, int reset);
 
 /* ---- AES-128 ECB ---------------------------------------------------------
  * In-place FIPS-197 AES-128 of `nblocks` blocks under `key` (host, 16 bytes).
@@ -157,6 +173,17 @@ int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16],
                           const cuot_block *kk_d, int64_t k, int d,
                           cuot_block *e_rows_d, int64_t row_lo,
                           int64_t row_hi, int64_t n, void *stream);
+/* Both roles of one extension when they run on the same GPU (a dealer, a
+ * test harness, the batched engine and server, which hold both parties):
+ * the two calls LpnF2::compute makes, one per party with the seed ALICE sends
+ * BOB (lpn_f2.h:81-101), share the public index matrix, so it is generated
+ * once and each index gathers from both kk_send_d and kk_recv_d.  Equal to
+ * cuot_lpn_primal on (kk_send_d, e_send_io_d) and on (kk_recv_d,
+ * e_recv_io_d); the two row arrays must not alias. */
+int cuot_lpn_primal_dual(cuot_ctx *ctx, const uint8_t seed[16],
+                         const cuot_block *kk_send_d, const cuot_block *kk_recv_d,
+                         int64_t k, int d, cuot_block *e_send_io_d,
+                         cuot_block *e_recv_io_d, int64_t n, void *stream);
 
 /* ---- SOT PPRF ----------------------------------------------------------------
  * Structure of SOTSender/SOTRecver::seed_expand (silent/sender.cu:76-108,
@@ -305,11 +332,13 @@ int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *plan, const cuot_block *in_d,
 
 /* ---- batched engine ------------------------------------------------------
  * Many OT-extension instances of uneven n and depth, both roles each, run as
- * one device program: one persistent PPRF launch over all trees of all
- * senders (per-tree work queue, deepest trees first), one over all
- * receivers, one persistent LPN launch over all Ferret rows of both roles,
- * and for SOT one set of QC transform passes per transform size spanning
- * the planes of every instance of that size.  On first run the whole program is
+ * one device program of two branches that run side by side: Ferret (one
+ * persistent PPRF launch over all Ferret sender trees -- per-tree work queue,
+ * deepest trees first --, one over the receivers, one persistent LPN launch
+ * over all Ferret rows, both roles of a row from one index computation) and
+ * SOT (the same PPRF launches over the SOT trees, then for each transform
+ * size, on its own stream, one set of QC transform passes spanning the planes
+ * of every instance of that size).  On first run the whole program is
  * captured into a CUDA graph (cfg.use_graph) and replayed afterwards.
  * No counterpart call in the reference, which runs one instance per call
  * (FerretCOT::extend, ferret_cot.hpp:80-91; SOT roles, silent/roles.h).
@@ -349,6 +378,9 @@ typedef struct {
   int lpn_rows_per_task;   /* LPN work-queue granularity, multiple of 4 (0: 65536) */
   int qc_planes_per_pass;  /* planes per QC pass (0: 512 MiB of intermediate) */
   int use_graph;           /* capture into a CUDA graph on first run */
+  int serial;              /* 1: every launch in one chain on the caller's
+                              stream; 0: the Ferret branch and each SOT size
+                              run side by side (forked and joined) */
 } cuot_batch_config;
 
 typedef struct cuot_batch cuot_batch;

@@ -106,6 +106,21 @@ def emp_spcot_recver(mc, choice, secret_sum, h: int):
     return leaves, pos
 
 
+def emp_mpcot_trees(roots, h: int, delta, choice):
+    """Both roles of the trees `roots` through the reference's own
+    SPCOT_Sender / SPCOT_Recver::compute in one single-threaded call (the
+    level OT by selection: choice[i*h + l] = 1 picks ot_msg_1).  Returns
+    (sender leaves, receiver leaves), tree-major.  h >= 2."""
+    roots = np.ascontiguousarray(roots, np.uint8).reshape(-1, 16)
+    t = roots.shape[0]
+    ch = np.ascontiguousarray(choice, np.uint8).reshape(t * h)
+    ls = np.empty((t << h, 16), np.uint8)
+    lr = np.empty((t << h, 16), np.uint8)
+    rc = emp_lib().ref_mpcot_trees(_p(roots), INT(t), INT(h), _p(_u8(delta)), _p(ch), _p(ls), _p(lr))
+    assert rc == 0, f"ref_mpcot_trees rejected h={h}"
+    return ls, lr
+
+
 def emp_lpn_task(seed, kk, nn, d: int = 10, start: int = 0, end: int | None = None,
                  inplace: bool = False) -> np.ndarray:
     """LpnF2<IO, d>::task(nn, kk, start, end) (lpn_f2.h:46-79): one task

@@ -126,6 +126,34 @@ int ref_spcot_recver(int h, const uint8_t *b, const uint8_t *m, const uint8_t *s
   return 0;
 }
 
+// Both roles of `T` trees of one MPCOT, one thread: SPCOT_Sender::compute per
+// tree (seed = roots[i]), the level OT by selection (choice[i*h + l] picks
+// ot_msg_1), then SPCOT_Recver::compute.  leaves_s / leaves_r: T * 2^h blocks
+// each, tree-major.  h >= 2.
+int ref_mpcot_trees(const uint8_t *roots, int T, int h, const uint8_t *delta, const uint8_t *choice,
+                    uint8_t *leaves_s, uint8_t *leaves_r) {
+  if (h < 2 || h > 24 || T < 0) return -1;
+  NullIO io;
+  const size_t W = size_t(1) << h;
+  std::vector<block> rtree(W + 4);
+  for (int i = 0; i < T; ++i) {
+    SPCOT_Sender<NullIO> s(&io, h + 1);
+    s.seed = load(roots + 16 * size_t(i));
+    block *tree = reinterpret_cast<block *>(leaves_s) + size_t(i) * W;
+    s.compute(tree, load(delta));
+    SPCOT_Recver<NullIO> r(&io, h + 1);
+    for (int l = 0; l < h; ++l) {
+      r.b[l] = choice[size_t(i) * h + l] != 0;
+      r.m[l] = r.b[l] ? s.m[h + l] : s.m[l];
+    }
+    r.secret_sum_f2 = s.secret_sum_f2;
+    r.get_index();
+    r.compute(rtree.data());
+    std::memcpy(leaves_r + size_t(i) * W * 16, rtree.data(), W * sizeof(block));
+  }
+  return 0;
+}
+
 // LpnF2<IO, d>::task(nn, kk, start, end) with seed = `seed`: nn[i] ^= the d
 // indexed kk blocks for rows [start, end), the last <= 4 rows through
 // __compute1.  d in [1, 32].

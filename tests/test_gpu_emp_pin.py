@@ -122,3 +122,34 @@ def test_emp_callers_through_the_adapter():
         pytest.skip("oracle/_ref/test_emp_callers not built (needs the reference tree)")
     r = subprocess.run([CALLERS], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("n,k,d", [(65536, 8192, 10), (4099, 1000, 10), (7, 33, 10), (1, 5, 10),
+                                   (1030, 777, 7), (64, 200, 3)])
+def test_dual_role_lpn_equals_reference_code_per_role(ctx, n, k, d):
+    """cuot_lpn_primal_dual (both roles from one index computation) gives each
+    role exactly LpnF2::task over [0, n) with that role's kk."""
+    rng = np.random.default_rng(n + 13 * k + d)
+    seed = rng_blocks(rng, 1)[0]
+    kk_s, kk_r, e_s, e_r = rng_blocks(rng, k), rng_blocks(rng, k), rng_blocks(rng, n), rng_blocks(rng, n)
+    ds, dr = to_dev(e_s), to_dev(e_r)
+    ctx.lpn_primal_dual(seed, to_dev(kk_s), to_dev(kk_r), ds, dr, d=d)
+    assert np.array_equal(to_host(ds), oracle.emp_lpn_task(seed, kk_s, e_s, d=d))
+    assert np.array_equal(to_host(dr), oracle.emp_lpn_task(seed, kk_r, e_r, d=d))
+
+
+def test_dual_role_lpn_full_size_b13(ctx):
+    """ferret_b13 (n = 10,485,760, k = 452,000): the dual-role launch equals
+    two single-role launches, bit for bit, on both roles."""
+    rng = np.random.default_rng(1300)
+    n, k = 10485760, 452000
+    seed = rng_blocks(rng, 1)[0]
+    kk_s, kk_r = to_dev(rng_blocks(rng, k)), to_dev(rng_blocks(rng, k))
+    e_s = torch.randint(0, 256, (n, 16), dtype=torch.uint8, device="cuda")
+    e_r = torch.randint(0, 256, (n, 16), dtype=torch.uint8, device="cuda")
+    a_s, a_r = e_s.clone(), e_r.clone()
+    ctx.lpn_primal_dual(seed, kk_s, kk_r, e_s, e_r)
+    ctx.lpn_primal(seed, kk_s, a_s)
+    ctx.lpn_primal(seed, kk_r, a_r)
+    torch.cuda.synchronize()
+    assert torch.equal(e_s, a_s) and torch.equal(e_r, a_r)

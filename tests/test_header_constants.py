@@ -19,7 +19,7 @@ def defines() -> dict:
 
 def test_tuning_keys():
     d = defines()
-    for name in ("PPRF_THREADS", "QC_PLANES", "QC_BACKEND", "QC_STREAMS"):
+    for name in ("PPRF_THREADS", "QC_PLANES", "QC_BACKEND", "QC_STREAMS", "QC_RECORD_MARGIN"):
         assert getattr(Context, "TUNE_" + name) == d["CUOT_TUNE_" + name], name
 
 
