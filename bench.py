@@ -69,6 +69,7 @@ WORKLOADS = {
     "ferret_b13_mal": dict(kind="ferret", t=1280, h=13, k=452000, d=10, mal=True),
     "ferret_c1": dict(kind="ferret", t=64, h=10, k=8192, d=10),
     "ferret_rcot": dict(kind="session", t=1280, h=13, k=452000, d=10),
+    "aes_ecb": dict(kind="aes", n=1 << 26),
 }
 CONFIG_TEXT = {
     "mixed64": "batched mix: 64 instances (32 SOT, 32 Ferret-style), log2 n uniform in [16,22], depth 10-14, "
@@ -85,6 +86,8 @@ CONFIG_TEXT = {
     "ferret_b13_mal": "ferret_b13 plus the malicious consistency check's per-tree GF(2^128) sums of both roles "
                       "(seeds given; their SHA-256 derivation is host protocol)",
     "ferret_c1": "plain Ferret small: n=65536, t=64, h=10, k=8192, d=10 (both roles)",
+    "aes_ecb": "diagnostic: AES-128 ECB of 2^26 blocks (1 GiB) in place, the shared-memory T-table kernel "
+               "against the bitsliced register kernel",
     "ferret_rcot": "Ferret rcot session at ferret_b13 parameters: one extension per step (both roles), its M = "
                    "k + t*h + 128 pre-COTs carried over on the device; value counts the ot_limit = 10,016,992 "
                    "usable COTs per extension",
@@ -92,6 +95,8 @@ CONFIG_TEXT = {
 
 
 def metric_name(workload: str) -> str:
+    if WORKLOADS[workload]["kind"] == "aes":
+        return "AES-128 blocks/sec on 1 B200 (T-table vs bitsliced)"
     if WORKLOADS[workload]["kind"] == "batch":
         return "COTs/sec on 1 B200, batched vs plain path (bit-exact)"
     return "COTs/sec on 1 B200 (plain path, bit-exact)"
@@ -691,6 +696,46 @@ class CpuMix:
         return sum(t << h for _, t, h, _ in self.shapes) / (total / self.threads)
 
 
+def reference_gpu_context(workload: str, pprf_ms: float, lpn_ms: float, reps: int = 5):
+    """Speed context only: the reference's own GPU path rebuilt for sm_100a
+    (oracle/_ref/librefgpu.so) on this workload's shape, beside this
+    library's stage times.  The reference calls are its blocking API
+    (dev_layer.h's cuda_mpcot_sender and cuda_primal_lpn, with their own host
+    copies; SOTSender::dual_lpn's transpose + cuFFT encode + transpose),
+    timed per role; their outputs are not bit-exact (non-FIPS AES schedule,
+    racy level sums, float FFT), so this is not a parity baseline.  None
+    when the library was not built or the shape is outside the reference
+    kernels' safe range."""
+    import oracle
+    L = oracle.refgpu_lib()
+    spec = WORKLOADS[workload]
+    if L is None or spec["kind"] not in ("ferret", "sot") or spec.get("r2") or spec.get("mal"):
+        return None
+    t, h = spec["t"], spec["h"]
+    n = t << h
+    if spec["kind"] == "ferret":
+        if n % 2048 or n > (1 << 22):
+            return None
+        snd = L.ref_gpu_mpcot_sender_ms(t, h, reps)
+        lpn = L.ref_gpu_primal_lpn_ms(n, spec["k"], reps)
+        if snd <= 0 or lpn <= 0:
+            return None
+        return {"what": "reference cuda_mpcot_sender and cuda_primal_lpn (dev_layer.cu), per role, blocking, "
+                        "host copies included; sm_100a -O2",
+                "mpcot_sender_ms_per_role": snd, "primal_lpn_ms_per_role": lpn,
+                "ours_pprf_ms_per_role": pprf_ms / 2, "ours_lpn_ms_per_role": lpn_ms / 2,
+                "note": "ours: device time of the stage (both roles) halved; the reference receiver "
+                        "(cuda_mpcot_recver) is not run"}
+    if n < (1 << 17) or n > (1 << 23):
+        return None
+    dl = L.ref_gpu_sot_dual_lpn_ms(n, reps)
+    if dl <= 0:
+        return None
+    return {"what": "reference SOTSender::dual_lpn content (Mat::bit_transpose, QuasiCyclic::encode_dense with "
+                    "cuFFT, Mat::bit_transpose), one role, sm_100a -O2",
+            "dual_lpn_ms_per_role": dl, "ours_dual_lpn_ms_per_role": lpn_ms / 2}
+
+
 # --------------------------------------------------------------------------
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -757,7 +802,7 @@ def run_batch(args):
     if not args.no_autotune:
         from cuot_b200.autotune import TuningTable, tune_batch
         tuned, _ = tune_batch(ctx, insts, table=TuningTable())  # CUOT_TUNING_TABLE sets its path
-    batch = Batch(ctx, insts, use_graph=True, **tuned)
+    batch = Batch(ctx, insts, use_graph=True, serial=args.batch_serial, **tuned)
     for _ in range(args.warmup):
         batch.run(stream)
         batch.run_plain(stream)
@@ -822,7 +867,7 @@ def run_batch(args):
     # same outputs): step j's input copy runs during step j-1.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     insts2 = [i.input_copy() for i in insts]
-    batch2 = Batch(ctx, insts2, use_graph=True, **tuned)
+    batch2 = Batch(ctx, insts2, use_graph=True, serial=args.batch_serial, **tuned)
     batch2.run(stream)
     batches = [batch, batch2]
     host_in, host_out = [[], []], []
@@ -901,7 +946,8 @@ def run_batch(args):
         "value": world * cots / (ms / 1e3), "unit": "COTs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "qc_backend": args.qc_backend, "instances": len(insts),
+        "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "qc_backend": args.qc_backend,
+                   "schedule": "one chain" if args.batch_serial else "concurrent branches", "instances": len(insts),
                    "cots_per_step_per_gpu": cots, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "plain": {"value": world * cots / (ms_plain / 1e3), "ms_per_step": ms_plain,
@@ -940,12 +986,51 @@ def run_batch(args):
     return 0
 
 
+def run_aes(args):
+    """Diagnostic: the two AES-128 designs on the same data, CUDA events,
+    the 1 GiB buffer larger than L2 (each kernel reads and writes it once)."""
+    import torch
+    import cuot_b200
+    spec = WORKLOADS[args.workload]
+    n = spec["n"]
+    torch.cuda.set_device(0)
+    ctx = new_context(cuot_b200, 0)
+    key = np.arange(16, dtype=np.uint8)
+    buf = torch.randint(0, 256, (n, 16), dtype=torch.uint8, device="cuda")
+    res = {}
+    clk = ClockSampler(0)
+    clk.start()
+    for name, fn in (("ttable", ctx.aes128_ecb), ("bitsliced", ctx.aes128_ecb_bitsliced)):
+        for _ in range(args.warmup):
+            fn(key, buf)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            fn(key, buf)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        res[name] = {"ms": ms, "aes_per_s": n / (ms / 1e3), "hbm_gbs": 32 * n / (ms / 1e3) / 1e9}
+    clocks = clk.stop()
+    out = {"metric": metric_name(args.workload), "value": res["ttable"]["aes_per_s"], "unit": "AES/s",
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ttable"]["ms"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+           "data": "synthetic (random)", "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload],
+                                                     "blocks": n},
+           "aes": res, "bitsliced_over_ttable": res["bitsliced"]["aes_per_s"] / res["ttable"]["aes_per_s"],
+           "clocks": clocks}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_served(args, device: int) -> dict:
     """The served request stream.  Saturation throughput of the
     continuous-batching server sets the sustained rate (90 % of it); the
     same Poisson stream is then served by the continuous-batching server and
     by plain per-request execution (one request at a time)."""
-    from cuot_b200.serve import Server, make_stream, sustained_rate
+    from cuot_b200.serve import Server, make_stream, saturation
 
     lo, hi = 14, 24
     # small requests (n < 2^20) on high-priority streams; at most one request
@@ -954,23 +1039,29 @@ def run_served(args, device: int) -> dict:
     big_n, prio_n = 1 << 22, 1 << 20
     cont = Server(slots=args.serve_slots, device=device, max_log_n=hi, budget_bytes=1e15,
                   high_priority_below_n=prio_n)
-    probe = make_stream(min(100, args.serve_requests), rate=0.0, seed=5, lo=lo, hi=hi)
-    rate = sustained_rate(cont, probe)
+    plain = Server(slots=1, device=device, max_log_n=hi, budget_bytes=120e9)
+    # saturation: the same probe (every request present at t = 0) through both
+    probe = make_stream(min(200, args.serve_requests), rate=0.0, seed=5, lo=lo, hi=hi)
+    sat = saturation(cont, probe)
+    sat_plain = saturation(plain, make_stream(len(probe), rate=0.0, seed=5, lo=lo, hi=hi))
+    rate = 0.9 * sat["req_per_s"]
     reqs = make_stream(args.serve_requests, rate=rate, seed=6, lo=lo, hi=hi)
     cont.configure(budget_bytes=120e9, big_n=big_n, high_priority_below_n=prio_n)
     rep = cont.run(reqs)
     cont.close()
-    plain = Server(slots=1, device=device, max_log_n=hi, budget_bytes=120e9)
     rep_plain = plain.run(reqs)
     plain.close()
     keys = ("done", "cots_per_s", "p50_ms", "p99_ms", "mean_ms", "wall_s")
     return {"requests": args.serve_requests, "slots": args.serve_slots, "budget_gb": 120,
             "log2_n": [lo, hi], "rate_rps": rate,
             "policy": {"high_priority_below_n": prio_n, "max_in_flight_with_n_ge": [big_n, 1]},
+            "saturation": {"probe_requests": len(probe), "continuous": sat, "plain_per_request": sat_plain,
+                           "continuous_over_plain": sat["req_per_s"] / sat_plain["req_per_s"]},
             "continuous": {k: rep[k] for k in keys},
             "plain_per_request": {k: rep_plain[k] for k in keys},
             "note": "latency = arrival -> outputs in device memory; rate = 0.9 x saturation throughput "
-                    "of the continuous-batching server"}
+                    "of the continuous-batching server (its probe: every request present at t = 0, the "
+                    "same probe for plain per-request execution)"}
 
 
 def run_session(args):
@@ -1082,6 +1173,8 @@ def run_ours(args):
         return run_batch(args)
     if WORKLOADS[args.workload]["kind"] == "session":
         return run_session(args)
+    if WORKLOADS[args.workload]["kind"] == "aes":
+        return run_aes(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1217,6 +1310,10 @@ def run_ours(args):
         out["transpose"] = transpose_roofline(inst, flush, peaks, peak_kind)
     if inst.spec["kind"] == "sot":
         out["qc_transform"] = qc_transform_report([inst.n], lpn_ms)
+    if rank == 0 and world == 1:
+        rg = reference_gpu_context(args.workload, pprf_ms, lpn_ms)
+        if rg:
+            out["reference_gpu"] = rg
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, sample = cpu_sample(args.workload, threads)
@@ -1240,10 +1337,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=1000,
+    ap.add_argument("--serve-requests", type=int, default=10000,
                     help="requests of the served stream reported with mixed64 (0: skip; the full served configuration is 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--batch-serial", action="store_true",
+                    help="batched mix: one chain of launches instead of the concurrent branches (A/B diagnostic)")
     ap.add_argument("--qc-backend", default="auto", choices=sorted(QC_BACKENDS),
                     help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^22, Karatsuba over it for "
                          "dual LPNs at 2^23 and 2^24, NTT above)")
@@ -1251,6 +1350,9 @@ def main():
     global _qc_backend
     _qc_backend = QC_BACKENDS[args.qc_backend]
     if args.impl == "reference":
+        if WORKLOADS[args.workload]["kind"] == "aes":
+            print(json.dumps({"impl": "reference", "unavailable": "diagnostic workload without a reference CPU path"}))
+            return 0
         return run_reference(args)
     return run_ours(args)
 

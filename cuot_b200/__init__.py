@@ -152,6 +152,11 @@ class Context:
                                         _stream(stream)), "cuot_aes128_ecb")
         return io
 
+    def aes128_ecb_bitsliced(self, key, io, stream=None):
+        _check(self.lib.cuot_aes128_ecb_bitsliced(self.h, _host_block(key), _ptr(io), C.c_uint64(_nblocks(io)),
+                                                  _stream(stream)), "cuot_aes128_ecb_bitsliced")
+        return io
+
     def prg_fill(self, seed, out, block_offset: int = 0, stream=None):
         _check(self.lib.cuot_prg_fill(self.h, _host_block(seed), C.c_uint64(block_offset), _ptr(out),
                                       C.c_uint64(_nblocks(out)), _stream(stream)), "cuot_prg_fill")

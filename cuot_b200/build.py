@@ -80,18 +80,21 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
 def build_oracle() -> str:
     """Test infrastructure: the CPU oracle and, when the reference tree is
     present, its pins built from the reference's own sources (oracle/_ref:
-    cryptoTools AES/PRNG, emp-ot's GGM/SPCOT/LPN headers, and the program
-    that drives emp-ot's MpcotReg/LpnF2 callers through libcuot.so)."""
+    cryptoTools AES/PRNG, emp-ot's GGM/SPCOT/LPN headers, the program that
+    drives emp-ot's MpcotReg/LpnF2 callers through libcuot.so, and the
+    reference's own GPU path for speed context and the transpose pin)."""
     odir = os.path.join(ROOT, "oracle")
     subprocess.check_call(["make", "-s", "-C", odir])
     ref_script = os.path.join(odir, "build_ref.sh")
     shim = os.path.join(odir, "emp_shim")
     deps = [os.path.join(odir, "ref_driver.cpp"), os.path.join(odir, "emp_ref.cpp"), ref_script, LIB,
+            os.path.join(odir, "ref_gpu_driver.cu"), os.path.join(odir, "refgpu.map"),
             os.path.join(ROOT, "tests", "cpp", "test_emp_callers.cpp"),
             os.path.join(ROOT, "include", "cuot_dev_layer.h")]
     for d, _, files in os.walk(shim):
         deps += [os.path.join(d, f) for f in files]
-    outs = [os.path.join(odir, "_ref", f) for f in ("libctref.so", "libempref.so", "test_emp_callers")]
+    outs = [os.path.join(odir, "_ref", f) for f in ("libctref.so", "libempref.so", "test_emp_callers",
+                                                      "librefgpu.so")]
     if any(_stale(o, [d for d in deps if os.path.exists(d)]) for o in outs):
         subprocess.check_call(["sh", ref_script])  # skips itself without the reference tree
     return os.path.join(odir, "liboracle.so")

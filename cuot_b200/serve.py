@@ -242,10 +242,18 @@ def report(requests: list[Request], wall: float) -> dict:
             "mean_ms": float(lat.mean() * 1e3)}
 
 
-def sustained_rate(server: Server, probe: list[Request], headroom: float = 0.9) -> float:
-    """Requests/s the server sustains under its current policy: saturation
-    throughput on `probe` (every request present at t = 0), times `headroom`."""
+def saturation(server: Server, probe: list[Request]) -> dict:
+    """Saturation throughput of the server under its current policy: every
+    request of `probe` present at t = 0.  Returns {"req_per_s", "cots_per_s",
+    "requests", "wall_s"}."""
     for r in probe:
         r.arrival = 0.0
     rep = server.run(probe)
-    return headroom * rep["done"] / rep["wall_s"]
+    return {"req_per_s": rep["done"] / rep["wall_s"], "cots_per_s": rep["cots_per_s"], "requests": rep["done"],
+            "wall_s": rep["wall_s"]}
+
+
+def sustained_rate(server: Server, probe: list[Request], headroom: float = 0.9) -> float:
+    """Requests/s the server sustains under its current policy: saturation
+    throughput on `probe` (every request present at t = 0), times `headroom`."""
+    return headroom * saturation(server, probe)["req_per_s"]

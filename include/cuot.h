@@ -98,6 +98,13 @@ int cuot_qc_fft_margin(cuot_ctx *ctx, double *out, int reset);
  * schedule (the reference XORs Rcon[i-1], gpu/aes_expand.cu:59). */
 int cuot_aes128_ecb(cuot_ctx *ctx, const uint8_t key[16], cuot_block *io_d,
                     uint64_t nblocks, void *stream);
+/* The same encryption, bitsliced: 32 blocks per thread as 128 bit-planes in
+ * registers, the S-box as a GF(2) circuit (tower-field inversion), no table
+ * lookups.  Same results as cuot_aes128_ecb; kept to measure the two AES
+ * designs against each other on the same GPU (the library's PPRF and LPN
+ * use the faster one, the T-table).  No counterpart in the reference. */
+int cuot_aes128_ecb_bitsliced(cuot_ctx *ctx, const uint8_t key[16], cuot_block *io_d,
+                              uint64_t nblocks, void *stream);
 
 /* Seeded PRG on the device: blocks [block_offset, +nblocks) of the
  * cryptoTools PRNG stream for `seed` (block i = AES_seed(i as a little-endian

@@ -59,6 +59,46 @@ def emp_lib():
     return _EMP
 
 
+_REFGPU = None
+
+
+def refgpu_lib():
+    """oracle/_ref/librefgpu.so: the reference's own GPU path (gpu/*.cu,
+    dev_layer.cu, silent/quasi_cyclic.cu) for sm_100a with a timing and
+    transpose harness (oracle/ref_gpu_driver.cu), or None when it was not
+    built.  Speed context and the transpose pin only: its other outputs are
+    not the oracle's semantics."""
+    global _REFGPU
+    if _REFGPU is None:
+        path = os.path.join(_HERE, "_ref", "librefgpu.so")
+        if not os.path.exists(path):
+            return None
+        try:
+            L = ctypes.CDLL(path)
+        except OSError:  # no CUDA driver on this host (libcuda.so.1)
+            return None
+        L.ref_gpu_mpcot_sender_ms.restype = C.c_double
+        L.ref_gpu_mpcot_sender_ms.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.ref_gpu_primal_lpn_ms.restype = C.c_double
+        L.ref_gpu_primal_lpn_ms.argtypes = [C.c_int64, C.c_int, C.c_int]
+        L.ref_gpu_sot_dual_lpn_ms.restype = C.c_double
+        L.ref_gpu_sot_dual_lpn_ms.argtypes = [C.c_uint64, C.c_int]
+        L.ref_gpu_bit_transpose.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
+        _REFGPU = L
+    return _REFGPU
+
+
+def refgpu_bit_transpose(blocks: np.ndarray) -> np.ndarray:
+    """The reference's Mat::bit_transpose of n one-block rows (n a multiple
+    of 256, at most 2^23): 128 planes of n/8 bytes."""
+    inp = np.ascontiguousarray(blocks, np.uint8).reshape(-1, 16)
+    n = inp.shape[0]
+    out = np.empty((128, n // 8), np.uint8)
+    rc = refgpu_lib().ref_gpu_bit_transpose(_p(inp), n, _p(out))
+    assert rc == 0, f"ref_gpu_bit_transpose rejected n={n} ({rc})"
+    return out
+
+
 def emp_aes_ecb(key, blocks: np.ndarray):
     """AES-128 ECB through the emp-tool shim (AES_set_encrypt_key +
     AES_ecb_encrypt_blks)."""

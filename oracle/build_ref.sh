@@ -45,3 +45,26 @@ if [ -f "$ROOT/cuot_b200/libcuot.so" ]; then
     -o "$HERE/_ref/test_emp_callers"
   echo "built $HERE/_ref/test_emp_callers"
 fi
+# The reference's own GPU path (gpu/*.cu, silent/quasi_cyclic.cu,
+# ferret/emp-ot/emp-ot/ferret/dev_layer.cu) for sm_100a at -O2, with the
+# timing / transpose harness oracle/ref_gpu_driver.cu: speed context and the
+# transpose pin only.  Only the ref_gpu_* entry points are exported
+# (refgpu.map), so its Mat / dev_layer names stay private.
+if command -v nvcc >/dev/null 2>&1; then
+  OBJ="$HERE/_ref/refgpu_obj"
+  mkdir -p "$OBJ"
+  NVF="-gencode arch=compute_100a,code=sm_100a -O2 -std=c++20 -w -Xcompiler -fPIC"
+  INC="-I$REF/gpu -I$REF/silent -I$EMPOT/emp-ot/ferret"
+  pids=""
+  for f in "$REF"/gpu/aes_expand.cu "$REF"/gpu/aes_op.cu "$REF"/gpu/gpu_data.cu "$REF"/gpu/gpu_matrix.cu \
+           "$REF"/gpu/gpu_ops.cu "$REF"/gpu/gpu_span.cu "$REF"/gpu/gpu_tests.cu "$REF"/gpu/logger.cu \
+           "$REF"/silent/quasi_cyclic.cu "$EMPOT"/emp-ot/ferret/dev_layer.cu "$HERE"/ref_gpu_driver.cu; do
+    nvcc $NVF $INC -c "$f" -o "$OBJ/$(basename "$f" .cu).o" &
+    pids="$pids $!"
+  done
+  for p in $pids; do wait "$p"; done
+  nvcc -shared -gencode arch=compute_100a,code=sm_100a "$OBJ"/*.o -o "$HERE/_ref/librefgpu.so" \
+    -lcufft -lcurand -L"${CUDA:-/usr/local/cuda}/lib64/stubs" -lcuda -Xlinker --version-script="$HERE/refgpu.map" -Xlinker -Bsymbolic \
+    -Xlinker -rpath="${CUDA:-/usr/local/cuda}/lib64"
+  echo "built $HERE/_ref/librefgpu.so"
+fi

@@ -1,0 +1,122 @@
+// ref_gpu_driver.cu -- TEST INFRASTRUCTURE ONLY: speed context and one pin.
+//
+// Drives the reference's own GPU path, compiled from the reference tree for
+// sm_100a by oracle/build_ref.sh into oracle/_ref/librefgpu.so (only the
+// ref_gpu_* entry points below are exported, so the reference's Mat and
+// dev_layer names cannot collide with libcuot's adapter of the same names):
+//   cuda_mpcot_sender   ferret/emp-ot/emp-ot/ferret/dev_layer.cu:20-59
+//   cuda_primal_lpn     ferret/emp-ot/emp-ot/ferret/dev_layer.cu:161-186
+//   QuasiCyclic::encode_dense + two Mat::bit_transpose, the content of
+//                       SOTSender::dual_lpn (silent/sender.cu:110-119,
+//                       silent/quasi_cyclic.cu:118-128, gpu/gpu_matrix.cu:95-121)
+// These outputs are not an oracle: the reference GPU path uses a non-FIPS key
+// schedule, races on its level sums and rounds a float FFT.  Only
+// Mat::bit_transpose is exact, and the tests compare it with this library's
+// transpose.  Every entry point accepts only shapes for which the reference
+// kernels' index arithmetic (none of them checks bounds) stays inside the
+// buffers the reference's own callers allocate:
+//   MPCOT: t * 2^h >= 1024 leaves (level widths below 512 then read and write
+//     inside the t * 2^h-block matrices);
+//   LPN: n a multiple of 2048 (make_block and lpn_single_row launch exactly
+//     n*d/4 / 1024 and n / 1024 full blocks of 1024 threads);
+//   transpose: n a multiple of 256 rows, at most 2^23 (beyond that the
+//     kernel's row-block count no longer covers the grid);
+//   QC encode: n a power of two in [2^17, 2^23] (a's make_block launch needs
+//     n / 128 to be a multiple of 1024).
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "dev_layer.h"
+#include "gpu_matrix.h"
+#include "gpu_ops.h"
+#include "pprf.h"
+#include "quasi_cyclic.h"
+
+namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
+
+}  // namespace
+
+extern "C" {
+
+// Mean wall-clock ms of the reference's blocking cuda_mpcot_sender for t
+// trees of depth h (one GPU), over `reps` calls after one warm-up call.
+__attribute__((visibility("default"))) double ref_gpu_mpcot_sender_ms(int t, int h, int reps) {
+  const uint64_t n = uint64_t(t) << h;
+  if (t < 1 || h < 1 || h > 20 || n < 1024 || reps < 1) return -1.0;
+  // FerretCOT::expSeed and MpcotReg::buffer / separated (ferret_cot.hpp:19-22,
+  // mpcot_reg.h:55-61): t * 2^h blocks each
+  Mat expanded({n}), buffer({n}), sep({n});
+  expanded.clear();
+  std::vector<blk> ls(size_t(t) * h), rs(size_t(t) * h), ss(t);
+  blk delta{{1, 2, 3, 4}};
+  int tt[1] = {t};
+  cuda_mpcot_sender(&expanded, &buffer, &sep, ls.data(), rs.data(), ss.data(), tt, h, &delta, 1);
+  const double t0 = now_ms();
+  for (int i = 0; i < reps; i++)
+    cuda_mpcot_sender(&expanded, &buffer, &sep, ls.data(), rs.data(), ss.data(), tt, h, &delta, 1);
+  return (now_ms() - t0) / reps;
+}
+
+// Mean wall-clock ms of the reference's blocking cuda_primal_lpn (index
+// matrix generation, kk upload, lpn_single_row, nn download) for n rows,
+// k inputs, d = 10.
+__attribute__((visibility("default"))) double ref_gpu_primal_lpn_ms(int64_t n, int k, int reps) {
+  const int64_t d = 10;
+  if (n < 2048 || n % 2048 || k < 1 || reps < 1) return -1.0;
+  // LpnF2's pubMats / kk_d (lpn_f2.h:32-38) and the MPCOT output rows
+  Mat pub({uint64_t((n * d + 3) / 4)}), kk_d({uint64_t(k)}), expanded({uint64_t(n)});
+  expanded.clear();
+  std::vector<blk> kk(k), nn(n);
+  for (int i = 0; i < k; i++)
+    for (int w = 0; w < 4; w++) kk[i].data[w] = uint32_t(i * 2654435761u + w);
+  uint32_t key[44] = {0x01020304, 0x05060708, 0x090a0b0c, 0x0d0e0f10};
+  int64_t rows[1] = {n};
+  cuda_primal_lpn(Sender, &pub, d, rows, k, key, &expanded, nn.data(), &kk_d, kk.data(), 1);
+  const double t0 = now_ms();
+  for (int i = 0; i < reps; i++)
+    cuda_primal_lpn(Sender, &pub, d, rows, k, key, &expanded, nn.data(), &kk_d, kk.data(), 1);
+  return (now_ms() - t0) / reps;
+}
+
+// Mean ms of one role's SOT dual LPN on the reference's GPU path: the
+// leaves (n blocks) to 128 bit planes, QuasiCyclic(Sender, 2n, n,
+// 128).encode_dense, and back (silent/sender.cu:110-119), device time with
+// a synchronisation on both sides.  The QuasiCyclic set-up (a and its
+// transform) is outside the timed region, as in the reference's constructor.
+__attribute__((visibility("default"))) double ref_gpu_sot_dual_lpn_ms(uint64_t n, int reps) {
+  if (!pow2(n) || n < (1ull << 17) || n > (1ull << 23) || reps < 1) return -1.0;
+  Mat b({n, 1});
+  b.clear();
+  QuasiCyclic qc(Sender, 2 * n, n, 128);
+  auto one = [&] {
+    b.bit_transpose(0, 0);  // (n, 1) -> (128, n / 128)
+    qc.encode_dense(b);
+    b.bit_transpose(0, 0);  // back to (n, 1)
+  };
+  one();
+  cudaDeviceSynchronize();
+  const double t0 = now_ms();
+  for (int i = 0; i < reps; i++) one();
+  cudaDeviceSynchronize();
+  return (now_ms() - t0) / reps;
+}
+
+// The reference's Mat::bit_transpose of n rows of one block each: in (host,
+// n * 16 bytes) -> out (host, 128 planes of n / 8 bytes).  0 on success.
+__attribute__((visibility("default"))) int ref_gpu_bit_transpose(const uint8_t *in, uint64_t n, uint8_t *out) {
+  if (n < 256 || n % 256 || n > (1ull << 23)) return -1;
+  Mat m({n, 1});
+  if (cudaMemcpy(m.data(), in, n * 16, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+  m.bit_transpose(0, 0);
+  if (cudaMemcpy(out, m.data(), n * 16, cudaMemcpyDeviceToHost) != cudaSuccess) return -3;
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
+}
+
+}  // extern "C"
