@@ -802,7 +802,8 @@ def run_batch(args):
     if not args.no_autotune:
         from cuot_b200.autotune import TuningTable, tune_batch
         tuned, _ = tune_batch(ctx, insts, table=TuningTable())  # CUOT_TUNING_TABLE sets its path
-    batch = Batch(ctx, insts, use_graph=True, serial=args.batch_serial, **tuned)
+    from cuot_b200.batch import SCHEDULES
+    batch = Batch(ctx, insts, use_graph=True, schedule=SCHEDULES[args.batch_schedule], **tuned)
     for _ in range(args.warmup):
         batch.run(stream)
         batch.run_plain(stream)
@@ -867,7 +868,7 @@ def run_batch(args):
     # same outputs): step j's input copy runs during step j-1.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     insts2 = [i.input_copy() for i in insts]
-    batch2 = Batch(ctx, insts2, use_graph=True, serial=args.batch_serial, **tuned)
+    batch2 = Batch(ctx, insts2, use_graph=True, schedule=SCHEDULES[args.batch_schedule], **tuned)
     batch2.run(stream)
     batches = [batch, batch2]
     host_in, host_out = [[], []], []
@@ -947,7 +948,7 @@ def run_batch(args):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
         "config": {"workload": args.workload, "what": CONFIG_TEXT[args.workload], "qc_backend": args.qc_backend,
-                   "schedule": "one chain" if args.batch_serial else "concurrent branches", "instances": len(insts),
+                   "schedule": args.batch_schedule, "instances": len(insts),
                    "cots_per_step_per_gpu": cots, "parallelism": f"replicas x{world}",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "plain": {"value": world * cots / (ms_plain / 1e3), "ms_per_step": ms_plain,
@@ -1341,8 +1342,9 @@ def main():
                     help="requests of the served stream reported with mixed64 (0: skip; the full served configuration is 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--batch-serial", action="store_true",
-                    help="batched mix: one chain of launches instead of the concurrent branches (A/B diagnostic)")
+    ap.add_argument("--batch-schedule", default="fork_ferret", choices=["fork_ferret", "serial", "fork_sizes"],
+                    help="batched mix: Ferret branch beside the SOT chain (default), one chain, or every SOT size "
+                         "on its own stream too")
     ap.add_argument("--qc-backend", default="auto", choices=sorted(QC_BACKENDS),
                     help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^22, Karatsuba over it for "
                          "dual LPNs at 2^23 and 2^24, NTT above)")

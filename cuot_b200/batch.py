@@ -16,6 +16,9 @@ from . import _check, _ptr, _stream, load
 
 C = ctypes
 KIND_FERRET, KIND_SOT = 0, 1
+# cuot_batch_config.schedule
+FORK_FERRET, SERIAL, FORK_SIZES = 0, 1, 2
+SCHEDULES = {"fork_ferret": FORK_FERRET, "serial": SERIAL, "fork_sizes": FORK_SIZES}
 
 
 class BatchItem(C.Structure):
@@ -29,7 +32,7 @@ class BatchItem(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("pprf_threads", C.c_int), ("ctas_per_sm", C.c_int), ("lpn_rows_per_task", C.c_int),
-                ("qc_planes_per_pass", C.c_int), ("use_graph", C.c_int), ("serial", C.c_int)]
+                ("qc_planes_per_pass", C.c_int), ("use_graph", C.c_int), ("schedule", C.c_int)]
 
 
 class Instance:
@@ -97,11 +100,11 @@ class Instance:
 
 class Batch:
     def __init__(self, ctx, instances, pprf_threads: int = 0, ctas_per_sm: int = 0, lpn_rows_per_task: int = 0,
-                 qc_planes_per_pass: int = 0, use_graph: bool = True, serial: bool = False):
+                 qc_planes_per_pass: int = 0, use_graph: bool = True, schedule: int = 0):
         self.lib, self.ctx, self.instances = load(), ctx, list(instances)
         arr = (BatchItem * len(self.instances))(*[i.item() for i in self.instances])
         cfg = BatchConfig(pprf_threads, ctas_per_sm, lpn_rows_per_task, qc_planes_per_pass, int(use_graph),
-                          int(serial))
+                          int(schedule))
         h = C.c_void_p()
         _check(self.lib.cuot_batch_create(ctx.h, arr, C.c_int(len(self.instances)), C.byref(cfg), C.byref(h)),
                "cuot_batch_create")

@@ -12,14 +12,17 @@
 //     of rows of every instance, both roles of a row from one index
 //     computation (the two roles share the public LPN seed).
 //   SOT branch: the persistent PPRF launches over the SOT sender and then
-//     receiver trees; then each transform size on its own stream (sizes that
-//     share per-size FFT state, qc_lane, on one): blocks into the encode's
-//     layout, transform passes that span every instance of that size (each
-//     with its own A_hat), back to blocks, and the receivers' choice-bit
-//     encodes.
-// Independent work thus shares the GPU: the Ferret chain and the small
-// sizes' passes fill the SMs that the large sizes' passes leave idle.
-// cfg.serial runs the same launches as one chain on the caller's stream.
+//     receiver trees; then per transform size, largest first: blocks into the
+//     encode's layout, transform passes that span every instance of that
+//     size (each with its own A_hat), back to blocks, and the receivers'
+//     choice-bit encodes.
+// cfg.schedule: CUOT_BATCH_FORK_FERRET (default) runs the Ferret branch on a
+// stream of its own beside the SOT branch; CUOT_BATCH_FORK_SIZES also puts
+// each transform size on its own stream (sizes that share per-size FFT
+// state, qc_lane, on one); CUOT_BATCH_SERIAL runs every launch in one chain
+// on the caller's stream.  Measured on B200 (the 64-instance mix of
+// log2 n in [16, 22]): one chain 92.0 ms, sizes side by side 99.0 ms (the
+// sizes' transform passes evict each other's intermediate from L2).
 // The whole program is captured into a CUDA graph on the first run.
 // Spin-free: work queues are atomic counters, reset by a memset node.
 #include <algorithm>
@@ -101,7 +104,8 @@ struct LpnBatchArgs {
   const uint32_t *t0;
 };
 
-__global__ void __launch_bounds__(kLpnThreads, 3) lpn_batch_kernel(LpnBatchArgs b) {
+// Two CTAs per SM: a dual-role group keeps both roles' accumulators live.
+__global__ void __launch_bounds__(kLpnThreads, 2) lpn_batch_kernel(LpnBatchArgs b) {
   extern __shared__ __align__(16) uint32_t smem_tab[];
   __shared__ __align__(16) LpnArgs s_job;
   __shared__ uint32_t s_task;
@@ -118,16 +122,11 @@ __global__ void __launch_bounds__(kLpnThreads, 3) lpn_batch_kernel(LpnBatchArgs 
     for (int i = threadIdx.x; i < int(sizeof(LpnArgs) / 4); i += blockDim.x)
       reinterpret_cast<uint32_t *>(&s_job)[i] = src[i];
     __syncthreads();
-    const LpnArgs &a = s_job;
-    const bool dual = a.kk2 != nullptr;
+    const LpnArgs &a = s_job;  // every job holds both roles (make_lpn_job)
     for (int64_t w = tk.w0 + threadIdx.x; w < tk.w1; w += blockDim.x) {
       if (w < a.ngroups) {
-        if (a.d == 10) {
-          if (dual) lpn_group4<10, true>(a, T, a.g0 + w);
-          else lpn_group4<10>(a, T, a.g0 + w);
-        } else {
-          lpn_group4_dyn(a, T, a.g0 + w);
-        }
+        if (a.d == 10) lpn_group4<10, true>(a, T, a.g0 + w);
+        else lpn_group4_dyn(a, T, a.g0 + w);
       } else {
         lpn_row1(a, T, a.j0 + (w - a.ngroups));
       }
@@ -335,7 +334,7 @@ int ev_fail() {
 // Enqueues the batched program on `st`.  ev (optional, diagnostic): 5 events
 // recorded before the sender PPRF, the receiver PPRF, the LPN, the SOT
 // encodes, and at the end; with ev the program runs as one chain (phases in
-// order), as it does with cfg.serial.
+// order), as it does with CUOT_BATCH_SERIAL.
 int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
   const unsigned long long k0 = cuot_launch_count();
   auto mark = [&](int i) {
@@ -345,7 +344,8 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
     cudaGetLastError();
     return fail(CUOT_ECUDA, "counter reset failed");
   }
-  if (ev || b->cfg.serial) {
+  const int sched = ev ? CUOT_BATCH_SERIAL : b->cfg.schedule;
+  if (sched == CUOT_BATCH_SERIAL) {
     int launches = 0;
     mark(0);
     launches += pprf_launch(b, b->send[kBrSot], kBrSot, st);
@@ -377,17 +377,23 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
     // SOT branch: PPRFs on the caller's stream, then the lanes side by side
     CUOT_TRY(launch_status(pprf_launch(b, b->send[kBrSot], kBrSot, st) +
                            pprf_launch(b, b->recv[kBrSot], kBrSot, st)));
-    if (cudaEventRecord(E[kEvSotPprf], st) != cudaSuccess) return ev_fail();
-    for (size_t j = 1; j < b->lanes.size(); j++) {
-      cudaStream_t sl = b->streams[j];
-      if (cudaStreamWaitEvent(sl, E[kEvSotPprf], 0) != cudaSuccess) return ev_fail();
-      CUOT_TRY(enqueue_lane(b, b->lanes[j], sl));
-      if (cudaEventRecord(E[kEvLane0 + j], sl) != cudaSuccess) return ev_fail();
+    const bool sizes = sched == CUOT_BATCH_FORK_SIZES;
+    if (sizes) {
+      if (cudaEventRecord(E[kEvSotPprf], st) != cudaSuccess) return ev_fail();
+      for (size_t j = 1; j < b->lanes.size(); j++) {
+        cudaStream_t sl = b->streams[j];
+        if (cudaStreamWaitEvent(sl, E[kEvSotPprf], 0) != cudaSuccess) return ev_fail();
+        CUOT_TRY(enqueue_lane(b, b->lanes[j], sl));
+        if (cudaEventRecord(E[kEvLane0 + j], sl) != cudaSuccess) return ev_fail();
+      }
+      if (!b->lanes.empty()) CUOT_TRY(enqueue_lane(b, b->lanes[0], st));
+    } else {
+      for (const auto &lane : b->lanes) CUOT_TRY(enqueue_lane(b, lane, st));
     }
-    if (!b->lanes.empty()) CUOT_TRY(enqueue_lane(b, b->lanes[0], st));
     if (fer && cudaStreamWaitEvent(st, E[kEvFerret], 0) != cudaSuccess) return ev_fail();
-    for (size_t j = 1; j < b->lanes.size(); j++)
-      if (cudaStreamWaitEvent(st, E[kEvLane0 + j], 0) != cudaSuccess) return ev_fail();
+    if (sizes)
+      for (size_t j = 1; j < b->lanes.size(); j++)
+        if (cudaStreamWaitEvent(st, E[kEvLane0 + j], 0) != cudaSuccess) return ev_fail();
   }
   b->kernels_per_run = int(cuot_launch_count() - k0);
   return CUOT_OK;
@@ -418,6 +424,8 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
   const int per_sm = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : 3;
   if (b->cfg.pprf_threads != 0 && b->cfg.pprf_threads != 128 && b->cfg.pprf_threads != 256)
     return cleanup(fail(CUOT_EINVAL, "pprf_threads must be 128 or 256"));
+  if (b->cfg.schedule < CUOT_BATCH_FORK_FERRET || b->cfg.schedule > CUOT_BATCH_FORK_SIZES)
+    return cleanup(fail(CUOT_EINVAL, "schedule must be one of CUOT_BATCH_FORK_FERRET / SERIAL / FORK_SIZES"));
   b->pprf_threads = b->cfg.pprf_threads ? b->cfg.pprf_threads : 256;
 
   // ---- per-item device state

@@ -54,9 +54,10 @@ __device__ __forceinline__ Blk mask_lsb(Blk b) {
   return b;
 }
 
-// Shared-memory state of one tree expansion.
+// Shared-memory state of one tree expansion: per-warp level sums (left,
+// right), double-buffered by level parity, and the receiver's path.
 struct PprfSmem {
-  Blk red[2][kPprfThreads / 32];
+  Blk red[2][2][kPprfThreads / 32];
   unsigned long long ap;
 };
 
@@ -66,8 +67,15 @@ struct PprfSmem {
 template <int MODE>
 __device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk *scratch_tree,
                                           const TabRef &T, PprfSmem &sm) {
-  Blk (&red)[2][kPprfThreads / 32] = sm.red;
   unsigned long long &s_ap = sm.ap;
+  // Senders: the sums of level l leave the CTA (global stores by thread 0)
+  // and nothing of them is read back, so one barrier per level suffices,
+  // with the warp partials double-buffered by level parity: thread 0 reads
+  // red[l & 1] before it enters level l + 1, and red[l & 1] is written again
+  // only after the barrier that ends level l + 1.  Receivers patch a node of
+  // the level just written, which the next level reads, so they keep a
+  // second barrier.
+  constexpr bool kSend = MODE == FERRET_SEND || MODE == SOT_SEND;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int h = a.h;
   const uint64_t W = 1ull << h;
@@ -106,6 +114,7 @@ __device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk 
     }
     accL = warp_xor(accL);
     accR = warp_xor(accR);
+    Blk(&red)[2][kPprfThreads / 32] = sm.red[l & 1];
     if (lane == 0) {
       red[0][warp] = accL;
       red[1][warp] = accR;
@@ -174,7 +183,7 @@ __device__ __forceinline__ void pprf_tree(const PprfArgs &a, uint64_t tree, Blk 
         }
       }
     }
-    __syncthreads();
+    if (!kSend) __syncthreads();
   }
 }
 

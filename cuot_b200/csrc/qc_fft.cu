@@ -403,6 +403,14 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
   double2 *xs = sm, *Ts = xs + NT * ld;
   const double2 *T0 = G0 ? T2 : Ts;
   const int r0 = blockIdx.x * NT;
+  if (mode == 0 && threadIdx.x == 0) {
+    // The pointwise product reads this CTA's A_hat rows (NT * N2 contiguous
+    // values, 64 KiB) in the middle of the kernel; start moving them into L2
+    // now, so those reads do not wait for DRAM.
+    const double2 *ahp = static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
+                         (uint64_t(r0) << E2);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ahp), "r"(uint32_t(NT * N2 * 16)) : "memory");
+  }
   if constexpr (G0)
     stage(Ts, T2 + qcf_tw_off(E2, 1), qcf_tw_off(E2, NP - 1) - qcf_tw_off(E2, 1));
   else

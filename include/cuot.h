@@ -344,9 +344,10 @@ int cuot_qc_plan_dual_lpn_r2(cuot_qc_plan *plan, const cuot_block *in_d,
  * deepest trees first --, one over the receivers, one persistent LPN launch
  * over all Ferret rows, both roles of a row from one index computation) and
  * SOT (the same PPRF launches over the SOT trees, then for each transform
- * size, on its own stream, one set of QC transform passes spanning the planes
- * of every instance of that size).  On first run the whole program is
- * captured into a CUDA graph (cfg.use_graph) and replayed afterwards.
+ * size one set of QC transform passes spanning the planes of every instance
+ * of that size; cfg.schedule chooses how the parts overlap).  On first run
+ * the whole program is captured into a CUDA graph (cfg.use_graph) and
+ * replayed afterwards.
  * No counterpart call in the reference, which runs one instance per call
  * (FerretCOT::extend, ferret_cot.hpp:80-91; SOT roles, silent/roles.h).
  * Each item produces v (sender) and w (receiver) with w = v except on the
@@ -385,10 +386,15 @@ typedef struct {
   int lpn_rows_per_task;   /* LPN work-queue granularity, multiple of 4 (0: 65536) */
   int qc_planes_per_pass;  /* planes per QC pass (0: 512 MiB of intermediate) */
   int use_graph;           /* capture into a CUDA graph on first run */
-  int serial;              /* 1: every launch in one chain on the caller's
-                              stream; 0: the Ferret branch and each SOT size
-                              run side by side (forked and joined) */
+  int schedule;            /* CUOT_BATCH_FORK_FERRET (0, default): the Ferret
+                              branch beside the SOT chain; CUOT_BATCH_SERIAL:
+                              every launch in one chain on the caller's
+                              stream; CUOT_BATCH_FORK_SIZES: the Ferret branch
+                              and each SOT transform size side by side */
 } cuot_batch_config;
+#define CUOT_BATCH_FORK_FERRET 0
+#define CUOT_BATCH_SERIAL 1
+#define CUOT_BATCH_FORK_SIZES 2
 
 typedef struct cuot_batch cuot_batch;
 /* Validates the items, allocates the batch's device state and transforms

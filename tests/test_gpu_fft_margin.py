@@ -57,7 +57,7 @@ def test_fft_rounding_margin_below_bound(e, akind, pkind):
         ctx.sot_dual_lpn(a, io, n)
         torch.cuda.synchronize()
         m = ctx.qc_fft_margin()
-        print(f"\nn=2^{e} a={akind} planes={pkind}: max |v - round(v)| = {m:.4f} (bound {BOUND[e]})")
+        print(f"\nn=2^{e} a={akind} planes={pkind}: max |v - round(v)| = {m:.3g} (bound {BOUND[e]})")
         assert 0.0 <= m < BOUND[e]
         # the read reset the record: a second encode (fresh planes of the same
         # kind) starts from zero and stays below the bound too

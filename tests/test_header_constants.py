@@ -33,3 +33,10 @@ def test_request_states():
     d = defines()
     for i, s in enumerate(serve.STATUS):
         assert d["CUOT_REQ_" + s.upper()] == i, s
+
+
+def test_batch_schedules():
+    d = defines()
+    assert batch.FORK_FERRET == d["CUOT_BATCH_FORK_FERRET"]
+    assert batch.SERIAL == d["CUOT_BATCH_SERIAL"]
+    assert batch.FORK_SIZES == d["CUOT_BATCH_FORK_SIZES"]
