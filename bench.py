@@ -276,10 +276,15 @@ class Instance:
 # backend (gather, 3 transform passes, scatter per role); the NTT figure is
 # the same workload with the NTT backend, which scales the SOT encodes of
 # larger n.
+# sot_n22: the three transform passes captured at n = 2^22 (252.9 MB per
+# transform, 32 transforms per role, both roles; profiles/qc_fft_sot_n22.md)
+# plus gather and scatter scaled from the n = 2^20 capture (4 x 16.8 MB per
+# role there, x 4 here).
 NCU_TRAFFIC_PER_STEP = {
     "ferret_b13:lpn": 570.44e6,
     "sot_n20:dual_lpn": 4050.8e6,
     "sot_n20_ntt:dual_lpn": 3990.2e6,
+    "sot_n22:dual_lpn": 2 * (32 * 252.9e6 + 4 * 4 * 16.8e6),
 }
 
 QC_FFT_MAX_LOG_N = 22  # the fp64 FFT encodes n <= 2^22 (exactness bound)
@@ -915,20 +920,24 @@ def run_batch(args):
     peaks, peak_kind = measured_peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
     # traffic: the batch is too large for a multi-metric ncu capture; the SOT
-    # encode runs the same kernels as sot_n20 (FFT up to 2^22, Karatsuba over
-    # it at 2^23 and 2^24, NTT above),
-    # whose captured DRAM bytes per COT (both roles) scale it; other stages
-    # have no capture (null)
+    # encode runs the same kernels as the single-instance sot_n20 / sot_n22
+    # lines (FFT up to 2^22, Karatsuba over 2^22 FFTs at 2^23 and 2^24, NTT
+    # above), whose captured DRAM bytes per COT (both roles) scale it: the
+    # 2^22 capture for the 1024 x 4096 split of 2^22 (and the Karatsuba
+    # leaves), the 2^20 capture below; other stages have no capture (null)
     traffic = None
     if dom == "sot_encode":
         fft_cot = NCU_TRAFFIC_PER_STEP["sot_n20:dual_lpn"] / (1 << 20)  # FFT dual LPN, both roles
+        fft22_cot = NCU_TRAFFIC_PER_STEP["sot_n22:dual_lpn"] / (1 << 22)
         ntt_cot = NCU_TRAFFIC_PER_STEP["sot_n20_ntt:dual_lpn"] / (1 << 20)
         traffic = 0.0
         for i in insts:
             if i.kind == KIND_FERRET:
                 continue
-            leaves = qc_leaves(i.n.bit_length() - 1)
-            traffic += fft_cot * leaves * min(i.n, 1 << QC_FFT_MAX_LOG_N) if leaves else i.n * ntt_cot
+            lg = i.n.bit_length() - 1
+            leaves = qc_leaves(lg)
+            per = fft22_cot if lg >= QC_FFT_MAX_LOG_N else fft_cot
+            traffic += per * leaves * min(i.n, 1 << QC_FFT_MAX_LOG_N) if leaves else i.n * ntt_cot
     props = torch.cuda.get_device_properties(local)
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
     aes_peak = props.multi_processor_count * 32 * mhz * 1e6 / 160
@@ -959,9 +968,11 @@ def run_batch(args):
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": alg[dom],
-                     "basis": "stage totals per step (both roles); traffic scaled from the sot_n20 ncu captures: "
-                              "3,863 DRAM bytes per COT for FFT sizes, 3^L times a 2^22 FFT dual LPN for the "
-                              "Karatsuba sizes, 3,805 per COT for NTT sizes (cold cache per kernel)"},
+                     "basis": "stage totals per step (both roles); traffic scaled from ncu captures of the "
+                              "single-instance lines (cold cache per kernel): n = 2^22 (profiles/"
+                              "qc_fft_sot_n22.md) 3,987 DRAM bytes per COT for the 2^22 instances and, 3^L "
+                              "times, the Karatsuba leaves; n = 2^20 3,863 per COT for smaller FFT sizes; "
+                              "3,805 per COT for NTT sizes"},
         "aes_roofline": aes,
         "qc_transform": qc_transform_report([i.n for i in insts if i.kind != KIND_FERRET], stages["sot_encode"]),
         "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
@@ -1342,9 +1353,9 @@ def main():
                     help="requests of the served stream reported with mixed64 (0: skip; the full served configuration is 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--batch-schedule", default="fork_ferret", choices=["fork_ferret", "serial", "fork_sizes"],
-                    help="batched mix: Ferret branch beside the SOT chain (default), one chain, or every SOT size "
-                         "on its own stream too")
+    ap.add_argument("--batch-schedule", default="serial", choices=["serial", "fork_ferret", "fork_sizes"],
+                    help="batched mix: one chain (default), the Ferret branch beside the SOT chain, or every SOT "
+                         "size on its own stream too")
     ap.add_argument("--qc-backend", default="auto", choices=sorted(QC_BACKENDS),
                     help="transform of the exact QC encode (auto: fp64 FFT for n <= 2^22, Karatsuba over it for "
                          "dual LPNs at 2^23 and 2^24, NTT above)")

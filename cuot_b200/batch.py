@@ -17,8 +17,8 @@ from . import _check, _ptr, _stream, load
 C = ctypes
 KIND_FERRET, KIND_SOT = 0, 1
 # cuot_batch_config.schedule
-FORK_FERRET, SERIAL, FORK_SIZES = 0, 1, 2
-SCHEDULES = {"fork_ferret": FORK_FERRET, "serial": SERIAL, "fork_sizes": FORK_SIZES}
+SERIAL, FORK_FERRET, FORK_SIZES = 0, 1, 2
+SCHEDULES = {"serial": SERIAL, "fork_ferret": FORK_FERRET, "fork_sizes": FORK_SIZES}
 
 
 class BatchItem(C.Structure):

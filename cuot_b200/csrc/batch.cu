@@ -1,7 +1,7 @@
 // batch.cu -- the batched engine: many OT-extension instances (Ferret and
 // SOT, uneven n and depth, both roles) as one device program.
 //
-// Two independent branches, forked from the caller's stream and joined back:
+// Two independent branches (run as one chain by default, see cfg.schedule):
 //   Ferret branch: a persistent PPRF launch over every Ferret sender tree
 //     (each CTA pulls (instance, tree) tasks from an atomic work counter,
 //     deepest trees first, and expands one whole tree per task with
@@ -16,13 +16,16 @@
 //     encode's layout, transform passes that span every instance of that
 //     size (each with its own A_hat), back to blocks, and the receivers'
 //     choice-bit encodes.
-// cfg.schedule: CUOT_BATCH_FORK_FERRET (default) runs the Ferret branch on a
+// cfg.schedule: CUOT_BATCH_SERIAL (default) runs every launch in one chain
+// on the caller's stream; CUOT_BATCH_FORK_FERRET runs the Ferret branch on a
 // stream of its own beside the SOT branch; CUOT_BATCH_FORK_SIZES also puts
 // each transform size on its own stream (sizes that share per-size FFT
-// state, qc_lane, on one); CUOT_BATCH_SERIAL runs every launch in one chain
-// on the caller's stream.  Measured on B200 (the 64-instance mix of
-// log2 n in [16, 22]): one chain 92.0 ms, sizes side by side 99.0 ms (the
-// sizes' transform passes evict each other's intermediate from L2).
+// state, qc_lane, on one).  Measured on B200 (the 64-instance mix of
+// log2 n in [16, 22], 10 graph replays each): one chain 86.1 ms, Ferret
+// beside SOT 88.7 ms, sizes side by side 97.3 ms.  Every part already fills
+// the GPU; run together, the persistent PPRF / LPN CTAs take SMs and
+// shared memory from the FFT passes, and the sizes' transform passes evict
+// each other's intermediate from L2.
 // The whole program is captured into a CUDA graph on the first run.
 // Spin-free: work queues are atomic counters, reset by a memset node.
 #include <algorithm>
