@@ -427,8 +427,9 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
   const int per_sm = b->cfg.ctas_per_sm > 0 ? b->cfg.ctas_per_sm : 3;
   if (b->cfg.pprf_threads != 0 && b->cfg.pprf_threads != 128 && b->cfg.pprf_threads != 256)
     return cleanup(fail(CUOT_EINVAL, "pprf_threads must be 128 or 256"));
-  if (b->cfg.schedule < CUOT_BATCH_FORK_FERRET || b->cfg.schedule > CUOT_BATCH_FORK_SIZES)
-    return cleanup(fail(CUOT_EINVAL, "schedule must be one of CUOT_BATCH_FORK_FERRET / SERIAL / FORK_SIZES"));
+  if (b->cfg.schedule != CUOT_BATCH_SERIAL && b->cfg.schedule != CUOT_BATCH_FORK_FERRET &&
+      b->cfg.schedule != CUOT_BATCH_FORK_SIZES)
+    return cleanup(fail(CUOT_EINVAL, "schedule must be one of CUOT_BATCH_SERIAL / FORK_FERRET / FORK_SIZES"));
   b->pprf_threads = b->cfg.pprf_threads ? b->cfg.pprf_threads : 256;
 
   // ---- per-item device state

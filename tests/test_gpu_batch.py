@@ -9,7 +9,9 @@ import oracle
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
-from cuot_b200.batch import KIND_FERRET, KIND_SOT, Batch, Instance, mixed_workload  # noqa: E402
+from cuot_b200 import CuotError  # noqa: E402
+from cuot_b200.batch import (FORK_FERRET, FORK_SIZES, KIND_FERRET, KIND_SOT, SERIAL, Batch, Instance,  # noqa: E402
+                             mixed_workload)
 
 
 def oracle_outputs(inst):
@@ -32,12 +34,16 @@ def snapshot(insts):
              None if i.kind == KIND_FERRET else i.cbits.cpu().numpy().view(np.uint64).copy()) for i in insts]
 
 
-def test_mixed_batch_equals_plain_and_oracle(ctx):
+@pytest.mark.parametrize("schedule", [SERIAL, FORK_FERRET, FORK_SIZES])
+def test_mixed_batch_equals_plain_and_oracle(ctx, schedule):
+    """Every schedule of the batched program (one chain; the Ferret branch
+    beside the SOT chain; every SOT size on its own stream) gives the same
+    outputs."""
     specs = [(KIND_FERRET, 8, 10, 1000), (KIND_SOT, 4, 10, 0), (KIND_FERRET, 3, 12, 77), (KIND_SOT, 16, 10, 0),
              (KIND_FERRET, 64, 10, 8192), (KIND_SOT, 2, 11, 0), (KIND_FERRET, 5, 1, 9), (KIND_SOT, 1, 12, 0)]
     insts = [Instance(ctx, kd, t, h, 100 + i, k=k) for i, (kd, t, h, k) in enumerate(specs)]
     stream = torch.cuda.Stream()
-    b = Batch(ctx, insts, use_graph=True)
+    b = Batch(ctx, insts, use_graph=True, schedule=schedule)
     b.run(stream)        # captures the graph and runs it
     b.run(stream)        # replays: a second run must give the same outputs
     got = snapshot(insts)
@@ -96,4 +102,18 @@ def test_large_sot_batch_equals_plain_and_is_a_cot(ctx):
             assert not diff[~cbits].any()
             assert (diff[cbits] == inst.delta).all()
             assert 0.4 < cbits.mean() < 0.6
+    b.close()
+
+
+def test_unknown_schedule_is_rejected(ctx):
+    insts = [Instance(ctx, KIND_FERRET, 4, 8, 500, k=300), Instance(ctx, KIND_SOT, 2, 10, 501)]
+    for bad in (-1, 3):
+        with pytest.raises(CuotError):
+            Batch(ctx, insts, use_graph=True, schedule=bad)
+    b = Batch(ctx, insts, use_graph=True, schedule=SERIAL)  # the context stays usable
+    b.run(torch.cuda.Stream())
+    torch.cuda.synchronize()
+    for inst in insts:
+        ev, ew, _ = oracle_outputs(inst)
+        assert np.array_equal(inst.v.cpu().numpy(), ev) and np.array_equal(inst.w.cpu().numpy(), ew)
     b.close()
