@@ -273,12 +273,19 @@ __device__ __forceinline__ void middle_passes(double2 *xs, const double2 *T) {
 }
 
 // w_n^(j2 * k1) for the CTA's column c and k1 = rev_e1(r), from the column's
-// two factor tables in shared memory.
-template <int E1>
-__device__ __forceinline__ double2 fourstep_w(const double2 *fs, int c, int r) {
+// two factor tables in shared memory (low lo bits of k1, high bits), for the
+// 2^K rows r = i0 + m (m < 2^K) of one item of the last column pass (i0 a
+// multiple of 2^K): k1 = rev(i0) | rev_K(m) << (E1 - K), and since E1 - K >= lo
+// every row shares the low table entry, read once.
+template <int E1, int K>
+__device__ __forceinline__ void fourstep_ws(const double2 *fs, int c, int i0, double2 (&w)[1 << K]) {
   constexpr int lo = qcf_fs_lo(E1), W = qcf_fs_ld(E1);
-  const int k1 = __brev(r) >> (32 - E1);
-  return cmul(fs[c * W + (k1 & ((1 << lo) - 1))], fs[c * W + (1 << lo) + (k1 >> lo)]);
+  static_assert(E1 - K >= lo, "the rows of an item share the low factor");
+  const int k10 = __brev(i0) >> (32 - E1);
+  const double2 wl = fs[c * W + (k10 & ((1 << lo) - 1))];
+  const double2 *hi = fs + c * W + (1 << lo) + (k10 >> lo);
+#pragma unroll
+  for (int m = 0; m < (1 << K); m++) w[m] = cmul(wl, hi[(__brev(m) >> (32 - K)) << (E1 - K - lo)]);
 }
 
 __device__ __forceinline__ void stage(double2 *dst, const double2 *src, int cnt) {
@@ -375,11 +382,10 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
 #pragma unroll
       for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + spos<E1, KC>(i0 + m)];
       dif_regs<Q::K>(x);
+      double2 fw[Q::R];
+      fourstep_ws<E1, Q::K>(fss, c, i0, fw);
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) {
-        const int r = i0 + m;
-        Yp[(uint64_t(r) << e2) + c0 + c] = cmul(x[m], fourstep_w<E1>(fss, c, r));
-      }
+      for (int m = 0; m < Q::R; m++) Yp[(uint64_t(i0 + m) << e2) + c0 + c] = cmul(x[m], fw[m]);
     }
   }
 }
@@ -545,12 +551,12 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
     for (int it = threadIdx.x; it < KC * Q::items; it += blockDim.x) {
       const int c = it & (KC - 1), w = it / KC;
       const int i0 = Q::first(w);
-      double2 x[Q::R];
+      double2 x[Q::R], fw[Q::R];
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) {
-        const int r = i0 + m;
-        x[m] = cmulc(Yp[(uint64_t(r) << e2) + c0 + c], fourstep_w<E1>(fss, c, r));
-      }
+      for (int m = 0; m < Q::R; m++) x[m] = Yp[(uint64_t(i0 + m) << e2) + c0 + c];
+      fourstep_ws<E1, Q::K>(fss, c, i0, fw);
+#pragma unroll
+      for (int m = 0; m < Q::R; m++) x[m] = cmulc(x[m], fw[m]);
       dit_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) xs[c * ld + spos<E1, KC>(i0 + m)] = x[m];

@@ -2,42 +2,172 @@
 // gpu/gpu_matrix.cu:95-121 with bit_transposer, gpu/gpu_ops.cu:31-70):
 // output row (c - col_lo) bit r = input row r bit c, bits LSB-first.
 //
-// Fast paths (the two SOT shapes):
-//   blocks -> planes: rows of 16 bytes, plane range multiple of 32.
-//   planes -> blocks: up to 128 rows (planes) of n bits -> n rows.
-// Both move 32x32 bit tiles with a five-step warp-shuffle transpose (one
-// word per lane), stage through padded shared memory (stride 33 words, no
-// bank conflicts) and read/write HBM with coalesced 16-byte or 128-byte
-// accesses.  Any other shape uses a byte-granular 8x8 kernel.
+// Fast paths (the SOT shapes):
+//   blocks -> all 128 planes, and 128 planes -> blocks: 16-byte global
+//     accesses on both sides, plane rows staged in an XOR-swizzled shared
+//     tile (tr_blocks_to_planes128, tr_planes128_to_blocks);
+//   blocks -> any multiple of 32 planes, and up to 128 planes -> blocks:
+//     padded shared tile (stride 33 words), 4-byte plane-row accesses.
+// All move 32x32 bit tiles with a five-stage warp-shuffle transpose (one word
+// per lane).  Any other shape, or a pointer not aligned for the fast path's
+// accesses, uses a byte-granular 8x8 kernel.
 #include "ctx.cuh"
 
 namespace cuot {
 
-// Lane i holds row i of a 32x32 bit tile (bit j = column j).  Returns the
-// word of column `lane` (bit i = row i).
-__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
-  const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+// Per-lane constants of warp_transpose32: byte-permute selectors of the
+// 16- and 8-bit stages, rotate amounts and keep-masks of the 4-, 2- and
+// 1-bit stages.
+struct TrLane {
+  uint32_t sel16, sel8, amt[3], keep[3];
+};
+__device__ __forceinline__ TrLane tr_lane(int lane) {
+  TrLane t;
+  t.sel16 = (lane & 16) ? 0x3276u : 0x5410u;  // (y.hi16, x.hi16) : (x.lo16, y.lo16) as (hi, lo)
+  t.sel8 = (lane & 8) ? 0x3715u : 0x6240u;
+  const uint32_t m[3] = {0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
 #pragma unroll
-  for (int k = 0; k < 5; k++) {
-    const int s = 16 >> k;
-    const uint32_t m = masks[k];
-    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, s);
-    if (lane & s) x = (x & ~m) | ((y >> s) & m);
-    else x = (x & m) | ((y << s) & ~m);
+  for (int k = 0; k < 3; k++) {
+    const int s = 4 >> k;
+    const bool up = lane & s;
+    t.amt[k] = up ? 32 - s : s;
+    t.keep[k] = up ? ~m[k] : m[k];
+  }
+  return t;
+}
+
+// Lane i holds row i of a 32x32 bit tile (bit j = column j).  Returns the
+// word of column `lane` (bit i = row i).  Five exchange stages with the lane
+// 16, 8, 4, 2, 1 apart: a lane keeps the half of its word whose column bit
+// equals its own lane bit and takes the other half from its partner.  The
+// 16- and 8-bit stages are one byte permute each; the others rotate the
+// partner's word by s (lower lane) or 32 - s (upper lane), which lands the
+// wanted half in place either way, and merge by a bit-select.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, const TrLane &t) {
+  uint32_t y = __shfl_xor_sync(0xffffffffu, x, 16);
+  x = __byte_perm(x, y, t.sel16);
+  y = __shfl_xor_sync(0xffffffffu, x, 8);
+  x = __byte_perm(x, y, t.sel8);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    y = __shfl_xor_sync(0xffffffffu, x, 4 >> k);
+    const uint32_t r = __funnelshift_l(y, y, t.amt[k]);
+    x = (x & t.keep[k]) | (r & ~t.keep[k]);
   }
   return x;
 }
 
 constexpr int kTrThreads = 256;     // 8 warps
+
+// 128-plane fast paths.  A CTA moves kTrG groups of 32 rows: 16 * 32 * kTrG
+// bytes of blocks <-> 128 plane rows of 4 * kTrG bytes.  The plane rows are
+// staged in shared memory as [plane][kTrG / 4 chunks of 16 bytes] with chunk
+// c of plane p at c ^ (p & 7): a warp storing one chunk of 32 planes and a
+// warp reading 8 consecutive chunks of a plane both hit 8 distinct 16-byte
+// bank groups per quarter-warp (conflict-free).  Global memory is read and
+// written in 16-byte words only.
+constexpr int kTrG = 32;
+constexpr int kTrCh = kTrG / 4;                   // 16-byte chunks per plane row
+constexpr int kTrCpw = kTrCh / (kTrThreads / 32);  // chunks per warp
+static_assert(kTrCpw >= 1 && kTrCh >= 8, "tile shape");
+
+// blocks -> planes, all 128 planes.  in: rows x 16 bytes (rows % 128 == 0).
+// out: 128 rows of rows / 8 bytes.
+__global__ void __launch_bounds__(kTrThreads) tr_blocks_to_planes128(const uint4 *__restrict__ in, uint64_t rows,
+                                                                     uint4 *__restrict__ out) {
+  __shared__ uint4 st[128 * kTrCh];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const TrLane tl = tr_lane(lane);
+  const uint64_t ngroups = rows / 32;
+  const uint64_t g0 = uint64_t(blockIdx.x) * kTrG;
+  const int gvalid = int(ngroups - g0 < uint64_t(kTrG) ? ngroups - g0 : uint64_t(kTrG));  // multiple of 4
+  // the warp's 4 * kTrCpw row groups are all loaded before any is transposed
+  uint4 v[4 * kTrCpw];
+#pragma unroll
+  for (int c = 0; c < kTrCpw; c++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int gg = (warp * kTrCpw + c) * 4 + j;
+      v[c * 4 + j] = gg < gvalid ? __ldcs(in + (g0 + gg) * 32 + lane) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+  for (int c = 0; c < kTrCpw; c++) {
+    const int ch = warp * kTrCpw + c;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uint32_t o[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint4 &x = v[c * 4 + j];
+        o[j] = warp_transpose32(q == 0 ? x.x : q == 1 ? x.y : q == 2 ? x.z : x.w, tl);
+      }
+      const int p = q * 32 + lane;
+      st[p * kTrCh + (ch ^ (p & 7))] = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+  }
+  __syncthreads();
+  const uint64_t row4 = rows / 128;  // 16-byte words per plane row
+  for (int i = threadIdx.x; i < 128 * kTrCh; i += kTrThreads) {
+    const int p = i / kTrCh, ch = i % kTrCh;
+    if (4 * ch < gvalid) out[uint64_t(p) * row4 + g0 / 4 + ch] = st[p * kTrCh + (ch ^ (p & 7))];
+  }
+}
+
+// planes -> blocks, 128 planes.  in: 128 rows of in_row4 16-byte words, of
+// which the first ncols / 128 are read (ncols % 128 == 0).  out: ncols rows of
+// 16 bytes.
+__global__ void __launch_bounds__(kTrThreads) tr_planes128_to_blocks(const uint4 *__restrict__ in, uint64_t ncols,
+                                                                     uint64_t in_row4, uint4 *__restrict__ out) {
+  __shared__ uint4 st[128 * kTrCh];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const TrLane tl = tr_lane(lane);
+  const uint64_t ngroups = ncols / 32;
+  const uint64_t g0 = uint64_t(blockIdx.x) * kTrG;
+  const int gvalid = int(ngroups - g0 < uint64_t(kTrG) ? ngroups - g0 : uint64_t(kTrG));  // multiple of 4
+  constexpr int kLd = 128 * kTrCh / kTrThreads;
+  uint4 v[kLd];
+#pragma unroll
+  for (int j = 0; j < kLd; j++) {
+    const int i = threadIdx.x + j * kTrThreads, p = i / kTrCh, ch = i % kTrCh;
+    v[j] = 4 * ch < gvalid ? __ldcs(in + uint64_t(p) * in_row4 + g0 / 4 + ch) : make_uint4(0, 0, 0, 0);
+  }
+#pragma unroll
+  for (int j = 0; j < kLd; j++) {
+    const int i = threadIdx.x + j * kTrThreads, p = i / kTrCh, ch = i % kTrCh;
+    st[p * kTrCh + (ch ^ (p & 7))] = v[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < kTrCpw; c++) {
+    const int ch = warp * kTrCpw + c;
+    if (4 * ch >= gvalid) break;
+    uint32_t o[4][4];  // [row group j][plane word q]
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int p = q * 32 + lane;
+      const uint4 x = st[p * kTrCh + (ch ^ (p & 7))];
+      o[0][q] = warp_transpose32(x.x, tl);
+      o[1][q] = warp_transpose32(x.y, tl);
+      o[2][q] = warp_transpose32(x.z, tl);
+      o[3][q] = warp_transpose32(x.w, tl);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      out[(g0 + ch * 4 + j) * 32 + lane] = make_uint4(o[j][0], o[j][1], o[j][2], o[j][3]);
+  }
+}
+
 constexpr int kTrGroups = 32;       // row groups of 32 rows per CTA (128 B of each plane row)
 constexpr int kTrStride = kTrGroups + 1;
 
-// blocks -> planes.  in: rows x 16 bytes.  out: nplanes rows of rows/8 bytes.
+// blocks -> planes, any multiple of 32 planes from col_lo.  in: rows x 16
+// bytes.  out: nplanes rows of rows/8 bytes.
 __global__ void __launch_bounds__(kTrThreads) tr_blocks_to_planes(
     const uint4 *__restrict__ in, uint64_t rows, int col_lo, int nplanes,
     uint32_t *__restrict__ out) {
   __shared__ uint32_t st[128 * kTrStride];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const TrLane tl = tr_lane(lane);
   const uint64_t ngroups = rows / 32;
   const uint64_t g0 = uint64_t(blockIdx.x) * kTrGroups;
   const int wlo = col_lo / 32, nw = nplanes / 32;
@@ -57,7 +187,7 @@ __global__ void __launch_bounds__(kTrThreads) tr_blocks_to_planes(
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       if (q < wlo || q >= wlo + nw) continue;
-      const uint32_t col = warp_transpose32(w[q], lane);
+      const uint32_t col = warp_transpose32(w[q], tl);
       st[((q - wlo) * 32 + lane) * kTrStride + gg] = col;
     }
   }
@@ -71,13 +201,15 @@ __global__ void __launch_bounds__(kTrThreads) tr_blocks_to_planes(
   }
 }
 
-// planes -> blocks.  in: nrows (<= 128, multiple of 32) rows of ncols bits.
-// out: ncols rows of nrows/8 bytes.
+// planes -> blocks.  in: nrows (<= 128, multiple of 32) rows of in_row_words
+// 32-bit words, of which the first ncols bits are read.  out: ncols rows of
+// nrows/8 bytes.
 __global__ void __launch_bounds__(kTrThreads) tr_planes_to_blocks(
     const uint32_t *__restrict__ in, int nrows, uint64_t ncols, uint64_t in_row_words,
     uint32_t *__restrict__ out) {
   __shared__ uint32_t st[128 * kTrStride];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const TrLane tl = tr_lane(lane);
   const uint64_t ngroups = ncols / 32;
   const uint64_t g0 = uint64_t(blockIdx.x) * kTrGroups;
   const int gvalid = int(ngroups - g0 < uint64_t(kTrGroups) ? ngroups - g0 : uint64_t(kTrGroups));
@@ -105,7 +237,7 @@ __global__ void __launch_bounds__(kTrThreads) tr_planes_to_blocks(
     uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (q < nq) w[q] = warp_transpose32(st[(q * 32 + lane) * kTrStride + gg], lane);
+      if (q < nq) w[q] = warp_transpose32(st[(q * 32 + lane) * kTrStride + gg], tl);
     const uint64_t row = (g0 + gg) * 32 + lane;
     if (nq == 4) {
       reinterpret_cast<uint4 *>(out)[row] = make_uint4(w[0], w[1], w[2], w[3]);
@@ -138,10 +270,28 @@ __global__ void tr_generic(const uint8_t *__restrict__ in, uint64_t rows, uint64
   }
 }
 
+static bool aligned(const void *p, uintptr_t a) { return reinterpret_cast<uintptr_t>(p) % a == 0; }
+
 int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t col_lo,
                      uint64_t col_hi, void *out, cudaStream_t st) {
   const uint64_t ncols = col_hi - col_lo;
-  if (row_bytes == 16 && rows % 32 == 0 && col_lo % 32 == 0 && ncols % 32 == 0 && ncols > 0) {
+  if (row_bytes == 16 && rows % 128 == 0 && col_lo == 0 && ncols == 128 && aligned(in, 16) && aligned(out, 16)) {
+    const uint64_t grid = (rows / 32 + kTrG - 1) / kTrG;
+    if (grid > 0x7fffffffull) return fail(CUOT_EINVAL, "too many rows");
+    tr_blocks_to_planes128<<<unsigned(grid), kTrThreads, 0, st>>>(static_cast<const uint4 *>(in), rows,
+                                                                   static_cast<uint4 *>(out));
+    return launch_status();
+  }
+  if (rows == 128 && col_lo == 0 && ncols % 128 == 0 && ncols <= row_bytes * 8 && row_bytes % 16 == 0 &&
+      aligned(in, 16) && aligned(out, 16)) {
+    const uint64_t grid = (ncols / 32 + kTrG - 1) / kTrG;
+    if (grid > 0x7fffffffull) return fail(CUOT_EINVAL, "too many columns");
+    tr_planes128_to_blocks<<<unsigned(grid), kTrThreads, 0, st>>>(static_cast<const uint4 *>(in), ncols,
+                                                                   row_bytes / 16, static_cast<uint4 *>(out));
+    return launch_status();
+  }
+  if (row_bytes == 16 && rows % 32 == 0 && col_lo % 32 == 0 && ncols % 32 == 0 && ncols > 0 &&
+      aligned(in, 16) && aligned(out, 4)) {
     const uint64_t ngroups = rows / 32;
     const uint64_t grid = (ngroups + kTrGroups - 1) / kTrGroups;
     if (grid > 0x7fffffffull) return fail(CUOT_EINVAL, "too many rows");
@@ -150,8 +300,8 @@ int transpose_launch(const void *in, uint64_t rows, uint64_t row_bytes, uint64_t
         static_cast<uint32_t *>(out));
     return launch_status();
   }
-  if (rows % 32 == 0 && rows <= 128 && col_lo == 0 && ncols == row_bytes * 8 &&
-      ncols % 32 == 0 && (row_bytes % 4) == 0) {
+  if (rows % 32 == 0 && rows <= 128 && col_lo == 0 && ncols <= row_bytes * 8 && ncols % 32 == 0 &&
+      (row_bytes % 4) == 0 && aligned(in, 4) && aligned(out, rows == 128 ? 16 : 4)) {
     const uint64_t ngroups = ncols / 32;
     const uint64_t grid = (ngroups + kTrGroups - 1) / kTrGroups;
     if (grid > 0x7fffffffull) return fail(CUOT_EINVAL, "too many columns");

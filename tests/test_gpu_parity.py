@@ -134,17 +134,29 @@ def test_transpose_golden(ctx, golden):
         assert to_host(out).tobytes().hex() == c["out"]
 
 
-@pytest.mark.parametrize("rows,rb,lo,hi", [(1 << 20, 16, 0, 128), (4096 + 32 * 5, 16, 32, 96),
-                                           (128, 1 << 14, 0, 1 << 17), (64, 1024, 0, 8192),
+@pytest.mark.parametrize("rows,rb,lo,hi", [(1 << 20, 16, 0, 128), (1152, 16, 0, 128), (4096 + 32 * 5, 16, 32, 96),
+                                           (128, 1 << 14, 0, 1 << 17), (128, 144, 0, 1152), (128, 512, 0, 2048),
+                                           (128, 1024, 0, 4096 + 96), (64, 1024, 0, 8192),
                                            (96, 40, 16, 320), (8, 1, 0, 8)])
-def test_transpose_vs_oracle(ctx, rows, rb, lo, hi):
+@pytest.mark.parametrize("offset", [0, 4])
+def test_transpose_vs_oracle(ctx, rows, rb, lo, hi, offset):
+    """Every path of the transpose: all 128 planes (partial last tiles at
+    1152 rows / columns), plane ranges, fewer than 128 planes, the leading
+    columns of wider plane rows (the rate-1/2 form's second transpose), the
+    byte-granular shapes; offset 4: input and output 4 bytes past a 16-byte
+    boundary, where the 16-byte fast paths give way."""
     rng = np.random.default_rng(rows + rb)
     m = rng.integers(0, 256, rows * rb, dtype=np.uint8)
-    out = torch.empty((hi - lo) * rows // 8, dtype=torch.uint8, device="cuda")
-    ctx.bit_transpose(to_dev(m), rows, rb, lo, hi, out)
+    nout = (hi - lo) * rows // 8
+    src = torch.zeros(rows * rb + 16, dtype=torch.uint8, device="cuda")
+    src[offset:offset + rows * rb] = to_dev(m)
+    dst = torch.zeros(nout + 16, dtype=torch.uint8, device="cuda")
+    ctx.bit_transpose(src[offset:], rows, rb, lo, hi, dst[offset:])
     exp = np.unpackbits(m.reshape(rows, rb), axis=1, bitorder="little")[:, lo:hi].T
     exp = np.packbits(np.ascontiguousarray(exp), axis=1, bitorder="little").reshape(-1)
-    assert np.array_equal(to_host(out), exp)
+    got = to_host(dst)
+    assert np.array_equal(got[offset:offset + nout], exp)
+    assert not got[:offset].any() and not got[offset + nout:].any()  # nothing written outside
 
 
 def test_transpose_past_2p23_rows(ctx):
