@@ -379,6 +379,9 @@ def transpose_roofline(inst: Instance, flush, peaks: dict, peak_kind: str, reps:
             ms = 0.0
             for _ in range(reps):
                 flush.zero_()
+                # keep the GPU busy (~100 us) while the host enqueues the call, so the events
+                # bracket the kernel and not the host's launch latency
+                torch.cuda._sleep(200_000)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record()
                 fn()

@@ -303,8 +303,9 @@ __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0
 // transform y holds planes 4y .. 4y+3 (< nplanes) with base 2^21 + wide;
 // one_plane: `a` (real part only; centred mode: its complement if wa[0] >
 // n / 2).  With tiles != nullptr the input is in the tile layout
-// instead: word tiles[y][j1][tile] holds the four planes' bytes of the 8
-// columns of the CTA's tile in row j1 (qcf_gather).  centred mode (par !=
+// instead: word tiles[y][tile][j1] holds the four planes' bytes of the 8
+// columns of the CTA's tile in row j1 (qcf_gather), so the CTA reads N1
+// consecutive words.  centred mode (par !=
 // nullptr): planes centred, and par[y] ^= the XOR of the CTA's words (byte q:
 // column parities of plane 4y + q; only the CTA's KC columns).  CEN: the
 // kernel has the centred mode (compiled in for the 1024-point columns of
@@ -327,8 +328,8 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
   const int p0 = 4 * blockIdx.y;
   stage_fs<E1, KC>(fss, fs, c0);
   if (tiles) {
-    const uint32_t *tp = tiles + (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (c0 >> 3);
-    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) bits[j1] = __ldg(tp + (uint64_t(j1) << (e2 - 3)));
+    const uint32_t *tp = tiles + (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (uint64_t(c0 >> 3) << E1);
+    for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) bits[j1] = __ldg(tp + j1);
   } else {
     for (int j1 = threadIdx.x; j1 < N1; j1 += blockDim.x) {
       const uint64_t byte = ((uint64_t(j1) << e2) | uint64_t(c0)) >> 3;
@@ -599,7 +600,7 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
 #pragma unroll
         for (int q = 0; q < 4; q++) word |= ((__ballot_sync(0xffffffffu, pl[q]) >> (lane & ~(KC - 1))) & cm) << (KC * q);
         if (c != 0) continue;
-        const uint64_t wi = (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (uint64_t(j1) << (e2 - 3)) + (c0 >> 3);
+        const uint64_t wi = (uint64_t(blockIdx.y) << (E1 + e2 - 3)) + (uint64_t(c0 >> 3) << E1) + j1;
         if constexpr (KC == 4) {
           reinterpret_cast<uint16_t *>(tiles)[2 * wi + ((c0 & 7) >> 2)] = uint16_t(word);
           continue;
@@ -636,16 +637,20 @@ __device__ __forceinline__ uint64_t transpose8(uint64_t x) {
 }
 
 // Tile layout of 128 planes of n = N1 * N2 bits (the dual LPN's input and
-// output): word tiles[t][j1][g] (t < 32 transforms, g < N2 / 8 column tiles)
-// holds, in byte q, bits (N2 j1 + 8 g + c), c < 8, of plane 4t + q.  The
-// 8 blocks j = 8 (N2/8 j1 + g) + c of the block vector give all 32 words of
-// one (j1, g): per 32-bit word wd and byte k of the blocks, the 8x8 bit
-// transpose of those 8 bytes yields planes 32 wd + 8 k + b in byte b, i.e.
-// words t = 8 wd + 2 k (low half) and t + 1 (high half).
-__global__ void __launch_bounds__(256) qcf_gather(const uint4 *__restrict__ in, uint64_t ngroups,
+// output): word tiles[t][g][j1] (t < 32 transforms, g < N2 / 8 column tiles,
+// j1 < N1 rows) holds, in byte q, bits (N2 j1 + 8 g + c), c < 8, of plane
+// 4t + q, so a column CTA's words are contiguous.  The 8 blocks
+// j = 8 (N2/8 j1 + g) + c of the block vector give all 32 words of one
+// (g, j1): per 32-bit word wd and byte k of the blocks, the 8x8 bit transpose
+// of those 8 bytes yields planes 32 wd + 8 k + b in byte b, i.e. words
+// t = 8 wd + 2 k (low half) and t + 1 (high half).  Thread u = g N1 + j1
+// (j1 fastest): its tile words are written coalesced and its 8 blocks are
+// one 128-byte line.
+__global__ void __launch_bounds__(256) qcf_gather(const uint4 *__restrict__ in, uint64_t ngroups, int e1, int e2,
                                                   uint32_t *__restrict__ tiles) {
-  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups;
-       g += uint64_t(gridDim.x) * blockDim.x) {
+  for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < ngroups;
+       u += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t g = ((u & ((1ull << e1) - 1)) << (e2 - 3)) | (u >> e1);  // block group N2/8 j1 + g
     uint32_t w[8][4];
 #pragma unroll
     for (int c = 0; c < 8; c++) {
@@ -661,8 +666,8 @@ __global__ void __launch_bounds__(256) qcf_gather(const uint4 *__restrict__ in, 
         for (int c = 0; c < 8; c++) x |= uint64_t((w[c][wd] >> (8 * k)) & 0xffu) << (8 * c);
         x = transpose8(x);
         const int t = 8 * wd + 2 * k;
-        tiles[uint64_t(t) * ngroups + g] = uint32_t(x);
-        tiles[uint64_t(t + 1) * ngroups + g] = uint32_t(x >> 32);
+        tiles[uint64_t(t) * ngroups + u] = uint32_t(x);
+        tiles[uint64_t(t + 1) * ngroups + u] = uint32_t(x >> 32);
       }
     }
   }
@@ -680,10 +685,11 @@ __device__ __forceinline__ uint32_t spread_nibbles(uint32_t x) {
 // (a template parameter: a runtime branch in the unrolled loop cost the
 // loads' overlap, 2-7 % of the small dual LPNs).
 template <bool HALVES>
-__global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ tiles, uint64_t ngroups,
-                                                   const uint4 *__restrict__ xor_in, uint4 *__restrict__ out) {
-  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups;
-       g += uint64_t(gridDim.x) * blockDim.x) {
+__global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ tiles, uint64_t ngroups, int e1,
+                                                   int e2, const uint4 *__restrict__ xor_in, uint4 *__restrict__ out) {
+  for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < ngroups;
+       u += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t g = ((u & ((1ull << e1) - 1)) << (e2 - 3)) | (u >> e1);
     uint32_t w[8][4];
 #pragma unroll
     for (int c = 0; c < 8; c++)
@@ -694,7 +700,7 @@ __global__ void __launch_bounds__(256) qcf_scatter(const uint32_t *__restrict__ 
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         const int t = 8 * wd + 2 * k;
-        uint32_t lo = __ldg(&tiles[uint64_t(t) * ngroups + g]), hi = __ldg(&tiles[uint64_t(t + 1) * ngroups + g]);
+        uint32_t lo = __ldg(&tiles[uint64_t(t) * ngroups + u]), hi = __ldg(&tiles[uint64_t(t + 1) * ngroups + u]);
         if constexpr (HALVES) {
           lo = spread_nibbles(lo & 0xffffu) | (spread_nibbles(lo >> 16) << 4);
           hi = spread_nibbles(hi & 0xffffu) | (spread_nibbles(hi >> 16) << 4);
@@ -1048,18 +1054,20 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
 
 int qcf_gather(int e, const cuot_block *in, uint32_t *tiles, cudaStream_t st) {
   const uint64_t ng = 1ull << (e - 3);
-  qcf_gather<<<unsigned((ng + 255) / 256), 256, 0, st>>>(reinterpret_cast<const uint4 *>(in), ng, tiles);
+  const int e1 = qcf_e1(e);
+  qcf_gather<<<unsigned((ng + 255) / 256), 256, 0, st>>>(reinterpret_cast<const uint4 *>(in), ng, e1, e - e1, tiles);
   return launch_status();
 }
 
 int qcf_scatter(int e, const uint32_t *tiles, const cuot_block *xor_in, cuot_block *out, cudaStream_t st) {
   const uint64_t ng = 1ull << (e - 3);
+  const int e1 = qcf_e1(e);
   const dim3 grid(unsigned((ng + 255) / 256));
   if (qcf_tile_kc(e) == 4)
-    qcf_scatter<true><<<grid, 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
+    qcf_scatter<true><<<grid, 256, 0, st>>>(tiles, ng, e1, e - e1, reinterpret_cast<const uint4 *>(xor_in),
                                             reinterpret_cast<uint4 *>(out));
   else
-    qcf_scatter<false><<<grid, 256, 0, st>>>(tiles, ng, reinterpret_cast<const uint4 *>(xor_in),
+    qcf_scatter<false><<<grid, 256, 0, st>>>(tiles, ng, e1, e - e1, reinterpret_cast<const uint4 *>(xor_in),
                                              reinterpret_cast<uint4 *>(out));
   return launch_status();
 }
