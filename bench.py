@@ -281,7 +281,7 @@ class Instance:
 # plus gather and scatter scaled from the n = 2^20 capture (4 x 16.8 MB per
 # role there, x 4 here).
 NCU_TRAFFIC_PER_STEP = {
-    "ferret_b13:lpn": 570.44e6,
+    "ferret_b13:lpn": 631.83e6,
     "sot_n20:dual_lpn": 4050.8e6,
     "sot_n20_ntt:dual_lpn": 3990.2e6,
     "sot_n22:dual_lpn": 2 * (32 * 252.9e6 + 4 * 4 * 16.8e6),
@@ -345,17 +345,19 @@ AES_PEAK_MODEL = ("T-table AES: 160 shared-memory lookups per block (10 rounds x
                   "32-lane lookup wavefront per clock per SM; peak = SMs x 32 x median SM clock / 160")
 
 
-LPN_L1_MODEL = ("L1 wavefronts per LPN row: index-AES table lookups (145 per block for d = 10 blocks of a "
-                "4-row group plus 15 shared round-1 lookups, i.e. (145 d + 15) / 4 per row, 32 lanes per "
-                "wavefront) + d random 16-byte kk gathers (one line, one wavefront each) + the row's 16-byte "
-                "read and write (1/8 wavefront each); peak rows/s = SMs x median SM clock / wavefronts per row")
+LPN_L1_MODEL = ("L1 wavefronts per LPN row pair (the dual-role kernel: one index computation for the two "
+                "parties' rows): index-AES table lookups (145 per block for d = 10 blocks of a 4-row group "
+                "plus 15 shared round-1 lookups, i.e. (145 d + 15) / 4 per row, 32 lanes per wavefront) + 2d "
+                "random 16-byte kk gathers (one line, one wavefront each) + both rows' 16-byte read and write "
+                "(1/8 wavefront each); rows counted per role, peak rows/s = SMs x median SM clock / "
+                "wavefronts per role row")
 
 
 def lpn_l1_roofline(rows: int, d: int, ms: float, clocks: dict, props) -> dict:
     """LPN rows per second against the L1 wavefront bound the index AES and
     the kk gathers share (both go through the L1/shared data pipe)."""
     mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
-    per_row = (145 * d + 15) / 4 / 32 + d + 0.25
+    per_row = ((145 * d + 15) / 4 / 32 + 2 * d + 0.5) / 2  # per role row
     peak = props.multi_processor_count * mhz * 1e6 / per_row
     achieved = rows / (ms / 1e3)
     return {"rows_per_step": rows, "rows_per_s": achieved, "peak_rows_per_s": peak, "frac": achieved / peak,
@@ -407,7 +409,7 @@ def aes_roofline(inst: Instance, stages: dict, clocks: dict, props) -> dict:
     t, h = inst.t, inst.h
     counts = {"pprf": 4 * t * ((1 << h) - 1)}  # 2 AES per internal node, both roles
     if inst.spec["kind"] == "ferret":
-        counts["lpn"] = 2 * inst.n * inst.d // 4  # d index blocks per 4 rows, both roles
+        counts["lpn"] = inst.n * inst.d // 4  # d index blocks per 4 rows, computed once for both roles
     res = {"peak_aes_per_s": peak, "model": AES_PEAK_MODEL}
     for k, cnt in counts.items():
         a = cnt / (stages[k][0] / 1e3)
@@ -946,7 +948,7 @@ def run_batch(args):
     aes_peak = props.multi_processor_count * 32 * mhz * 1e6 / 160
     aes_counts = {"pprf_send": sum(2 * i.t * ((1 << i.h) - 1) for i in insts),
                   "pprf_recv": sum(2 * i.t * ((1 << i.h) - 1) for i in insts),
-                  "lpn": sum(2 * i.n * i.d // 4 for i in insts if i.kind == KIND_FERRET)}
+                  "lpn": sum(i.n * i.d // 4 for i in insts if i.kind == KIND_FERRET)}  # once for both roles
     aes = {"peak_aes_per_s": aes_peak, "model": AES_PEAK_MODEL}
     for k, cnt in aes_counts.items():
         a = cnt / (stages[k] / 1e3)
