@@ -17,7 +17,8 @@
 //     size (each with its own A_hat), back to blocks, and the receivers'
 //     choice-bit encodes.
 // cfg.schedule: CUOT_BATCH_SERIAL (default) runs every launch in one chain
-// on the caller's stream; CUOT_BATCH_FORK_FERRET runs the Ferret branch on a
+// on the caller's stream, each role's PPRF as one persistent launch over the
+// trees of both branches; CUOT_BATCH_FORK_FERRET runs the Ferret branch on a
 // stream of its own beside the SOT branch; CUOT_BATCH_FORK_SIZES also puts
 // each transform size on its own stream (sizes that share per-size FFT
 // state, qc_lane, on one).  Measured on B200 (the 64-instance mix of
@@ -483,15 +484,19 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
   if ((st = upload(b, &sd, sargs)) || (st = upload(b, &rd, rargs)) || (st = upload(b, &smd, smodes)) ||
       (st = upload(b, &rmd, rmodes)) || (st = balloc(b, &b->counters, kCounters * sizeof(unsigned int))))
     return cleanup(st);
-  // ---- PPRF tasks per branch: every tree, deepest first; each branch has
-  // its own per-CTA scratch slots (the branches run at the same time)
+  // ---- PPRF tasks: every tree, deepest first.  Concurrent schedules keep
+  // one list per branch, each with its own per-CTA scratch slots (the
+  // branches run at the same time); the serial schedule puts every tree in
+  // one list (slot 0) so each role is a single persistent launch.
   std::vector<int> order(count);
   for (int i = 0; i < count; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return items[x].h > items[y].h; });
+  const bool merged = b->cfg.schedule == CUOT_BATCH_SERIAL;
+  if (merged) hmax[0] = hmax[1] = std::max(hmax[0], hmax[1]);
   for (int br = 0; br < 2; br++) {
     std::vector<PprfTask> tasks;
     for (int i : order)
-      if ((items[i].kind == CUOT_KIND_FERRET) == (br == kBrFerret))
+      if (merged ? br == 0 : (items[i].kind == CUOT_KIND_FERRET) == (br == kBrFerret))
         for (uint64_t tr = 0; tr < items[i].t; tr++) tasks.push_back(PprfTask{uint32_t(i), uint32_t(tr)});
     if (tasks.empty()) continue;
     b->pprf_grid[br] = int(std::min<uint64_t>(uint64_t(sms) * per_sm, tasks.size()));
