@@ -270,21 +270,20 @@ class Instance:
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant
-# stage's kernels per step, summed from one ncu launch capture of the same
-# bench command (ncu starts every kernel with cold caches, so intermediate
-# that steady state keeps in L2 is counted).  sot_n20 runs the fp64 FFT
-# backend (gather, 3 transform passes, scatter per role); the NTT figure is
-# the same workload with the NTT backend, which scales the SOT encodes of
-# larger n.
-# sot_n22: the three transform passes captured at n = 2^22 (252.9 MB per
-# transform, 32 transforms per role, both roles; profiles/qc_fft_sot_n22.md)
-# plus gather and scatter scaled from the n = 2^20 capture (4 x 16.8 MB per
-# role there, x 4 here).
+# stage's kernels per step, from ncu captures of the same bench command, one
+# kernel and one to three launches per capture (ncu starts every launch with
+# cold caches, so intermediate that steady state keeps in L2 is counted):
+# ferret_b13: the dual-role LPN launch (profiles/pprf_lpn_ferret_b13.md);
+# sot_n20: gather, 16 launches of each transform pass and scatter per role
+# (profiles/qc_fft_sot_n20.md); sot_n20_ntt: the same workload on the NTT
+# backend, which scales the SOT encodes of NTT sizes (profiles/qc_ntt_sot_n20.md);
+# sot_n22: 32 transforms of 251.8 MB per role plus gather and scatter
+# (profiles/qc_fft_sot_n22.md).
 NCU_TRAFFIC_PER_STEP = {
     "ferret_b13:lpn": 631.83e6,
-    "sot_n20:dual_lpn": 4050.8e6,
-    "sot_n20_ntt:dual_lpn": 3990.2e6,
-    "sot_n22:dual_lpn": 2 * (32 * 252.9e6 + 4 * 4 * 16.8e6),
+    "sot_n20:dual_lpn": 2 * (16.79e6 + 16 * 88.24e6 + 16.86e6),
+    "sot_n20_ntt:dual_lpn": 2 * (509.60e6 + 1024.36e6 + 563.98e6 + 33.58e6),
+    "sot_n22:dual_lpn": 2 * (32 * 251.75e6 + 84.17e6 + 82.25e6),
 }
 
 QC_FFT_MAX_LOG_N = 22  # the fp64 FFT encodes n <= 2^22 (exactness bound)
@@ -973,11 +972,12 @@ def run_batch(args):
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_step": alg[dom],
-                     "basis": "stage totals per step (both roles); traffic scaled from ncu captures of the "
-                              "single-instance lines (cold cache per kernel): n = 2^22 (profiles/"
-                              "qc_fft_sot_n22.md) 3,987 DRAM bytes per COT for the 2^22 instances and, 3^L "
-                              "times, the Karatsuba leaves; n = 2^20 3,863 per COT for smaller FFT sizes; "
-                              "3,805 per COT for NTT sizes"},
+                     "basis": "stage totals per step (both roles); traffic scaled from one-kernel ncu "
+                              "captures of the single-instance lines (cold cache per kernel): n = 2^22 "
+                              "(profiles/qc_fft_sot_n22.md) 3,921 DRAM bytes per COT for the 2^22 instances "
+                              "and, 3^L times, the Karatsuba leaves; n = 2^20 (profiles/qc_fft_sot_n20.md) "
+                              "2,757 per COT for smaller FFT sizes; 4,066 per COT for NTT sizes "
+                              "(profiles/qc_ntt_sot_n20.md)"},
         "aes_roofline": aes,
         "qc_transform": qc_transform_report([i.n for i in insts if i.kind != KIND_FERRET], stages["sot_encode"]),
         "e2e": {"value": world * cots / (e2e_ms / 1e3), "unit": "COTs/s", "h2d_bytes_per_step": h2d,
