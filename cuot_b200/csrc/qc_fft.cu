@@ -460,9 +460,12 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
         for (int m = 0; m < Q::R; m++) o[m * NT * Q::items] = make_double2(x[m].x * scale, x[m].y * scale);
         continue;
       }
+      // A_hat is read once per transform: evict-first, so it does not push the
+      // intermediate that the inverse column pass reads next out of L2
+      // (measured: the 64-instance mix 0.6 % faster, n = 2^20 1.1 %, 2^22 0.4 % slower)
       const double2 *a = ah + it;
 #pragma unroll
-      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldg(&a[m * NT * Q::items]));
+      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldcs(&a[m * NT * Q::items]));
       dit_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) row[spos<E2, NT>(i0 + m)] = x[m];
