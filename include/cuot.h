@@ -215,7 +215,10 @@ int cuot_sot_pprf_recver(cuot_ctx *ctx, const cuot_block *m0_d,
  * Mat::bit_transpose (gpu/gpu_matrix.cu:95-121): input `rows` rows of
  * `row_bytes` bytes; output row (c - col_lo) bit r = input row r bit c for
  * c in [col_lo, col_hi).  Output rows are rows/8 bytes.  rows % 8 == 0,
- * col_lo % 8 == 0, col_hi % 8 == 0, col_hi <= 8 * row_bytes. */
+ * col_lo % 8 == 0, col_hi % 8 == 0, col_hi <= 8 * row_bytes.  Any alignment
+ * of in_d / out_d works; 16-byte-aligned pointers with 16-byte rows -> 128
+ * planes (rows % 128 == 0), or 128 planes -> 16-byte rows (col_lo == 0,
+ * col_hi % 128 == 0, row_bytes % 16 == 0), take the fastest kernels. */
 int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
                        uint64_t row_bytes, uint64_t col_lo, uint64_t col_hi,
                        void *out_d, void *stream);
