@@ -397,34 +397,6 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
 // A_hat is stored in the order the last pass consumes it: for the NT rows
 // from r0, element m of item w of row c at r0 * N2 + (m * items + w) * NT + c,
 // so each warp reads 512 contiguous bytes per load.
-// With one row per CTA (NT = 1) the CTAs run in conjugate pairs: row r holds
-// frequencies k1 + N1 k2 with k1 = rev(r) and k2 = rev(i) at position i, and
-// since `a` is real, A_hat at n - k is the conjugate of A_hat at k, i.e. row
-// k1' = N1 - k1 at position ~i.  CTAs 2j and 2j + 1 take k1 = j and N1 - j
-// (N1 / 2 for j = 0, the two rows that pair with themselves), and the second
-// reads the first's A_hat row mirrored and conjugated, so the two CTAs, which
-// run side by side, fetch each A_hat row once.  Either entry carries the
-// transform's error bound, so the rounding argument is unchanged.
-// The row of CTA bx (NT = 1: conjugate-pair order, see above) and the row
-// whose A_hat it reads, mirrored or not.
-template <int NT>
-__device__ __forceinline__ int qcf_row_of(int bx, int e1, int &ra, bool &mirror) {
-  mirror = false;
-  if constexpr (NT == 1) {
-    const int N1 = 1 << e1, j = bx >> 1;
-    const int k1 = (bx & 1) == 0 ? j : j == 0 ? N1 / 2 : N1 - j;
-    const int r = int(__brev(uint32_t(k1)) >> (32 - e1));
-    ra = r;
-    if (k1 > N1 / 2) {
-      mirror = true;
-      ra = int(__brev(uint32_t(N1 - k1)) >> (32 - e1));
-    }
-    return r;
-  }
-  ra = bx * NT;
-  return bx * NT;
-}
-
 template <int E2>
 __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
     double2 *__restrict__ Y, int e1, const double2 *__restrict__ T2, QcfAhatTab ahat, int mode,
@@ -437,22 +409,14 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
   extern __shared__ double2 sm[];
   double2 *xs = sm, *Ts = xs + NT * ld;
   const double2 *T0 = G0 ? T2 : Ts;
-  int r0;
+  const int r0 = blockIdx.x * NT;
   if (mode == 0 && threadIdx.x == 0) {
-    // The pointwise product reads NT * N2 contiguous A_hat values (64 KiB)
-    // in the middle of the kernel; start moving them into L2 now, so those
-    // reads do not wait for DRAM.
-    int ra;
-    bool mirror;
-    r0 = qcf_row_of<NT>(blockIdx.x, e1, ra, mirror);
+    // The pointwise product reads this CTA's A_hat rows (NT * N2 contiguous
+    // values, 64 KiB) in the middle of the kernel; start moving them into L2
+    // now, so those reads do not wait for DRAM.
     const double2 *ahp = static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
-                         (uint64_t(ra) << E2);
+                         (uint64_t(r0) << E2);
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ahp), "r"(uint32_t(NT * N2 * 16)) : "memory");
-  }
-  {
-    int ra;
-    bool mirror;
-    r0 = qcf_row_of<NT>(blockIdx.x, e1, ra, mirror);
   }
   if constexpr (G0)
     stage(Ts, T2 + qcf_tw_off(E2, 1), qcf_tw_off(E2, NP - 1) - qcf_tw_off(E2, 1));
@@ -479,11 +443,8 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
   middle_passes<E2, false, NT, false, G0>(xs, Ts);
   {  // last forward pass; pointwise product; first inverse pass
     using Q = Pass<E2, NP - 1>;
-    int ra;
-    bool mirror;
-    qcf_row_of<NT>(blockIdx.x, e1, ra, mirror);
     const double2 *ah = mode == 0 ? static_cast<const double2 *>(ahat.p[(ahat.first + blockIdx.y) / ahat.per]) +
-                                        (uint64_t(ra) << E2)
+                                        (uint64_t(r0) << E2)
                                   : nullptr;
     for (int it = threadIdx.x; it < NT * Q::items; it += blockDim.x) {
       const int c = it & (NT - 1), w = it / NT;
@@ -502,15 +463,9 @@ __global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
       // A_hat is read once per transform: evict-first, so it does not push the
       // intermediate that the inverse column pass reads next out of L2
       // (measured: the 64-instance mix 0.6 % faster, n = 2^20 1.1 %, 2^22 0.4 % slower)
-      if (!mirror) {
-        const double2 *a = ah + it;
+      const double2 *a = ah + it;
 #pragma unroll
-        for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldcs(&a[m * NT * Q::items]));
-      } else {  // NT = 1: the partner position of (w, m) is (items - 1 - w, R - 1 - m)
-        const double2 *a = ah + (Q::items - 1 - it);
-#pragma unroll
-        for (int m = 0; m < Q::R; m++) x[m] = cmulc(x[m], __ldcs(&a[(Q::R - 1 - m) * Q::items]));
-      }
+      for (int m = 0; m < Q::R; m++) x[m] = cmul(x[m], __ldcs(&a[m * NT * Q::items]));
       dit_regs<Q::K>(x);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) row[spos<E2, NT>(i0 + m)] = x[m];
