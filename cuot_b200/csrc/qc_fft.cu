@@ -61,10 +61,19 @@ namespace cuot {
 
 constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
 
+// Radix-8 plans for the 4096-point rows (8^4) and the 1024-point transforms
+// (8 8 4 4): one more shared-memory pass than radix 16, but few enough live
+// registers for three CTAs per SM.
+constexpr bool kQcfRow12Radix8 = false;
+constexpr bool kQcfL10Radix8 = false;
 // Radix plan of an N = 2^L point transform, 5 <= L <= 12: K bits per pass.
-__host__ __device__ constexpr int qcf_npass(int L) { return L <= 8 ? 2 : 3; }
+__host__ __device__ constexpr int qcf_npass(int L) {
+  return L <= 8 ? 2 : (L == 12 && kQcfRow12Radix8) || (L == 10 && kQcfL10Radix8) ? 4 : 3;
+}
 __host__ __device__ constexpr int qcf_k(int L, int p) {
-  return L == 5 ? (p == 0 ? 3 : 2)
+  return L == 12 && kQcfRow12Radix8 ? 3
+       : L == 10 && kQcfL10Radix8 ? (p < 2 ? 3 : 2)
+       : L == 5 ? (p == 0 ? 3 : 2)
        : L == 6 ? 3
        : L == 7 ? (p == 0 ? 4 : 3)
        : L == 8 ? 4
@@ -85,7 +94,9 @@ __host__ __device__ constexpr int qcf_tw_off(int L, int p) {
 __host__ __device__ constexpr int qcf_threads(int L) { return L >= 10 ? 512 : L == 9 ? 256 : L == 8 ? 128 : 64; }
 // Column CTAs per SM: three up to 512 points and for 4-column CTAs, one for
 // 8 columns of 1024 points (143 KB of shared memory).
-__host__ __device__ constexpr int qcf_col_ctas(int L, int KC) { return L >= 10 ? (KC == 8 ? 1 : 2) : 3; }
+__host__ __device__ constexpr int qcf_col_ctas(int L, int KC) {
+  return L >= 10 ? (KC == 8 ? 1 : kQcfL10Radix8 ? 3 : 2) : 3;
+}
 // four-step factor tables per column: 2^lo + 2^(e1 - lo) entries (global
 // row stride), staged with an odd row stride so the 8 columns of a
 // quarter-warp hit distinct banks
@@ -104,6 +115,10 @@ __host__ __device__ constexpr int qcf_col_threads(int L, int KC) { return KC == 
 __host__ __device__ constexpr int qcf_rows(int L) { return L >= 12 ? 1 : L == 11 ? 2 : 4; }
 // Row pass reads pass 0's twiddles from global memory through L1.
 __host__ __device__ constexpr bool qcf_row_tg0(int L) { return L >= 12; }
+// Row CTAs per SM (launch bound).
+__host__ __device__ constexpr int qcf_row_ctas(int L) {
+  return (L == 12 && kQcfRow12Radix8) || (L == 10 && kQcfL10Radix8) ? 3 : 2;
+}
 __host__ __device__ constexpr int qcf_row_threads(int L) {
   return L >= 11 ? 256 : qcf_threads(L) / 2 < 32 ? 32 : qcf_threads(L) / 2;
 }
@@ -261,13 +276,24 @@ __device__ __forceinline__ void smem_pass(double2 *xs, const double2 *T) {
   }
 }
 
-// Middle passes [1, npass - 1) forward, or in reverse order inverse (REL:
-// T is pass 1's part of the table).
+// Middle pass P (REL: T is pass 1's part of the table, so pass P's part
+// starts tw_off(P) - tw_off(1) further on).
+template <int L, int P, bool INV, int NT, bool TG, bool REL>
+__device__ __forceinline__ void middle_pass(double2 *xs, const double2 *T) {
+  __syncthreads();
+  smem_pass<L, P, INV, NT, TG, REL>(xs, REL ? T + (qcf_tw_off(L, P) - qcf_tw_off(L, 1)) : T);
+}
+// Middle passes [1, npass - 1) forward, or in reverse order inverse.
 template <int L, bool INV, int NT, bool TG = false, bool REL = false>
 __device__ __forceinline__ void middle_passes(double2 *xs, const double2 *T) {
-  if constexpr (qcf_npass(L) == 3) {
-    __syncthreads();
-    smem_pass<L, 1, INV, NT, TG, REL>(xs, T);
+  constexpr int NP = qcf_npass(L);
+  static_assert(NP <= 4, "at most two middle passes");
+  if constexpr (!INV) {
+    if constexpr (NP >= 3) middle_pass<L, 1, INV, NT, TG, REL>(xs, T);
+    if constexpr (NP >= 4) middle_pass<L, 2, INV, NT, TG, REL>(xs, T);
+  } else {
+    if constexpr (NP >= 4) middle_pass<L, 2, INV, NT, TG, REL>(xs, T);
+    if constexpr (NP >= 3) middle_pass<L, 1, INV, NT, TG, REL>(xs, T);
   }
   __syncthreads();
 }
@@ -398,7 +424,7 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
 // from r0, element m of item w of row c at r0 * N2 + (m * items + w) * NT + c,
 // so each warp reads 512 contiguous bytes per load.
 template <int E2>
-__global__ void __launch_bounds__(qcf_row_threads(E2), 2) qcf_row(
+__global__ void __launch_bounds__(qcf_row_threads(E2), qcf_row_ctas(E2)) qcf_row(
     double2 *__restrict__ Y, int e1, const double2 *__restrict__ T2, QcfAhatTab ahat, int mode,
     double2 *__restrict__ out, double scale) {
   constexpr int NT = qcf_rows(E2);
