@@ -84,6 +84,9 @@ def refgpu_lib():
         L.ref_gpu_sot_dual_lpn_ms.restype = C.c_double
         L.ref_gpu_sot_dual_lpn_ms.argtypes = [C.c_uint64, C.c_int]
         L.ref_gpu_bit_transpose.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
+        L.ref_gpu_mpcot_sender_leaves.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_gpu_primal_lpn_run.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]
         _REFGPU = L
     return _REFGPU
 
@@ -96,6 +99,29 @@ def refgpu_bit_transpose(blocks: np.ndarray) -> np.ndarray:
     out = np.empty((128, n // 8), np.uint8)
     rc = refgpu_lib().ref_gpu_bit_transpose(_p(inp), n, _p(out))
     assert rc == 0, f"ref_gpu_bit_transpose rejected n={n} ({rc})"
+    return out
+
+
+def refgpu_mpcot_sender_leaves(roots: np.ndarray, h: int, delta) -> np.ndarray:
+    """Leaves (t * 2^h blocks, tree-major) of the reference's own GPU
+    cuda_mpcot_sender for the given roots (t * 2^h a multiple of 1024)."""
+    roots = np.ascontiguousarray(roots, np.uint8).reshape(-1, 16)
+    t = roots.shape[0]
+    out = np.empty((t << h, 16), np.uint8)
+    rc = refgpu_lib().ref_gpu_mpcot_sender_leaves(t, h, _p(roots), _p(_u8(delta)), _p(out))
+    assert rc == 0, f"ref_gpu_mpcot_sender_leaves rejected t={t} h={h} ({rc})"
+    return out
+
+
+def refgpu_primal_lpn(key, kk: np.ndarray, nn: np.ndarray) -> np.ndarray:
+    """The reference's own GPU cuda_primal_lpn (d = 10, one GPU) on rows nn
+    (n a multiple of 2048) with the 16-byte AES key it reads from LpnF2's
+    expanded schedule."""
+    kk = np.ascontiguousarray(kk, np.uint8).reshape(-1, 16)
+    inp = np.ascontiguousarray(nn, np.uint8).reshape(-1, 16)
+    out = np.empty_like(inp)
+    rc = refgpu_lib().ref_gpu_primal_lpn_run(inp.shape[0], kk.shape[0], _p(_u8(key)), _p(kk), _p(inp), _p(out))
+    assert rc == 0, f"ref_gpu_primal_lpn_run rejected n={inp.shape[0]} ({rc})"
     return out
 
 
@@ -207,6 +233,14 @@ def aes_ecb(key, blocks: np.ndarray, portable: bool = False) -> np.ndarray:
     return out
 
 
+def aes_ecb_rk(rk, blocks: np.ndarray) -> np.ndarray:
+    """AES-128 rounds under an explicit expanded schedule (176 bytes)."""
+    inp = np.ascontiguousarray(blocks, dtype=np.uint8).reshape(-1, 16)
+    out = np.empty_like(inp)
+    lib().or_aes128_encrypt(_p(_u8(rk)), _p(inp), _p(out), SZ(inp.shape[0]))
+    return out
+
+
 def prg(seed, nblocks: int, offset: int = 0) -> np.ndarray:
     out = np.empty((nblocks, 16), np.uint8)
     lib().or_prg_fill(_p(_u8(seed)), U64(offset), _p(out), SZ(nblocks))
@@ -251,6 +285,34 @@ def lpn_primal(seed, kk, nn, d: int = 10, threads: int = 1) -> np.ndarray:
     out = np.array(nn, dtype=np.uint8, copy=True).reshape(-1, 16)
     lib().or_lpn_primal(_p(_u8(seed)), _p(kk), I64(kk.shape[0]), INT(d), _p(out),
                         I64(out.shape[0]), INT(threads))
+    return out
+
+
+def compat_key_expand(key) -> np.ndarray:
+    """cuOT's GPU key schedule (round constants one entry early)."""
+    rk = np.zeros(176, np.uint8)
+    lib().or_compat_key_expand(_p(_u8(key)), _p(rk))
+    return rk
+
+
+def compat_ferret_sender(roots, h: int, delta, threads: int = 1):
+    """cuOT's GPU Ferret sender semantics (no parent XOR, its own keys and
+    schedule, no leaf mask): (leaves, secret sums)."""
+    roots = np.ascontiguousarray(roots, np.uint8).reshape(-1, 16)
+    t = roots.shape[0]
+    leaves = np.empty((t << h, 16), np.uint8)
+    ss = np.empty((t, 16), np.uint8)
+    lib().or_compat_ferret_sender(_p(roots), I64(t), INT(h), *_blk_by_value(_u8(delta)), _p(leaves), _p(ss),
+                                  INT(threads))
+    return leaves, ss
+
+
+def compat_lpn(key, kk, nn, d: int = 10, start: int = 0, threads: int = 1) -> np.ndarray:
+    """cuOT's GPU primal LPN semantics (swapped index plaintext, % k)."""
+    kk = np.ascontiguousarray(kk, np.uint8).reshape(-1, 16)
+    out = np.array(nn, dtype=np.uint8, copy=True).reshape(-1, 16)
+    lib().or_compat_lpn(_p(_u8(key)), _p(kk), I64(kk.shape[0]), INT(d), _p(out), I64(out.shape[0]), I64(start),
+                        INT(threads))
     return out
 
 

@@ -429,6 +429,119 @@ void or_lpn_primal(const uint8_t seed[16], const or_block *kk, int64_t k,
 }
 
 /* ======================================================================== */
+/* cuOT's GPU path restated (compat semantics; see cuot_oracle.h).  Used    */
+/* only to pin how the reference's own GPU kernels differ from emp-ot.      */
+/* ======================================================================== */
+
+/* FIPS-197 key expansion with the round constants one entry early: round i
+ * uses Rcon[i - 1] of the table 0x8d, 0x01, 0x02, ... (gpu/aes_expand.cu:59,
+ * gpu/utilsBox.h:61), i.e. 0x8d, then the standard 0x01 .. 0x1b. */
+void or_compat_key_expand(const uint8_t key[16], uint8_t rk[176]) {
+  const uint8_t *sb = sbox();
+  memcpy(rk, key, 16);
+  uint8_t rcon = 0x8d;
+  for (int i = 4; i < 44; i++) {
+    uint8_t t[4];
+    memcpy(t, rk + 4 * (i - 1), 4);
+    if (i % 4 == 0) {
+      uint8_t u = t[0];
+      t[0] = (uint8_t)(sb[t[1]] ^ rcon);
+      t[1] = sb[t[2]];
+      t[2] = sb[t[3]];
+      t[3] = sb[u];
+      /* the table continues 0x01, 0x02, ... after 0x8d (0x8d * 2 in GF(2^8)
+       * would be 0x01 too: 0x8d is the inverse of 2) */
+      rcon = gf_mul(rcon, 2);
+    }
+    for (int j = 0; j < 4; j++) rk[4 * i + j] = (uint8_t)(rk[4 * (i - 4) + j] ^ t[j]);
+  }
+}
+
+/* 16-byte key whose first little-endian 32-bit word is w (the rest zero),
+ * as cuda_mpcot_sender's k0_blk / k1_blk (dev_layer.cu:22-23). */
+static void compat_word_key(uint32_t w, uint8_t key[16]) {
+  memset(key, 0, 16);
+  for (int i = 0; i < 4; i++) key[i] = (uint8_t)(w >> (8 * i));
+}
+
+typedef struct {
+  const or_block *roots; int h; or_block delta; or_block *leaves; or_block *ss;
+  uint8_t rk0[176], rk1[176];
+} csend_ctx;
+
+/* Trees [lo, hi): level d's node j (tree-major) has children 2j (key 0) and
+ * 2j + 1 (key 1), each AES'(node) with no XOR of the parent (aes_op.cu:
+ * 176-266 writes the cipher text itself). */
+static void csend_range(void *vc, int64_t lo, int64_t hi) {
+  csend_ctx *c = (csend_ctx *)vc;
+  const int64_t w = (int64_t)1 << c->h;
+  for (int64_t t = lo; t < hi; t++) {
+    or_block *tree = c->leaves + t * w;
+    tree[0] = c->roots[t];
+    for (int d = 0; d < c->h; d++) {
+      const int64_t width = (int64_t)1 << d;
+      /* in place, from the last node down, so no parent is overwritten early */
+      for (int64_t j = width - 1; j >= 0; j--) {
+        or_block p = tree[j], l, r;
+        or_aes128_encrypt(c->rk0, (const uint8_t *)&p, (uint8_t *)&l, 1);
+        or_aes128_encrypt(c->rk1, (const uint8_t *)&p, (uint8_t *)&r, 1);
+        tree[2 * j] = l;
+        tree[2 * j + 1] = r;
+      }
+    }
+    or_block s = c->delta;
+    for (int64_t i = 0; i < w; i++) { s.lo ^= tree[i].lo; s.hi ^= tree[i].hi; }
+    if (c->ss) c->ss[t] = s;
+  }
+}
+
+void or_compat_ferret_sender(const or_block *roots, int64_t t, int h,
+                             or_block delta, or_block *leaves,
+                             or_block *secret_sum, int threads) {
+  csend_ctx c;
+  c.roots = roots; c.h = h; c.delta = delta; c.leaves = leaves; c.ss = secret_sum;
+  uint8_t k[16];
+  compat_word_key(3242342u, k);
+  or_compat_key_expand(k, c.rk0);
+  compat_word_key(8993849u, k);
+  or_compat_key_expand(k, c.rk1);
+  parallel_for(t, threads, 1, csend_range, &c);
+}
+
+typedef struct {
+  uint8_t rk[176]; const or_block *kk; int64_t k; int d; or_block *nn; int64_t start;
+} clpn_ctx;
+
+static void clpn_range(void *vc, int64_t lo, int64_t hi) {
+  clpn_ctx *c = (clpn_ctx *)vc;
+  for (int64_t i = lo; i < hi; i++) {
+    or_block acc = c->nn[i];
+    /* words [i d, i d + d) of the encrypted index blocks */
+    const int64_t w0 = i * c->d, b0 = w0 / 4, b1 = (w0 + c->d - 1) / 4;
+    uint32_t words[4 * 12];
+    for (int64_t b = b0; b <= b1; b++) {
+      or_block pt = {4 * (uint64_t)((b + c->start) / 10), (uint64_t)(b % 10)}, ct;
+      or_aes128_encrypt(c->rk, (const uint8_t *)&pt, (uint8_t *)&ct, 1);
+      memcpy(words + 4 * (b - b0), &ct, 16);
+    }
+    for (int j = 0; j < c->d; j++) {
+      const uint32_t w = words[w0 + j - 4 * b0];
+      const or_block *x = &c->kk[w % (uint64_t)c->k];
+      acc.lo ^= x->lo; acc.hi ^= x->hi;
+    }
+    c->nn[i] = acc;
+  }
+}
+
+void or_compat_lpn(const uint8_t key[16], const or_block *kk, int64_t k,
+                   int d, or_block *nn, int64_t n, int64_t start, int threads) {
+  clpn_ctx c;
+  or_compat_key_expand(key, c.rk);
+  c.kk = kk; c.k = k; c.d = d; c.nn = nn; c.start = start;
+  parallel_for(n, threads, 1, clpn_range, &c);
+}
+
+/* ======================================================================== */
 /* Bit transpose: cuOT bit_transposer (gpu/gpu_ops.cu:31-70) as driven by   */
 /* Mat::bit_transpose (gpu/gpu_matrix.cu:95-121): input row r bit c (LSB-   */
 /* first inside each byte, bytes in order) becomes output row (c - col_lo)  */

@@ -51,6 +51,28 @@ void or_ferret_pprf_recver(const or_block *mc, const uint8_t *choice,
 void or_lpn_primal(const uint8_t seed[16], const or_block *kk, int64_t k,
                    int d, or_block *nn, int64_t n, int threads);
 
+/* ---- cuOT's own GPU path, restated (compat semantics) --------------------
+ * Not the path's semantics: the reference's GPU kernels differ from emp-ot in
+ * documented ways, restated here so tests can pin exactly those differences
+ * against the reference kernels run on a B200.
+ *   key schedule: FIPS-197 with round i's Rcon taken one entry early, i.e.
+ *     0x8d, 0x01, 0x02, ..., 0x1b (gpu/aes_expand.cu:52-65, utilsBox.h:61);
+ *   GGM node: child_y = AES'_{k_y}(parent) without the parent XOR, keys with
+ *     first word 3242342 (left) and 8993849 (right) (aesExpand128,
+ *     gpu/aes_op.cu:176-266; keys dev_layer.cu:22-23); no leaf LSB mask;
+ *   secret sum: XOR of a tree's leaves ^ delta (dev_layer.cu:50-53);
+ *   LPN: index block b (b in [0, n d / 4)) = (low 64 bits 4 floor((b + start)
+ *     / 10), high 64 bits b mod 10) encrypted under AES'_key (make_block,
+ *     gpu/gpu_ops.cu:102-109; dev_layer.cu:167-169), row i XORs kk[w % k]
+ *     for the d consecutive 32-bit words w from word i d on
+ *     (lpn_single_row, dev_layer.cu:146-159). */
+void or_compat_key_expand(const uint8_t key[16], uint8_t rk[176]);
+void or_compat_ferret_sender(const or_block *roots, int64_t t, int h,
+                             or_block delta, or_block *leaves,
+                             or_block *secret_sum, int threads);
+void or_compat_lpn(const uint8_t key[16], const or_block *kk, int64_t k,
+                   int d, or_block *nn, int64_t n, int64_t start, int threads);
+
 /* ---- bit transpose (cuOT bit_transposer semantics) ---------------------- */
 void or_bit_transpose(const uint8_t *in, uint64_t rows, uint64_t row_bytes,
                       uint64_t col_lo, uint64_t col_hi, uint8_t *out);

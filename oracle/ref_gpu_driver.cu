@@ -1,4 +1,4 @@
-// ref_gpu_driver.cu -- TEST INFRASTRUCTURE ONLY: speed context and one pin.
+// ref_gpu_driver.cu -- TEST INFRASTRUCTURE ONLY: speed context and pins.
 //
 // Drives the reference's own GPU path, compiled from the reference tree for
 // sm_100a by oracle/build_ref.sh into oracle/_ref/librefgpu.so (only the
@@ -9,13 +9,17 @@
 //   QuasiCyclic::encode_dense + two Mat::bit_transpose, the content of
 //                       SOTSender::dual_lpn (silent/sender.cu:110-119,
 //                       silent/quasi_cyclic.cu:118-128, gpu/gpu_matrix.cu:95-121)
-// These outputs are not an oracle: the reference GPU path uses a non-FIPS key
-// schedule, races on its level sums and rounds a float FFT.  Only
-// Mat::bit_transpose is exact, and the tests compare it with this library's
-// transpose.  Every entry point accepts only shapes for which the reference
-// kernels' index arithmetic (none of them checks bounds) stays inside the
-// buffers the reference's own callers allocate:
-//   MPCOT: t * 2^h >= 1024 leaves (level widths below 512 then read and write
+// These outputs are not the oracle's semantics: the reference GPU path uses a
+// non-FIPS key schedule, other GGM keys and no parent XOR, races on its level
+// sums and rounds a float FFT.  The tests compare Mat::bit_transpose with
+// this library's transpose, and the MPCOT leaves and the LPN outputs with the
+// oracle's restatement of those GPU semantics (or_compat_*).  Every entry
+// point accepts only shapes for which the reference kernels' index
+// arithmetic (none of them checks bounds) stays inside the buffers the
+// reference's own callers allocate:
+//   MPCOT: t * 2^h a multiple of 1024 leaves (aesExpand128 launches whole
+//     blocks of 512 threads per level, so the last level of t * 2^h / 2 parents
+//     must fill them exactly; the earlier, narrower levels then read and write
 //     inside the t * 2^h-block matrices);
 //   LPN: n a multiple of 2048 (make_block and lpn_single_row launch exactly
 //     n*d/4 / 1024 and n / 1024 full blocks of 1024 threads);
@@ -49,7 +53,7 @@ extern "C" {
 // trees of depth h (one GPU), over `reps` calls after one warm-up call.
 __attribute__((visibility("default"))) double ref_gpu_mpcot_sender_ms(int t, int h, int reps) {
   const uint64_t n = uint64_t(t) << h;
-  if (t < 1 || h < 1 || h > 20 || n < 1024 || reps < 1) return -1.0;
+  if (t < 1 || h < 1 || h > 20 || n < 1024 || n % 1024 || reps < 1) return -1.0;
   // FerretCOT::expSeed and MpcotReg::buffer / separated (ferret_cot.hpp:19-22,
   // mpcot_reg.h:55-61): t * 2^h blocks each
   Mat expanded({n}), buffer({n}), sep({n});
@@ -106,6 +110,45 @@ __attribute__((visibility("default"))) double ref_gpu_sot_dual_lpn_ms(uint64_t n
   for (int i = 0; i < reps; i++) one();
   cudaDeviceSynchronize();
   return (now_ms() - t0) / reps;
+}
+
+// Leaves of the reference's cuda_mpcot_sender (one GPU) for t roots and
+// delta (host, 16 bytes each): out = t * 2^h blocks, tree-major (the
+// function leaves them in `expanded`, dev_layer.cu:46-49).  0 on success.
+__attribute__((visibility("default"))) int ref_gpu_mpcot_sender_leaves(int t, int h, const uint8_t *roots,
+                                                                       const uint8_t *delta, uint8_t *out) {
+  const uint64_t n = uint64_t(t) << h;
+  if (t < 1 || h < 1 || h > 20 || n < 1024 || n % 1024) return -1;
+  Mat expanded({n}), buffer({n}), sep({n});
+  expanded.clear();
+  if (cudaMemcpy(expanded.data(), roots, size_t(t) * 16, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+  std::vector<blk> ls(size_t(t) * h), rs(size_t(t) * h), ss(t);
+  blk dl;
+  memcpy(&dl, delta, 16);
+  int tt[1] = {t};
+  cuda_mpcot_sender(&expanded, &buffer, &sep, ls.data(), rs.data(), ss.data(), tt, h, &dl, 1);
+  if (cudaMemcpy(out, expanded.data(), n * 16, cudaMemcpyDeviceToHost) != cudaSuccess) return -3;
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
+}
+
+// The reference's cuda_primal_lpn (d = 10, one GPU) on n rows `in` (host)
+// with k blocks kk (host) and the 16-byte AES key it takes from the front of
+// LpnF2's expanded schedule (lpn_f2.h:85, dev_layer.cu:168): out (host) = the
+// rows after the LPN.  n a multiple of 2048.  0 on success.
+__attribute__((visibility("default"))) int ref_gpu_primal_lpn_run(int64_t n, int k, const uint8_t *key16,
+                                                                  const uint8_t *kk, const uint8_t *in,
+                                                                  uint8_t *out) {
+  const int64_t d = 10;
+  if (n < 2048 || n % 2048 || k < 1) return -1;
+  Mat pub({uint64_t((n * d + 3) / 4)}), kk_d({uint64_t(k)}), expanded({uint64_t(n)});
+  if (cudaMemcpy(expanded.data(), in, size_t(n) * 16, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+  uint32_t key[44] = {0};
+  memcpy(key, key16, 16);
+  std::vector<blk> kkh(k);
+  memcpy(kkh.data(), kk, size_t(k) * 16);
+  int64_t rows[1] = {n};
+  cuda_primal_lpn(Sender, &pub, d, rows, k, key, &expanded, reinterpret_cast<blk *>(out), &kk_d, kkh.data(), 1);
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
 }
 
 // The reference's Mat::bit_transpose of n rows of one block each: in (host,

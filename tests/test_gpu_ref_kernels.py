@@ -1,11 +1,16 @@
 """GPU tests against the reference's own GPU kernels, rebuilt for sm_100a
 from the reference tree (oracle/_ref/librefgpu.so, oracle/ref_gpu_driver.cu).
 
-Of the reference's GPU outputs only Mat::bit_transpose is exact
-(gpu/gpu_matrix.cu:95-121, bit_transposer gpu/gpu_ops.cu:31-70, for row
-counts that are multiples of 256 up to 2^23); it pins this library's
-transpose bit order against reference code run on the same GPU.  The timing
-entry points (speed context for bench.py) are smoke-tested here.
+Of the reference's GPU outputs only Mat::bit_transpose follows the path's
+(emp-ot / CPU) semantics (gpu/gpu_matrix.cu:95-121, bit_transposer
+gpu/gpu_ops.cu:31-70, for row counts that are multiples of 256 up to 2^23);
+it pins this library's transpose bit order against reference code run on
+the same GPU.  The reference's MPCOT leaves and LPN outputs follow its own GPU
+semantics instead; they are pinned here against the oracle's restatement of
+exactly those differences (or_compat_*: the Rcon-shifted key schedule, its
+GGM keys without the parent XOR, the swapped index plaintext and % k), which
+also shows where they part from emp-ot.  The timing entry points (speed
+context for bench.py) are smoke-tested here.
 """
 import numpy as np
 import pytest
@@ -31,6 +36,29 @@ def test_reference_bit_transposer_equals_ours(ctx, n):
         assert np.array_equal(oracle.bit_transpose(x, n, 16, 0, 128).reshape(128, n // 8), ref)
 
 
+@pytest.mark.parametrize("t,h", [(64, 10), (8, 7), (3, 10), (1, 13)])
+def test_reference_gpu_mpcot_leaves_follow_its_compat_semantics(t, h):
+    rng = np.random.default_rng(1000 * t + h)
+    roots = rng_blocks(rng, t)
+    delta = rng_blocks(rng, 1)[0]
+    ref = oracle.refgpu_mpcot_sender_leaves(roots, h, delta)
+    compat, _ = oracle.compat_ferret_sender(roots, h, delta, threads=8)
+    assert np.array_equal(ref, compat)
+    emp = oracle.ferret_pprf_sender(roots, h, delta, threads=8)[0]
+    assert not np.array_equal(ref, emp)  # the reference GPU path is not emp-ot's
+
+
+@pytest.mark.parametrize("n,k", [(2048, 1), (4096, 1000), (65536, 8192), (1 << 20, 452000)])
+def test_reference_gpu_lpn_follows_its_compat_semantics(n, k):
+    rng = np.random.default_rng(n + k)
+    key, kk, e = rng_blocks(rng, 1)[0], rng_blocks(rng, k), rng_blocks(rng, n)
+    ref = oracle.refgpu_primal_lpn(key, kk, e)
+    compat = oracle.compat_lpn(key, kk, e, threads=8)
+    assert np.array_equal(ref, compat)
+    if k > 1:
+        assert not np.array_equal(ref, oracle.lpn_primal(key, kk, e, threads=8))
+
+
 def test_reference_timing_entry_points_run():
     L = oracle.refgpu_lib()
     assert L.ref_gpu_mpcot_sender_ms(64, 10, 2) > 0
@@ -38,6 +66,9 @@ def test_reference_timing_entry_points_run():
     assert L.ref_gpu_sot_dual_lpn_ms(1 << 17, 1) > 0
     # shapes outside the reference kernels' safe range are refused, not run
     assert L.ref_gpu_mpcot_sender_ms(1, 5, 1) < 0
+    assert L.ref_gpu_mpcot_sender_ms(37, 9, 1) < 0  # 18,944 leaves: the last level's grid would overrun
+    assert L.ref_gpu_mpcot_sender_leaves(37, 9, None, None, None) != 0
     assert L.ref_gpu_primal_lpn_ms(1000, 10, 1) < 0
+    assert L.ref_gpu_primal_lpn_run(1000, 10, None, None, None, None) != 0
     assert L.ref_gpu_sot_dual_lpn_ms(1 << 16, 1) < 0
     assert L.ref_gpu_bit_transpose(None, 100, None) != 0
