@@ -87,6 +87,7 @@ def refgpu_lib():
         L.ref_gpu_mpcot_sender_leaves.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_gpu_primal_lpn_run.argtypes = [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p]
+        L.ref_gpu_qc_encode.argtypes = [C.c_uint64, C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _REFGPU = L
     return _REFGPU
 
@@ -123,6 +124,33 @@ def refgpu_primal_lpn(key, kk: np.ndarray, nn: np.ndarray) -> np.ndarray:
     rc = refgpu_lib().ref_gpu_primal_lpn_run(inp.shape[0], kk.shape[0], _p(_u8(key)), _p(kk), _p(inp), _p(out))
     assert rc == 0, f"ref_gpu_primal_lpn_run rejected n={inp.shape[0]} ({rc})"
     return out
+
+
+def refgpu_qc_encode(planes: np.ndarray, n: int, seed: int):
+    """The reference's float QuasiCyclic::encode_dense of 128 planes of n
+    bits (uint64 words, shape (128, n / 64)); returns (out, key, a): the key
+    its constructor drew for `a` (compat_qc_a(key, n) rebuilds it) and the
+    constructor's `a` itself (n / 64 words)."""
+    inp = np.ascontiguousarray(planes, np.uint64).reshape(128, n // 64)
+    out = np.empty_like(inp)
+    key = np.empty(16, np.uint8)
+    a = np.empty(n // 64, np.uint64)
+    rc = refgpu_lib().ref_gpu_qc_encode(n, seed, _p(inp), _p(out), _p(key), _p(a))
+    assert rc == 0, f"ref_gpu_qc_encode rejected n={n} ({rc})"
+    return out, key, a
+
+
+def compat_qc_a(key, n: int) -> np.ndarray:
+    """The reference GPU QuasiCyclic's `a` (silent/quasi_cyclic.cu:59-66): n
+    bits = AES' (the GPU key schedule) of make_block(i) = (low 64 bits
+    4 floor(i / 10), high 64 bits i mod 10), i < n / 128, as n / 64 words."""
+    nb = n // 128
+    i = np.arange(nb, dtype=np.uint64)
+    pt = np.empty((nb, 2), np.uint64)
+    pt[:, 0] = 4 * (i // 10)
+    pt[:, 1] = i % 10
+    ct = aes_ecb_rk(compat_key_expand(key), pt.view(np.uint8).reshape(nb, 16))
+    return ct.reshape(-1).view(np.uint64).copy()
 
 
 def emp_aes_ecb(key, blocks: np.ndarray):

@@ -28,14 +28,25 @@
 //   QC encode: n a power of two in [2^17, 2^23] (a's make_block launch needs
 //     n / 128 to be a multiple of 1024).
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
+#include <cufft.h>
+
 #include "dev_layer.h"
+#include "gpu_define.h"
 #include "gpu_matrix.h"
 #include "gpu_ops.h"
+#include "lpn.h"
 #include "pprf.h"
+// QuasiCyclic keeps its `a` (a64) private; this harness reads it back to pin
+// the restatement of how the constructor makes it.  Every header that
+// quasi_cyclic.h includes is already in, so the access change reaches only
+// that one class definition.
+#define private public
 #include "quasi_cyclic.h"
+#undef private
 
 namespace {
 
@@ -148,6 +159,31 @@ __attribute__((visibility("default"))) int ref_gpu_primal_lpn_run(int64_t n, int
   memcpy(kkh.data(), kk, size_t(k) * 16);
   int64_t rows[1] = {n};
   cuda_primal_lpn(Sender, &pub, d, rows, k, key, &expanded, reinterpret_cast<blk *>(out), &kk_d, kkh.data(), 1);
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
+}
+
+// The reference's QuasiCyclic(Sender, 2n, n, 128).encode_dense on 128 bit
+// planes of n bits (host, plane r at r * n / 8 bytes): out (host) = its float
+// (cuFFT) encode of them.  Its `a` is AES'(make_block(i)), i < n / 128, under
+// a key of four rand() values drawn in its constructor
+// (silent/quasi_cyclic.cu:59-66): srand(seed) first, the same four values go
+// to key_out (16 bytes), so a caller can rebuild `a`.  n a power of two in
+// [2^17, 2^23].  a_out (optional, n / 8 bytes): the constructor's `a`.  0 on
+// success.
+__attribute__((visibility("default"))) int ref_gpu_qc_encode(uint64_t n, unsigned seed, const uint8_t *in,
+                                                             uint8_t *out, uint8_t *key_out, uint8_t *a_out) {
+  if (!pow2(n) || n < (1ull << 17) || n > (1ull << 23)) return -1;
+  srand(seed);
+  uint32_t key[4];
+  for (int i = 0; i < 4; i++) key[i] = uint32_t(rand());
+  memcpy(key_out, key, 16);
+  srand(seed);
+  QuasiCyclic qc(Sender, 2 * n, n, 128);
+  if (a_out && cudaMemcpy(a_out, qc.a64.data(), n / 8, cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+  Mat b({128, n / 128});
+  if (cudaMemcpy(b.data(), in, n * 16, cudaMemcpyHostToDevice) != cudaSuccess) return -2;
+  qc.encode_dense(b);
+  if (cudaMemcpy(out, b.data(), n * 16, cudaMemcpyDeviceToHost) != cudaSuccess) return -3;
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
 }
 

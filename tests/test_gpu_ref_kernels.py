@@ -59,6 +59,35 @@ def test_reference_gpu_lpn_follows_its_compat_semantics(n, k):
         assert not np.array_equal(ref, oracle.lpn_primal(key, kk, e, threads=8))
 
 
+def _bit_error_rate(x: np.ndarray, y: np.ndarray) -> float:
+    return float(np.unpackbits((x ^ y).view(np.uint8)).mean())
+
+
+@pytest.mark.parametrize("n", [1 << 17, 1 << 20, 1 << 22])
+def test_reference_float_qc_encode_against_the_exact_encode(ctx, n):
+    """The reference's QuasiCyclic builds `a` exactly as restated
+    (compat_qc_a: its AES key schedule over make_block counters, under the
+    four rand() words its constructor draws).  Its float encode of 128 random
+    planes with that `a` is then compared with the exact a * b mod (x^n - 1)
+    of this library's encode (against the oracle at 2^17): it reads each
+    coefficient's parity from a truncated float32 value that is an exact
+    multiple of the bit tested, so a negative rounding error flips it.  The
+    printed rate is the share of wrong output bits."""
+    rng = np.random.default_rng(n)
+    planes = rng.integers(0, 2**63, (128, n // 64), dtype=np.uint64)
+    planes |= rng.integers(0, 2, (128, n // 64), dtype=np.uint64) << np.uint64(63)
+    ref, key, a = oracle.refgpu_qc_encode(planes, n, seed=11)
+    assert np.array_equal(a, oracle.compat_qc_a(key, n))
+    d = to_dev(planes.view(np.int64))
+    ctx.qc_encode(to_dev(a.view(np.int64)), d, n, 128)
+    exact = to_host(d).view(np.uint64).reshape(128, n // 64)
+    if n == 1 << 17:
+        assert np.array_equal(exact[:4], oracle.qc_encode(a, planes[:4].copy(), n, threads=8))
+    rate = _bit_error_rate(ref, exact)
+    print(f"reference float QC encode, n = 2^{n.bit_length() - 1}: {rate:.4f} of output bits wrong")
+    assert 0.0 < rate < 0.75
+
+
 def test_reference_timing_entry_points_run():
     L = oracle.refgpu_lib()
     assert L.ref_gpu_mpcot_sender_ms(64, 10, 2) > 0
@@ -72,3 +101,4 @@ def test_reference_timing_entry_points_run():
     assert L.ref_gpu_primal_lpn_run(1000, 10, None, None, None, None) != 0
     assert L.ref_gpu_sot_dual_lpn_ms(1 << 16, 1) < 0
     assert L.ref_gpu_bit_transpose(None, 100, None) != 0
+    assert L.ref_gpu_qc_encode(1 << 16, 1, None, None, None, None) != 0
