@@ -742,7 +742,9 @@ def reference_gpu_context(workload: str, pprf_ms: float, lpn_ms: float, reps: in
         return None
     return {"what": "reference SOTSender::dual_lpn content (Mat::bit_transpose, QuasiCyclic::encode_dense with "
                     "cuFFT, Mat::bit_transpose), one role, sm_100a -O2",
-            "dual_lpn_ms_per_role": dl, "ours_dual_lpn_ms_per_role": lpn_ms / 2}
+            "dual_lpn_ms_per_role": dl, "ours_dual_lpn_ms_per_role": lpn_ms / 2,
+            "note": "speed context only: the reference's float encode is not exact (57-64 % of its output bits "
+                    "differ from a * b mod (x^n - 1) with its own a at n = 2^17 .. 2^22)"}
 
 
 # --------------------------------------------------------------------------
