@@ -878,7 +878,7 @@ def run_batch(args):
     # API.  Two device input sets (a second batch over copies of the inputs,
     # same outputs): step j's input copy runs during step j-1.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    insts2 = [i.input_copy() for i in insts]
+    insts2 = [i.input_copy(own_outputs=True) for i in insts]
     batch2 = Batch(ctx, insts2, use_graph=True, schedule=SCHEDULES[args.batch_schedule], **tuned)
     batch2.run(stream)
     batches = [batch, batch2]
@@ -891,16 +891,19 @@ def run_batch(args):
             hs = pin(getattr(i, k))
             host_in[0].append((hs, getattr(i, dev[k])))
             host_in[1].append((hs, getattr(i2, dev[k])))
-        outs = [(torch.empty_like(i.v, device="cpu").pin_memory(), i.v), (torch.empty_like(i.w, device="cpu").pin_memory(), i.w)]
+        outs = [(torch.empty_like(i.v, device="cpu").pin_memory(), i.v, i2.v),
+                (torch.empty_like(i.w, device="cpu").pin_memory(), i.w, i2.w)]
         if i.kind != KIND_FERRET:
-            outs.append((torch.empty_like(i.cbits, device="cpu").pin_memory(), i.cbits))
+            outs.append((torch.empty_like(i.cbits, device="cpu").pin_memory(), i.cbits, i2.cbits))
         host_out += outs
     h2d = sum(hs.numel() * hs.element_size() for hs, _ in host_in[0])
-    d2h = sum(hs.numel() * hs.element_size() for hs, _ in host_out)
+    d2h = sum(hs.numel() * hs.element_size() for hs, _, _ in host_out)
 
-    # the host copy of step i overlaps step i+1's compute (HostPipeline)
+    # the host copy of step i overlaps step i+1's compute (HostPipeline); the
+    # two batches write their own outputs, which go to the host directly
     from cuot_b200.pipeline import HostPipeline
-    pipe = HostPipeline([dv for _, dv in host_out], stream=stream, input_sets=2)
+    pipe = HostPipeline([[d0 for _, d0, _ in host_out], [d1 for _, _, d1 in host_out]], stream=stream,
+                        input_sets=2, per_set_outputs=True)
 
     def run_flushed(st, slot):
         with torch.cuda.stream(st):
@@ -909,7 +912,7 @@ def run_batch(args):
 
     def e2e(st):
         slot = pipe.slot
-        pipe.step(host_in[slot], lambda s: run_flushed(s, slot), [hs for hs, _ in host_out])
+        pipe.step(host_in[slot], lambda s: run_flushed(s, slot), [hs for hs, _, _ in host_out])
 
     e2e(stream)
     pipe.join()

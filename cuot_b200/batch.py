@@ -72,14 +72,22 @@ class Instance:
     INPUTS = {KIND_FERRET: ("d_roots", "d_choice", "d_kk_s", "d_kk_r"),
               KIND_SOT: ("d_roots", "d_choice", "d_b0", "d_b1", "d_mc")}
 
-    def input_copy(self) -> "Instance":
+    def input_copy(self, own_outputs: bool = False) -> "Instance":
         """The same instance with its own copy of the per-step device inputs
-        (same outputs and polynomial): a second batch over these copies lets
-        host steps double-buffer their inputs (HostPipeline input_sets=2)."""
+        (same polynomial; same outputs, or its own with own_outputs): a
+        second batch over these copies lets host steps double-buffer their
+        inputs (HostPipeline input_sets=2), and with own_outputs their
+        outputs too (per_set_outputs)."""
         import copy
+
+        import torch
         other = copy.copy(self)
         for name in self.INPUTS[self.kind]:
             setattr(other, name, getattr(self, name).clone())
+        if own_outputs:
+            other.v, other.w = torch.empty_like(self.v), torch.empty_like(self.w)
+            if self.kind != KIND_FERRET:
+                other.cbits = torch.empty_like(self.cbits)
         return other
 
     def item(self) -> BatchItem:

@@ -19,21 +19,38 @@ input copies then wait behind that large device-to-host copy (sot_n20:
 device input buffers and gives step j the set `slot` (= j mod 2): its input
 copy runs on its own stream as soon as step j-2, the last reader of that
 set, has finished, i.e. during step j-1's compute.
+
+Outputs: with per_set_outputs the caller also keeps one set of device output
+buffers per input set (step j writes set `slot`); the host copy then reads
+them directly, without the device-to-device staging copy, and step j+2 waits
+for step j's host copy before it writes that set again.
 """
 from __future__ import annotations
 
 
 class HostPipeline:
-    def __init__(self, outputs, stream=None, copy_stream=None, input_sets: int = 1):
+    def __init__(self, outputs, stream=None, copy_stream=None, input_sets: int = 1,
+                 per_set_outputs: bool = False):
+        """outputs: the device output tensors, or with per_set_outputs one
+        list of them per input set."""
         import torch
         if input_sets not in (1, 2):
             raise ValueError("input_sets must be 1 or 2")
         self.torch = torch
-        self.outputs = list(outputs)
+        self.per_set = per_set_outputs
+        if per_set_outputs:
+            self.outputs = [list(o) for o in outputs]
+            if len(self.outputs) != input_sets or len({len(o) for o in self.outputs}) != 1:
+                raise ValueError("per_set_outputs needs one equally long output list per input set")
+            self.staging = None
+        else:
+            self.outputs = list(outputs)
         self.stream = stream if stream is not None else torch.cuda.current_stream()
         self.copy_stream = copy_stream if copy_stream is not None else torch.cuda.Stream()
-        self.staging = [torch.empty_like(o) for o in self.outputs]
+        if not per_set_outputs:
+            self.staging = [torch.empty_like(o) for o in self.outputs]
         self._d2h_done = None
+        self._set_d2h_done = [None] * input_sets  # per output set: its last host copy
         self.input_sets = input_sets
         self.h2d_stream = torch.cuda.Stream() if input_sets > 1 else None
         self._consumed = [None] * input_sets  # per input set: its last reader's compute
@@ -64,12 +81,27 @@ class HostPipeline:
             ready = torch.cuda.Event()
             ready.record(cs_in)
             st.wait_event(ready)
+        if self.per_set and self._set_d2h_done[slot] is not None:
+            st.wait_event(self._set_d2h_done[slot])  # the set's previous results are on the host
         compute(st)
         if self.input_sets > 1:
             done = torch.cuda.Event()
             done.record(st)
             self._consumed[slot] = done
         self._count += 1
+        cs = self.copy_stream
+        if self.per_set:
+            done = torch.cuda.Event()
+            done.record(st)
+            cs.wait_event(done)
+            with torch.cuda.stream(cs):
+                for o, h in zip(self.outputs[slot], host_outputs):
+                    h.copy_(o, non_blocking=True)
+                    d2h += h.numel() * h.element_size()
+            self._d2h_done = torch.cuda.Event()
+            self._d2h_done.record(cs)
+            self._set_d2h_done[slot] = self._d2h_done
+            return h2d, d2h
         if self._d2h_done is not None:
             st.wait_event(self._d2h_done)
         with torch.cuda.stream(st):
@@ -77,7 +109,6 @@ class HostPipeline:
                 s.copy_(o, non_blocking=True)
         staged = torch.cuda.Event()
         staged.record(st)
-        cs = self.copy_stream
         cs.wait_event(staged)
         with torch.cuda.stream(cs):
             for s, h in zip(self.staging, host_outputs):

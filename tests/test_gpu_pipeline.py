@@ -1,88 +1,52 @@
-"""HostPipeline (cuot_b200/pipeline.py): each step's results reach its own
-host buffers intact although the host copy of step i overlaps step i+1,
-which overwrites the device outputs."""
+"""HostPipeline (cuot_b200/pipeline.py): every step's outputs reach the host
+intact while the next steps compute, with staged outputs (one device set) and
+with one device output set per input set (no staging copy; a set is written
+again only after its previous results reached the host)."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
+from cuot_b200.pipeline import HostPipeline  # noqa: E402
 
-def test_pipeline_keeps_every_steps_results(ctx):
-    from cuot_b200.pipeline import HostPipeline
-    n = 1 << 22
-    out = torch.empty((n, 16), dtype=torch.uint8, device="cuda")
-    seed_d = torch.empty((1, 16), dtype=torch.uint8, device="cuda")
+N = 1 << 22  # int32 elements per output (16 MiB): each host copy takes a while
+
+
+def _run(per_set: bool, steps: int = 6):
     st = torch.cuda.Stream()
-    pipe = HostPipeline([out], stream=st)
-    hosts = [torch.empty((n, 16), dtype=torch.uint8).pin_memory() for _ in range(4)]
-    seeds = [torch.full((1, 16), 11 * i + 1, dtype=torch.uint8).pin_memory() for i in range(4)]
-
-    def compute(s, i):
-        # device output = PRG stream of this step's seed (a long kernel), then the seed byte in row 0
-        ctx.prg_fill(bytes([11 * i + 1] * 16), out, stream=s)
-        with torch.cuda.stream(s):
-            out[0].copy_(seed_d[0])
-    for i in range(4):
-        pipe.step([(seeds[i], seed_d)], lambda s, i=i: compute(s, i), [hosts[i]])
-    pipe.join()
-    st.synchronize()
-    import oracle
-    for i in range(4):
-        h = hosts[i].numpy()
-        assert (h[0] == 11 * i + 1).all()
-        exp = oracle.prg(bytes([11 * i + 1] * 16), 1024)
-        assert np.array_equal(h[1:1024], exp[1:1024])
-
-
-def test_double_buffered_inputs_reach_their_own_step(ctx):
-    """input_sets = 2: step j's input copy runs on its own stream while step
-    j-1 computes; every step must still see its own inputs (a copy that
-    overtook the last reader of its buffer set would show up as another
-    step's seed)."""
-    from cuot_b200.pipeline import HostPipeline
-    n = 1 << 22
-    out = torch.empty((n, 16), dtype=torch.uint8, device="cuda")
-    seed_d = [torch.empty((1, 16), dtype=torch.uint8, device="cuda") for _ in range(2)]
-    st = torch.cuda.Stream()
-    pipe = HostPipeline([out], stream=st, input_sets=2)
-    steps = 6
-    hosts = [torch.empty((n, 16), dtype=torch.uint8).pin_memory() for _ in range(steps)]
-    seeds = [torch.full((1, 16), 7 * i + 3, dtype=torch.uint8).pin_memory() for i in range(steps)]
-
-    def compute(s, slot):
-        # a long kernel first, so the next step's input copy has time to overtake
-        ctx.prg_fill(bytes(16), out, stream=s)
-        with torch.cuda.stream(s):
-            out[0].copy_(seed_d[slot][0])
-    for i in range(steps):
+    sets = 2 if per_set else 1
+    outs = [[torch.empty(N, dtype=torch.int32, device="cuda") for _ in range(2)] for _ in range(sets)]
+    ins = [torch.empty(4, dtype=torch.int32, device="cuda") for _ in range(2)]
+    host_in = [torch.tensor([j, 0, 0, 0], dtype=torch.int32).pin_memory() for j in range(steps)]
+    host_out = [[torch.empty(N, dtype=torch.int32).pin_memory() for _ in range(2)] for _ in range(steps)]
+    pipe = HostPipeline(outs if per_set else outs[0], stream=st, input_sets=2, per_set_outputs=per_set)
+    for j in range(steps):
         slot = pipe.slot
-        assert slot == i % 2
-        pipe.step([(seeds[i], seed_d[slot])], lambda s, slot=slot: compute(s, slot), [hosts[i]])
+        o = outs[slot if per_set else 0]
+
+        def compute(s, o=o, slot=slot):
+            with torch.cuda.stream(s):
+                torch.cuda._sleep(2_000_000)  # let the previous host copy still be running
+                o[0].fill_(0).add_(ins[slot][0])  # the step's own input, copied in by the pipeline
+                o[1].fill_(0).add_(ins[slot][0] * 3 + 1)
+        h2d, d2h = pipe.step([(host_in[j], ins[slot])], compute, host_out[j])
+        assert h2d == 16 and d2h == 2 * 4 * N
     pipe.join()
-    st.synchronize()
-    for i in range(steps):
-        assert (hosts[i].numpy()[0] == 7 * i + 3).all(), i
+    torch.cuda.synchronize()
+    for j in range(steps):
+        assert (host_out[j][0].numpy() == j).all() and (host_out[j][1].numpy() == 3 * j + 1).all(), j
 
 
-def test_copy_to_host_through_sm_stores(ctx):
-    """cuot_copy_to_host: device bytes land in pinned host memory, with
-    16-byte and byte-granular paths (aligned and odd sizes / offsets), two
-    calls in a row; an unpinned destination is refused."""
-    import cuot_b200
-    rng = np.random.default_rng(3)
-    for nbytes in (16 * 4097, 1000003):
-        src = torch.from_numpy(rng.integers(0, 256, nbytes, dtype=np.uint8)).cuda()
-        dst = torch.zeros(nbytes + 1, dtype=torch.uint8).pin_memory()
-        for view in (dst[:nbytes], dst[1:]):
-            view.zero_()
-            cuot_b200.copy_to_host(src, view)
-            torch.cuda.synchronize()
-            assert np.array_equal(view.numpy(), src.cpu().numpy())
-    import ctypes
-    pageable = np.zeros(64, np.uint8)
-    st = cuot_b200.load().cuot_copy_to_host(ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(pageable.ctypes.data),
-                                            ctypes.c_uint64(64), None)
-    assert st == 1 and b"mapped" in cuot_b200.load().cuot_last_error()
+def test_pipeline_staged_outputs():
+    _run(per_set=False)
+
+
+def test_pipeline_per_set_outputs():
+    _run(per_set=True)
+
+
+def test_pipeline_per_set_outputs_need_one_list_per_set():
+    t = torch.empty(4, device="cuda")
     with pytest.raises(ValueError):
-        cuot_b200.copy_to_host(src[:16], torch.zeros(16, dtype=torch.uint8))
+        HostPipeline([[t]], input_sets=2, per_set_outputs=True)
