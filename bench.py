@@ -1070,6 +1070,23 @@ def run_served(args, device: int) -> dict:
     reqs = make_stream(args.serve_requests, rate=rate, seed=6, lo=lo, hi=hi)
     cont.configure(budget_bytes=120e9, big_n=big_n, high_priority_below_n=prio_n)
     rep = cont.run(reqs)
+    sweep = None
+    if args.serve_sweep:
+        # offered rate swept as fractions of the saturation throughput; a rate
+        # is sustained while requests complete as fast as they arrive
+        sweep = {"requests_per_rate": args.serve_sweep_requests, "points": []}
+        for j, f in enumerate(float(x) for x in args.serve_sweep.split(",")):
+            offered = f * sat["req_per_s"]
+            stream = make_stream(args.serve_sweep_requests, rate=offered, seed=100 + j, lo=lo, hi=hi)
+            r = cont.run(stream)
+            arrived = max(q.arrival for q in stream)
+            point = {"fraction_of_saturation": f, "offered_rps": offered,
+                     "completed_rps": r["done"] / r["wall_s"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+                     "mean_ms": r["mean_ms"], "cots_per_s": r["cots_per_s"],
+                     "backlog_s": r["wall_s"] - arrived}
+            sweep["points"].append(point)
+        ok = [p for p in sweep["points"] if p["completed_rps"] >= 0.95 * p["offered_rps"]]
+        sweep["sustained_rps"] = max((p["offered_rps"] for p in ok), default=None)
     cont.close()
     rep_plain = plain.run(reqs)
     plain.close()
@@ -1081,6 +1098,7 @@ def run_served(args, device: int) -> dict:
                            "continuous_over_plain": sat["req_per_s"] / sat_plain["req_per_s"]},
             "continuous": {k: rep[k] for k in keys},
             "plain_per_request": {k: rep_plain[k] for k in keys},
+            **({"rate_sweep": sweep} if sweep else {}),
             "note": "latency = arrival -> outputs in device memory; rate = 0.9 x saturation throughput "
                     "of the continuous-batching server (its probe: every request present at t = 0, the "
                     "same probe for plain per-request execution)"}
@@ -1362,6 +1380,9 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=10000,
                     help="requests of the served stream reported with mixed64 (0: skip; the full served configuration is 10000)")
     ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-sweep", default="",
+                    help="comma-separated fractions of the saturation rate to serve a stream at (continuous server)")
+    ap.add_argument("--serve-sweep-requests", type=int, default=2000)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--batch-schedule", default="serial", choices=["serial", "fork_ferret", "fork_sizes"],
                     help="batched mix: one chain (default), the Ferret branch beside the SOT chain, or every SOT "
