@@ -1054,7 +1054,7 @@ def run_served(args, device: int) -> dict:
     three times the rate the servers can take (requests arrive faster than
     they finish, so the rate measures the server, not the arrivals).  The
     10,000-request stream is then offered at 70 % of the continuous server's
-    saturation, a rate it sustains (its queue stays bounded; see the
+    saturation, a rate at which its queue stays bounded (see the
     --serve-sweep option), and served by both."""
     from cuot_b200.serve import Server, make_stream, saturation
 
