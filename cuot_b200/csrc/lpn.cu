@@ -136,16 +136,16 @@ extern "C" {
 int cuot_lpn_primal_dual(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_send_d,
                          const cuot_block *kk_recv_d, int64_t k, int d, cuot_block *e_send_io_d,
                          cuot_block *e_recv_io_d, int64_t n, void *stream) {
-  if (!ctx || !seed || !kk_send_d || !kk_recv_d || !e_send_io_d || !e_recv_io_d)
+  if (!ctx || !seed || ((!kk_send_d || !kk_recv_d || !e_send_io_d || !e_recv_io_d) && n > 0))
     return fail(CUOT_EINVAL, "null argument");
-  if (e_send_io_d == e_recv_io_d) return fail(CUOT_EINVAL, "the two roles' rows must not alias");
+  if (n > 0 && e_send_io_d == e_recv_io_d) return fail(CUOT_EINVAL, "the two roles' rows must not alias");
   return lpn_rows(ctx, seed, kk_send_d, kk_recv_d, k, d, e_send_io_d, e_recv_io_d, 0, n, n, stream);
 }
 
 int cuot_lpn_primal_range(cuot_ctx *ctx, const uint8_t seed[16], const cuot_block *kk_d,
                           int64_t k, int d, cuot_block *e_rows_d, int64_t row_lo, int64_t row_hi,
                           int64_t n, void *stream) {
-  if (!ctx || !seed || !kk_d || !e_rows_d) return fail(CUOT_EINVAL, "null argument");
+  if (!ctx || !seed || ((!kk_d || !e_rows_d) && row_hi > row_lo)) return fail(CUOT_EINVAL, "null argument");
   return lpn_rows(ctx, seed, kk_d, nullptr, k, d, e_rows_d, nullptr, row_lo, row_hi, n, stream);
 }
 

@@ -338,7 +338,7 @@ using namespace cuot;
 extern "C" int cuot_bit_transpose(cuot_ctx *ctx, const void *in_d, uint64_t rows,
                                   uint64_t row_bytes, uint64_t col_lo, uint64_t col_hi,
                                   void *out_d, void *stream) {
-  if (!ctx || !in_d || !out_d) return fail(CUOT_EINVAL, "null argument");
+  if (!ctx || ((!in_d || !out_d) && rows > 0)) return fail(CUOT_EINVAL, "null argument");
   if (rows % 8 || col_lo % 8 || col_hi % 8 || col_hi <= col_lo || col_hi > row_bytes * 8)
     return fail(CUOT_EINVAL, "bad transpose shape rows=%llu row_bytes=%llu cols=[%llu,%llu)",
                 (unsigned long long)rows, (unsigned long long)row_bytes,

@@ -7,6 +7,10 @@
  * as void*.  Every call is stream-ordered, returns a status code, and never
  * synchronises the device unless its comment says so.
  *
+ * Calls with nothing to do (zero LPN rows, zero AES blocks, zero transpose
+ * rows) return CUOT_OK without launching and accept null data pointers; a
+ * zero tree count, plane count or instance count is CUOT_EINVAL.
+ *
  * Blocks are 16 bytes with the memory image of emp-tool's `block` and cuOT's
  * `blk` (gpu/gpu_define.h:12-16).  Bit vectors are little-endian: bit j of a
  * vector is bit (j % 8) of byte j / 8.

@@ -68,3 +68,38 @@ def test_host_block_arguments_need_no_alignment(ctx):
                                            _stream(None)), "cuot_ferret_pprf_sender")
     exp = oracle.ferret_pprf_sender(roots, h, delta)
     assert np.array_equal(to_host(lv), exp[0]) and np.array_equal(to_host(ss), exp[3])
+
+
+def test_empty_and_degenerate_inputs(ctx):
+    """Zero-size work is a no-op that launches nothing (null pointers allowed
+    where there is nothing to read or write); shapes with no valid meaning
+    are CUOT_EINVAL; the context stays usable."""
+    import cuot_b200
+    empty = torch.empty((0, 16), dtype=torch.uint8, device="cuda")
+    seed = np.arange(16, dtype=np.uint8)
+    kk = to_dev(rng_blocks(np.random.default_rng(2), 8))
+    k0 = cuot_b200.launch_count()
+    ctx.lpn_primal(seed, kk, empty)                        # n = 0 rows
+    ctx.lpn_primal_dual(seed, kk, kk, empty, empty)       # both roles, n = 0
+    ctx.aes128_ecb(seed, empty)                           # no blocks
+    ctx.aes128_ecb_bitsliced(seed, empty)
+    ctx.bit_transpose(empty, 0, 16, 0, 128, empty)        # no rows
+    assert cuot_b200.launch_count() == k0                 # nothing launched
+    # a tree count of zero and a plane count of zero have no meaning
+    delta = np.ones(16, np.uint8)
+    einval(lambda: ctx.ferret_pprf_sender(empty, 4, delta, empty, empty, empty, empty))
+    words = torch.zeros(1024 // 64, dtype=torch.int64, device="cuda")
+    einval(lambda: ctx.qc_encode(words, words, 1024, 0))
+    from cuot_b200.batch import Batch
+    einval(lambda: Batch(ctx, []))
+    # one-tree, depth-1 and one-row extremes still compute
+    rng = np.random.default_rng(3)
+    roots = rng_blocks(rng, 1)
+    e = lambda m: torch.empty((m, 16), dtype=torch.uint8, device="cuda")
+    lv, ls, rs, ss = e(2), e(1), e(1), e(1)
+    ctx.ferret_pprf_sender(to_dev(roots), 1, delta, lv, ls, rs, ss)
+    assert np.array_equal(to_host(lv), oracle.ferret_pprf_sender(roots, 1, delta)[0])
+    one = rng_blocks(rng, 1)
+    d1 = to_dev(one)
+    ctx.lpn_primal(seed, kk, d1)
+    assert np.array_equal(to_host(d1), oracle.lpn_primal(seed, to_host(kk), one))
