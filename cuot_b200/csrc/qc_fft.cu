@@ -54,7 +54,7 @@
 // transforms (columns) of a CTA sit in rows of N + 1 complex values and the 8
 // lanes of each quarter-warp work on the same item of the 8 transforms; with
 // 4 (2, 1) per CTA, rows of N + 2 (N + 4, N) and an XOR swizzle (spos), so
-// every shared-memory access is conflict-free.
+// the passes' shared-memory exchanges are conflict-free.
 #include "ctx.cuh"
 
 namespace cuot {
