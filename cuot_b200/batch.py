@@ -134,6 +134,20 @@ class Batch:
     def kernels_per_run(self) -> int:
         return int(self.lib.cuot_batch_kernels_per_run(self.h))
 
+    def item_rank(self, i: int) -> int:
+        """Completion point of instance i: 0 for Ferret instances (after the
+        LPN), then 1, 2, ... for the SOT sizes, largest first."""
+        r = int(self.lib.cuot_batch_item_rank(self.h, C.c_int(i)))
+        if r < 0:
+            raise IndexError(f"batch has no instance {i}")
+        return r
+
+    def wait_item(self, i: int, stream) -> None:
+        """Makes `stream` wait until instance i's outputs of the last run()
+        are final (earlier than the end of the run for all but the last
+        size)."""
+        _check(self.lib.cuot_batch_wait_item(self.h, C.c_int(i), _stream(stream)), "cuot_batch_wait_item")
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.cuot_batch_destroy(self.h)

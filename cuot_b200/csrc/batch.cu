@@ -208,6 +208,13 @@ struct cuot_batch {
   // lane j >= 1 (lane 0 runs on the caller's stream)
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
+  // Completion points: group 0 is every Ferret item (after the LPN), group
+  // 1 + k the k-th SOT size class in the order the lanes enqueue them (after
+  // its sparse encodes).  done_ev[g] is recorded there in every batched run,
+  // as an external event node when the run is a graph.
+  std::vector<cudaEvent_t> done_ev;
+  std::vector<int> class_group;  // per class
+  std::vector<int> item_group;   // per item
   int kernels_per_run = 0;  // kernels one batched run launches
   // graph
   cudaGraph_t graph = nullptr;
@@ -305,6 +312,25 @@ int lpn_launch(cuot_batch *b, cudaStream_t st) {
   return 1;
 }
 
+// Records completion group g's event on `st`: under stream capture as an
+// external event node, so a wait outside the graph sees it (the flag is
+// refused outside capture).
+int record_done(cuot_batch *b, int g, cudaStream_t st) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "cudaStreamIsCapturing failed");
+  }
+  const cudaError_t e = cap == cudaStreamCaptureStatusActive
+                            ? cudaEventRecordWithFlags(b->done_ev[g], st, cudaEventRecordExternal)
+                            : cudaEventRecord(b->done_ev[g], st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "batch completion event record failed");
+  }
+  return CUOT_OK;
+}
+
 // The SOT sizes of one lane, in order, on `st`.
 int enqueue_lane(cuot_batch *b, const std::vector<int> &lane, cudaStream_t st) {
   cuot_ctx *ctx = b->ctx;
@@ -326,6 +352,7 @@ int enqueue_lane(cuot_batch *b, const std::vector<int> &lane, cudaStream_t st) {
       const cuot_batch_item &it = b->items[i];
       CUOT_TRY(cuot_qc_encode_sparse(ctx, it.a_d, it.punct_d, int(it.t), n, it.cbits_d, st));
     }
+    CUOT_TRY(record_done(b, b->class_group[ci], st));
   }
   return CUOT_OK;
 }
@@ -361,6 +388,7 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
     mark(2);
     launches += lpn_launch(b, st);
     CUOT_TRY(launch_status(launches));
+    if (b->lpn.ntasks) CUOT_TRY(record_done(b, 0, st));
     mark(3);
     for (const auto &lane : b->lanes) CUOT_TRY(enqueue_lane(b, lane, st));
     mark(4);
@@ -376,6 +404,7 @@ int enqueue(cuot_batch *b, cudaStream_t st, cudaEvent_t *ev = nullptr) {
       launches += pprf_launch(b, b->recv[kBrFerret], kBrFerret, sf);
       launches += lpn_launch(b, sf);
       CUOT_TRY(launch_status(launches));
+      if (b->lpn.ntasks) CUOT_TRY(record_done(b, 0, sf));
       if (cudaEventRecord(E[kEvFerret], sf) != cudaSuccess) return ev_fail();
     }
     // SOT branch: PPRFs on the caller's stream, then the lanes side by side
@@ -593,6 +622,22 @@ int cuot_batch_create(cuot_ctx *ctx, const cuot_batch_item *items, int count,
     }
     b->events.push_back(e);
   }
+  // ---- completion groups: Ferret items, then the SOT classes in enqueue order
+  b->class_group.assign(b->classes.size(), 0);
+  int ngroups = 1;
+  for (const auto &lane : b->lanes)
+    for (int ci : lane) b->class_group[ci] = ngroups++;
+  b->item_group.assign(count, 0);
+  for (size_t ci = 0; ci < b->classes.size(); ci++)
+    for (int i : b->classes[ci].items) b->item_group[i] = b->class_group[ci];
+  for (int g = 0; g < ngroups; g++) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return cleanup(fail(CUOT_ECUDA, "batch event creation failed"));
+    }
+    b->done_ev.push_back(e);
+  }
   if (cudaDeviceSynchronize() != cudaSuccess) {
     cudaGetLastError();
     return cleanup(fail(CUOT_ECUDA, "batch set-up kernels failed"));
@@ -675,6 +720,21 @@ int cuot_batch_run_plain(cuot_batch *b, void *stream) {
 
 int cuot_batch_kernels_per_run(const cuot_batch *b) { return b ? b->kernels_per_run : 0; }
 
+int cuot_batch_item_rank(const cuot_batch *b, int item) {
+  if (!b || item < 0 || item >= int(b->items.size())) return -1;
+  return b->item_group[item];
+}
+
+int cuot_batch_wait_item(cuot_batch *b, int item, void *stream) {
+  if (!b || item < 0 || item >= int(b->items.size())) return fail(CUOT_EINVAL, "bad argument");
+  DeviceGuard g(b->ctx);
+  if (cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), b->done_ev[b->item_group[item]], 0) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CUOT_ECUDA, "cudaStreamWaitEvent failed");
+  }
+  return CUOT_OK;
+}
+
 int cuot_batch_run_phases(cuot_batch *b, void *stream, float *phase_ms) {
   if (!b || !phase_ms) return fail(CUOT_EINVAL, "bad argument");
   DeviceGuard g(b->ctx);
@@ -698,6 +758,7 @@ int cuot_batch_destroy(cuot_batch *b) {
     for (auto s : b->streams) cudaStreamSynchronize(s);
     for (auto s : b->streams) cudaStreamDestroy(s);
     for (auto e : b->events) cudaEventDestroy(e);
+    for (auto e : b->done_ev) cudaEventDestroy(e);
     for (void *p : b->allocs) cudaFree(p);
   }
   delete b;

@@ -23,7 +23,12 @@ set, has finished, i.e. during step j-1's compute.
 Outputs: with per_set_outputs the caller also keeps one set of device output
 buffers per input set (step j writes set `slot`); the host copy then reads
 them directly, without the device-to-device staging copy, and step j+2 waits
-for step j's host copy before it writes that set again.
+for step j's host copy before it writes that set again.  A step can also
+say, per output, when that output is final (`ready`): its host copy then
+waits only for that point instead of the whole step, so the outputs that
+are final early (a batch's Ferret instances after the LPN, its SOT sizes
+largest first) cross PCIe while the rest of the step still computes, and
+only the last ones are left after it.
 """
 from __future__ import annotations
 
@@ -61,13 +66,23 @@ class HostPipeline:
         """Input set the next step() must use (0 with input_sets = 1)."""
         return self._count % self.input_sets
 
-    def step(self, inputs, compute, host_outputs):
+    def step(self, inputs, compute, host_outputs, ready=None):
         """inputs: [(host_tensor, device_tensor)] copied host->device first
         (device tensors of input set `slot`); compute(stream) enqueues the
         step's device work; host_outputs: pinned host tensors receiving this
-        step's outputs (same shapes as `outputs`).  Returns (h2d_bytes,
+        step's outputs (same shapes as `outputs`).  ready (per_set_outputs
+        only): one entry per output, None or a callable ready(copy_stream)
+        that makes the copy stream wait until that output is final; the
+        outputs are copied in list order, each after the waits of the
+        entries up to it, so list them in the order they become final.
+        Without it every copy waits for the whole step.  Returns (h2d_bytes,
         d2h_bytes).  Nothing here blocks the host."""
         torch, st = self.torch, self.stream
+        if ready is not None:
+            if not self.per_set:
+                raise ValueError("ready needs per_set_outputs")
+            if len(ready) != len(host_outputs) or not ready or ready[0] is None:
+                raise ValueError("ready needs one entry per output, the first one a wait")
         h2d = d2h = 0
         slot = self.slot
         cs_in = self.h2d_stream if self.input_sets > 1 else st
@@ -78,9 +93,9 @@ class HostPipeline:
                 d.copy_(h, non_blocking=True)
                 h2d += h.numel() * h.element_size()
         if self.input_sets > 1:
-            ready = torch.cuda.Event()
-            ready.record(cs_in)
-            st.wait_event(ready)
+            copied = torch.cuda.Event()
+            copied.record(cs_in)
+            st.wait_event(copied)
         if self.per_set and self._set_d2h_done[slot] is not None:
             st.wait_event(self._set_d2h_done[slot])  # the set's previous results are on the host
         compute(st)
@@ -91,11 +106,14 @@ class HostPipeline:
         self._count += 1
         cs = self.copy_stream
         if self.per_set:
-            done = torch.cuda.Event()
-            done.record(st)
-            cs.wait_event(done)
+            if ready is None:
+                done = torch.cuda.Event()
+                done.record(st)
+                cs.wait_event(done)
             with torch.cuda.stream(cs):
-                for o, h in zip(self.outputs[slot], host_outputs):
+                for j, (o, h) in enumerate(zip(self.outputs[slot], host_outputs)):
+                    if ready is not None and ready[j] is not None:
+                        ready[j](cs)
                     h.copy_(o, non_blocking=True)
                     d2h += h.numel() * h.element_size()
             self._d2h_done = torch.cuda.Event()

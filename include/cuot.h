@@ -420,6 +420,17 @@ int cuot_batch_run_plain(cuot_batch *b, void *stream);
 int cuot_batch_destroy(cuot_batch *b);
 /* Kernels launched by one batched run (known after the first run). */
 int cuot_batch_kernels_per_run(const cuot_batch *b);
+/* Makes `stream` wait until item `item`'s outputs (v, w and, for SOT, cbits)
+ * are final in the batched run last enqueued (cuot_batch_run or
+ * cuot_batch_run_phases), which for all but the last items is before the run
+ * ends: the Ferret items are final after the LPN, each SOT size class after
+ * its own encodes.  A host copy of an item can start there.  Waits on nothing
+ * before the first run.  Does not block the host. */
+int cuot_batch_wait_item(cuot_batch *b, int item, void *stream);
+/* The item's completion point, in the order a CUOT_BATCH_SERIAL run reaches
+ * them: 0 for Ferret items, then 1, 2, ... for the SOT sizes, largest first.
+ * Items of one rank complete together; -1 for a bad argument. */
+int cuot_batch_item_rank(const cuot_batch *b, int item);
 /* Diagnostic: the batched program without a graph, timed per phase with
  * events (synchronises): phase_ms[0..3] = sender PPRF (+ OT selection),
  * receiver PPRF, LPN, SOT encodes. */

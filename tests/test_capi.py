@@ -55,6 +55,8 @@ def test_null_arguments_are_rejected_without_a_device():
     assert lib.cuot_ferret_pprf_sender(None, None, ctypes.c_uint64(1), 3, None, None, None, None, None, None) == 1
     assert lib.cuot_lpn_primal(None, None, None, ctypes.c_int64(1), 10, None, ctypes.c_int64(1), None) == 1
     assert lib.cuot_ctx_destroy(None) == 0
+    assert lib.cuot_batch_wait_item(None, 0, None) == 1
+    assert lib.cuot_batch_item_rank(None, 0) == -1
 
 
 def test_server_arguments_are_checked_without_a_device():

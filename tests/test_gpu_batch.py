@@ -117,3 +117,46 @@ def test_unknown_schedule_is_rejected(ctx):
         ev, ew, _ = oracle_outputs(inst)
         assert np.array_equal(inst.v.cpu().numpy(), ev) and np.array_equal(inst.w.cpu().numpy(), ew)
     b.close()
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_item_completion_points(ctx, use_graph):
+    """cuot_batch_wait_item: a copy stream that waits for each instance's
+    completion point (rank order: Ferret after the LPN, then the SOT sizes
+    largest first) and copies its outputs right away gets the final outputs,
+    though the run has not ended when the first copies start.  The outputs
+    are zeroed on the compute stream before the run, so a copy that ran early
+    would see zeros or a partial result."""
+    specs = [(KIND_SOT, 16, 10, 0), (KIND_FERRET, 8, 10, 1000), (KIND_SOT, 64, 10, 0), (KIND_FERRET, 3, 12, 77),
+             (KIND_SOT, 4, 10, 0), (KIND_SOT, 2, 12, 0)]
+    insts = [Instance(ctx, kd, t, h, 700 + i, k=k) for i, (kd, t, h, k) in enumerate(specs)]
+    b = Batch(ctx, insts, use_graph=use_graph, schedule=SERIAL)
+    ranks = [b.item_rank(i) for i in range(len(insts))]
+    assert ranks == [2, 0, 1, 0, 4, 3]  # 2^14, Ferret, 2^16, Ferret, 2^12, 2^13
+    with pytest.raises(IndexError):
+        b.item_rank(len(insts))
+    stream, cs = torch.cuda.Stream(), torch.cuda.Stream()
+    expect = [oracle_outputs(inst) for inst in insts]
+    for rep in range(2):
+        with torch.cuda.stream(stream):
+            for inst in insts:
+                inst.v.zero_(); inst.w.zero_()
+                if inst.kind != KIND_FERRET:
+                    inst.cbits.zero_()
+        b.run(stream)
+        host = {}
+        with torch.cuda.stream(cs):
+            for ix in sorted(range(len(insts)), key=lambda j: ranks[j]):
+                b.wait_item(ix, cs)
+                inst = insts[ix]
+                outs = [inst.v, inst.w] + ([] if inst.kind == KIND_FERRET else [inst.cbits])
+                host[ix] = [torch.empty_like(o, device="cpu").pin_memory() for o in outs]
+                for h, o in zip(host[ix], outs):
+                    h.copy_(o, non_blocking=True)
+        cs.synchronize()
+        for ix, (ev, ew, ec) in enumerate(expect):
+            assert np.array_equal(host[ix][0].numpy(), ev) and np.array_equal(host[ix][1].numpy(), ew), (rep, ix)
+            if ec is not None:
+                assert np.array_equal(host[ix][2].numpy().view(np.uint64), ec), (rep, ix)
+        torch.cuda.synchronize()
+    b.close()
