@@ -146,6 +146,13 @@ class Context:
         _check(self.lib.cuot_qc_fft_margin(self.h, C.byref(v), C.c_int(int(reset))), "cuot_qc_fft_margin")
         return v.value
 
+    def measure_fp64_tflops(self, reps: int = 5) -> float:
+        """The device's fp64 FMA rate in TFLOP/s (independent FMA chains at
+        full occupancy, best of `reps` launches; synchronises)."""
+        v = C.c_double()
+        _check(self.lib.cuot_measure_fp64_tflops(self.h, C.c_int(reps), C.byref(v)), "cuot_measure_fp64_tflops")
+        return v.value
+
     # ---- AES ---------------------------------------------------------------
     def aes128_ecb(self, key, io, stream=None):
         _check(self.lib.cuot_aes128_ecb(self.h, _host_block(key), _ptr(io), C.c_uint64(_nblocks(io)),

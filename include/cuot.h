@@ -43,6 +43,12 @@ const char *cuot_status_string(int status);
 const char *cuot_last_error(void);
 /* Number of kernels this library has launched in the process (diagnostic). */
 unsigned long long cuot_launch_count(void);
+/* Diagnostic: the fp64 fused-multiply-add rate of ctx's device in TFLOP/s
+ * (2 flops per FMA), from a kernel of independent FMA chains at full
+ * occupancy timed with CUDA events: the best of `reps` (1..1000) launches
+ * after one warm-up, about 9 ms each on B200.  Synchronises.  The measured
+ * denominator of the fp64 FFT encode's fraction. */
+int cuot_measure_fp64_tflops(cuot_ctx *ctx, int reps, double *tflops);
 
 /* ---- context -------------------------------------------------------------
  * A context binds one CUDA device, its AES tables and a grow-only scratch

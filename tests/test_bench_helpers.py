@@ -27,6 +27,9 @@ def test_qc_report_rate_only_for_pure_fft():
     r = bench.qc_transform_report([1 << 20], 1.0)
     assert abs(r["fp64_tflops"] - r["fft_fp64_flops"] / 1e-3 / 1e12) < 1e-9
     assert "fp64_tflops" not in bench.qc_transform_report([1 << 20, 1 << 25], 1.0)
+    assert "frac_of_measured" not in r
+    m = bench.qc_transform_report([1 << 20], 1.0, fp64_peak=40.0)
+    assert abs(m["frac_of_measured"] - m["fp64_tflops"] / 40.0) < 1e-12
 
 
 def test_lpn_l1_roofline_model():

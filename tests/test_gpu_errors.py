@@ -103,3 +103,18 @@ def test_empty_and_degenerate_inputs(ctx):
     d1 = to_dev(one)
     ctx.lpn_primal(seed, kk, d1)
     assert np.array_equal(to_host(d1), oracle.lpn_primal(seed, to_host(kk), one))
+
+
+def test_fp64_rate_probe(ctx):
+    """cuot_measure_fp64_tflops: argument checks, and a rate in a plausible
+    range for B200's fp64 pipe (nominal 37 TFLOP/s)."""
+    import ctypes
+    from cuot_b200 import CuotError
+    v = ctypes.c_double()
+    assert ctx.lib.cuot_measure_fp64_tflops(ctx.h, 0, ctypes.byref(v)) == 1
+    assert ctx.lib.cuot_measure_fp64_tflops(ctx.h, 1, None) == 1
+    with pytest.raises(CuotError):
+        ctx.measure_fp64_tflops(reps=1001)
+    rate = ctx.measure_fp64_tflops(reps=3)
+    print(f"fp64 FMA rate: {rate:.2f} TFLOP/s")
+    assert 10.0 < rate < 100.0
