@@ -1055,7 +1055,10 @@ int qcf_encode_tiles(const QcfTables *t, const QcfAhatTab &ahat, uint32_t *tiles
   // Measured on B200 (one role's 128 planes): n = 2^20, G = 2: 0.78 ms
   // against 0.80 ms for one launch group of all 32 transforms; n = 2^18,
   // G = 8: 0.20 against 0.23 ms; n = 2^22, G = 1: 3.86 against 4.04 ms (at
-  // 2^21, G = 1, 1.74 against 1.71 ms).  It needs Y for 2G transforms.  A context
+  // 2^21, G = 1, 1.74 against 1.71 ms); with the current passes, n = 2^22
+  // 3.48 against 3.65 ms on one stream, 2^21 1.59 against 1.61 ms, and a
+  // third stream loses everywhere (2^20 0.83, 2^21 1.71, 2^22 3.50 ms:
+  // intermediate evicted from L2).  It needs Y for 2G transforms.  A context
   // with CUOT_TUNE_QC_STREAMS = 1 keeps every group on the caller's stream
   // (callers that already run several encodes at once, such as the server).
   uint64_t g64 = (32ull << 20) / ybytes;
