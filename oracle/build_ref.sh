@@ -1,8 +1,8 @@
 #!/bin/sh
 # Builds the oracle's reference pins from the reference's own sources, where
 # they lie under the read-only reference tree (nothing is copied).  Output goes
-# only to oracle/_ref/.  Needs the reference tree, so it runs in the build
-# container only; the GPU box uses the prebuilt files.
+# only to oracle/_ref/.  Needs the reference tree, so it runs only where that
+# tree is present; elsewhere the prebuilt files are used as they are.
 #   _ref/libctref.so   the vendored cryptoTools AES and PRNG
 #                      (silent/lib/cryptoTools/Crypto/{AES,PRNG}.cpp)
 #   _ref/libempref.so  emp-ot's Ferret GGM / SPCOT / LPN headers
