@@ -119,18 +119,20 @@ def test_unknown_schedule_is_rejected(ctx):
     b.close()
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_item_completion_points(ctx, use_graph):
+@pytest.mark.parametrize("use_graph,schedule", [(True, SERIAL), (False, SERIAL), (True, FORK_FERRET),
+                                                (True, FORK_SIZES), (False, FORK_SIZES)])
+def test_item_completion_points(ctx, use_graph, schedule):
     """cuot_batch_wait_item: a copy stream that waits for each instance's
     completion point (rank order: Ferret after the LPN, then the SOT sizes
     largest first) and copies its outputs right away gets the final outputs,
     though the run has not ended when the first copies start.  The outputs
     are zeroed on the compute stream before the run, so a copy that ran early
-    would see zeros or a partial result."""
+    would see zeros or a partial result.  The forked schedules record the
+    points on their own streams (inside the graph when captured)."""
     specs = [(KIND_SOT, 16, 10, 0), (KIND_FERRET, 8, 10, 1000), (KIND_SOT, 64, 10, 0), (KIND_FERRET, 3, 12, 77),
              (KIND_SOT, 4, 10, 0), (KIND_SOT, 2, 12, 0)]
     insts = [Instance(ctx, kd, t, h, 700 + i, k=k) for i, (kd, t, h, k) in enumerate(specs)]
-    b = Batch(ctx, insts, use_graph=use_graph, schedule=SERIAL)
+    b = Batch(ctx, insts, use_graph=use_graph, schedule=schedule)
     ranks = [b.item_rank(i) for i in range(len(insts))]
     assert ranks == [2, 0, 1, 0, 4, 3]  # 2^14, Ferret, 2^16, Ferret, 2^12, 2^13
     with pytest.raises(IndexError):
