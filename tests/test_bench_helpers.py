@@ -30,6 +30,9 @@ def test_qc_report_rate_only_for_pure_fft():
     assert "frac_of_measured" not in r
     m = bench.qc_transform_report([1 << 20], 1.0, fp64_peak=40.0)
     assert abs(m["frac_of_measured"] - m["fp64_tflops"] / 40.0) < 1e-12
+    f = bench.fp64_roofline(m)
+    assert f["peak"] == 40.0 and f["frac"] == m["frac_of_measured"] and f["unit"] == "TFLOP/s"
+    assert bench.fp64_roofline(r) is None
 
 
 def test_lpn_l1_roofline_model():
