@@ -105,11 +105,20 @@ __host__ __device__ constexpr int qcf_col_ctas(int L, int KC) {
 __host__ __device__ constexpr int qcf_fs_lo(int e1) { return (e1 + 1) / 2; }
 __host__ __device__ constexpr int qcf_fs_width(int e1) { return (1 << qcf_fs_lo(e1)) + (1 << (e1 - qcf_fs_lo(e1))); }
 __host__ __device__ constexpr int qcf_fs_ld(int e1) { return qcf_fs_width(e1) + 1; }
+// Start of column c's factor row in shared memory.  In a 4-column CTA a
+// quarter-warp reads 4 columns x 2 items whose high-table entries lie 2
+// apart, so with rows of W = 1 (mod 8) columns c and c + 2 would share a
+// bank group; columns 2 and 3 start 2 values further on, which gives the 8
+// lanes 8 distinct groups (a model of the reads: 1,088 wavefronts per
+// 1024-point CTA before, the ideal 576 after).
+__host__ __device__ constexpr int qcf_fs_col(int e1, int kc, int c) {
+  return c * qcf_fs_ld(e1) + (kc == 4 ? 2 * (c >> 1) : 0);
+}
+__host__ __device__ constexpr int qcf_fs_span(int e1, int kc) { return qcf_fs_col(e1, kc, kc - 1) + qcf_fs_ld(e1); }
 // Columns per CTA of the column passes: 8 (one tile byte per plane and row),
 // or 4 for the 1024-point columns of the tile layout, whose 8-column CTAs
 // (143 KB) would run one per SM; two CTAs then share each tile byte and
 // write one 16-bit half of its word each (see qcf_col_inv).
-constexpr int kCols = 8;
 __host__ __device__ constexpr int qcf_col_threads(int L, int KC) { return KC == 8 ? qcf_threads(L) : qcf_threads(L) / 2; }
 // Rows per CTA of the row pass, so that two CTAs fit an SM: 4 up to 1024
 // points, 2 for 2048, 1 for 4096 (its first pass's twiddles are read
@@ -319,13 +328,14 @@ __device__ __forceinline__ void middle_passes(double2 *xs, const double2 *T) {
 // 2^K rows r = i0 + m (m < 2^K) of one item of the last column pass (i0 a
 // multiple of 2^K): k1 = rev(i0) | rev_K(m) << (E1 - K), and since E1 - K >= lo
 // every row shares the low table entry, read once.
-template <int E1, int K>
+template <int E1, int K, int KC>
 __device__ __forceinline__ void fourstep_ws(const double2 *fs, int c, int i0, double2 (&w)[1 << K]) {
-  constexpr int lo = qcf_fs_lo(E1), W = qcf_fs_ld(E1);
+  constexpr int lo = qcf_fs_lo(E1);
   static_assert(E1 - K >= lo, "the rows of an item share the low factor");
   const int k10 = __brev(i0) >> (32 - E1);
-  const double2 wl = fs[c * W + (k10 & ((1 << lo) - 1))];
-  const double2 *hi = fs + c * W + (1 << lo) + (k10 >> lo);
+  const double2 *fc = fs + qcf_fs_col(E1, KC, c);
+  const double2 wl = fc[k10 & ((1 << lo) - 1)];
+  const double2 *hi = fc + (1 << lo) + (k10 >> lo);
 #pragma unroll
   for (int m = 0; m < (1 << K); m++) w[m] = cmul(wl, hi[(__brev(m) >> (32 - K)) << (E1 - K - lo)]);
 }
@@ -333,12 +343,13 @@ __device__ __forceinline__ void fourstep_ws(const double2 *fs, int c, int i0, do
 __device__ __forceinline__ void stage(double2 *dst, const double2 *src, int cnt) {
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = __ldg(&src[i]);
 }
-// The KC columns' four-step factor rows (global stride W) into rows of W + 1.
+// The KC columns' four-step factor rows (global stride W) into their rows
+// in shared memory (qcf_fs_col).
 template <int E1, int KC>
 __device__ __forceinline__ void stage_fs(double2 *dst, const double2 *fs, int c0) {
   constexpr int W = qcf_fs_width(E1);
   const double2 *src = fs + uint64_t(c0) * W;
-  for (int i = threadIdx.x; i < KC * W; i += blockDim.x) dst[(i / W) * (W + 1) + i % W] = __ldg(&src[i]);
+  for (int i = threadIdx.x; i < KC * W; i += blockDim.x) dst[qcf_fs_col(E1, KC, i / W) + i % W] = __ldg(&src[i]);
 }
 
 // Pass A.  grid (N2 / KC, transforms).  in: plane p at in + p * stride_bytes;
@@ -357,14 +368,14 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
     const uint8_t *__restrict__ in, uint64_t stride_bytes, int nplanes, int one_plane, int e2, int wide,
     const uint32_t *__restrict__ tiles, const double2 *__restrict__ T1, const double2 *__restrict__ fs,
     double2 *__restrict__ Y, const unsigned long long *__restrict__ wa, uint32_t *__restrict__ par) {
-  constexpr int N1 = 1 << E1, ld = sld<KC>(N1), W = qcf_fs_ld(E1);
+  constexpr int N1 = 1 << E1, ld = sld<KC>(N1);
   const uint32_t base = (1u << 21) + uint32_t(wide);
   const double center = CEN && par ? double(kCenter) : 0.0;
   const uint32_t comp = CEN && wa && *wa > (1ull << (E1 + e2 - 1)) ? 1u : 0u;
   constexpr int NP = qcf_npass(E1);
   extern __shared__ double2 sm[];
   double2 *xs = sm, *fss = xs + KC * ld;
-  uint32_t *bits = reinterpret_cast<uint32_t *>(fss + KC * W);
+  uint32_t *bits = reinterpret_cast<uint32_t *>(fss + qcf_fs_span(E1, KC));
   const double2 *Ts = T1;  // pass twiddles read through L1
   const int c0 = blockIdx.x * KC, sub = c0 & 7;  // sub: the CTA's first bit in each tile byte
   const int p0 = 4 * blockIdx.y;
@@ -426,7 +437,7 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
       for (int m = 0; m < Q::R; m++) x[m] = xs[c * ld + spos<E1, KC>(i0 + m)];
       dif_regs<Q::K>(x);
       double2 fw[Q::R];
-      fourstep_ws<E1, Q::K>(fss, c, i0, fw);
+      fourstep_ws<E1, Q::K, KC>(fss, c, i0, fw);
       const uint64_t pol = l2_evict_last_policy();
 #pragma unroll
       for (int m = 0; m < Q::R; m++) st_keep(&Yp[(uint64_t(i0 + m) << e2) + c0 + c], cmul(x[m], fw[m]), pol);
@@ -602,7 +613,7 @@ __global__ void __launch_bounds__(qcf_col_threads(E1, KC), qcf_col_ctas(E1, KC))
       double2 x[Q::R], fw[Q::R];
 #pragma unroll
       for (int m = 0; m < Q::R; m++) x[m] = __ldcs(&Yp[(uint64_t(i0 + m) << e2) + c0 + c]);
-      fourstep_ws<E1, Q::K>(fss, c, i0, fw);
+      fourstep_ws<E1, Q::K, KC>(fss, c, i0, fw);
 #pragma unroll
       for (int m = 0; m < Q::R; m++) x[m] = cmulc(x[m], fw[m]);
       dit_regs<Q::K>(x);
@@ -848,7 +859,7 @@ void qcf_free(QcfTables *t) {
 
 int col_smem(int e1, int kc) {
   const int N1 = 1 << e1;
-  return (kc * (kc == 8 ? sld<8>(N1) : sld<4>(N1)) + kc * qcf_fs_ld(e1)) * 16 + N1 * 4;
+  return (kc * (kc == 8 ? sld<8>(N1) : sld<4>(N1)) + qcf_fs_span(e1, kc)) * 16 + N1 * 4;
 }
 int row_smem(int e2) {
   const int N2 = 1 << e2;
