@@ -507,14 +507,113 @@ __global__ void __launch_bounds__(256) qc_sparse(const uint64_t *__restrict__ a,
   if (acc) atomicXor(reinterpret_cast<unsigned long long *>(out + w), (unsigned long long)acc);
 }
 
+// Window form of the sparse encode (r2 = 0, fewer than 2^31 output words).
+// Positions listed in tree order (one punctured leaf per GGM tree of 2^h
+// leaves) lie close together, so the 257-word windows of `a` that a chunk's
+// positions rotate into the CTA's 256 output words overlap almost entirely:
+// the CTA stages their union (span + 257 words, span = the chunk's largest
+// minus smallest word shift) in shared memory once, and every (word,
+// position) pair then reads shared memory instead of L2.  A chunk whose
+// positions spread wider than kSparseWin (any order is accepted) takes the
+// global-memory loop of qc_sparse.  Positions >= n contribute nothing, as
+// there.
+constexpr int kSparseWin = 4608;  // words of `a` (36 KiB)
+__global__ void __launch_bounds__(256) qc_sparse_win(const uint64_t *__restrict__ a, const uint64_t *__restrict__ pos,
+                                                     int weight, int chunk, uint64_t n, uint64_t *__restrict__ out) {
+  __shared__ uint64_t win[kSparseWin];
+  __shared__ uint32_t sws[kSparseChunk];  // word shift, or ~0u for a position >= n
+  __shared__ uint8_t sbs[kSparseChunk];   // bit shift
+  __shared__ unsigned long long wmin, wmax;
+  const uint64_t nw = n / 64;
+  const int i0 = blockIdx.y * chunk;
+  const int cnt = min(chunk, weight - i0);
+  if (threadIdx.x == 0) {
+    wmin = ~0ull;
+    wmax = 0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const uint64_t p = __ldg(&pos[i0 + i]);
+    if (p < n) {
+      sws[i] = uint32_t(p >> 6);
+      sbs[i] = uint8_t(p & 63);
+      atomicMin(&wmin, (unsigned long long)(p >> 6));
+      atomicMax(&wmax, (unsigned long long)(p >> 6));
+    } else {
+      sws[i] = ~0u;
+    }
+  }
+  __syncthreads();
+  if (wmin > wmax) return;  // no position below n in this chunk (the same for every thread)
+  const uint64_t span = wmax - wmin;
+  const uint64_t w = uint64_t(blockIdx.x) * 256 + threadIdx.x;
+  uint64_t acc = 0;
+  if (span + 257 <= uint64_t(kSparseWin)) {
+    // win[j] = a[(W0 - wmax - 1 + j) mod nw], W0 = the CTA's first output word;
+    // word w = W0 + t under word shift ws needs a[w - ws] = win[t + wmax - ws + 1]
+    // and its lower neighbour win[t + wmax - ws], both inside [0, span + 257)
+    const uint64_t start = (uint64_t(blockIdx.x) * 256 + nw - wmax - 1) % nw;
+    const int len = int(span) + 257;
+    for (int j = threadIdx.x; j < len; j += blockDim.x) win[j] = __ldg(&a[(start + uint64_t(j)) % nw]);
+    __syncthreads();
+    if (w < nw) {
+      const int t1 = int(threadIdx.x) + int(wmax) + 1;
+#pragma unroll 4
+      for (int i = 0; i < cnt; i++) {
+        const uint32_t ws = sws[i];
+        if (ws == ~0u) continue;
+        const int bs = sbs[i];
+        const int idx = t1 - int(ws);
+        uint64_t v = win[idx] << bs;
+        if (bs) v |= win[idx - 1] >> (64 - bs);
+        acc ^= v;
+      }
+    }
+  } else if (w < nw) {
+    for (int i = 0; i < cnt; i++) {
+      const uint32_t ws32 = sws[i];
+      if (ws32 == ~0u) continue;
+      const uint64_t ws = ws32;
+      const int bs = sbs[i];
+      const uint64_t src = w >= ws ? w - ws : w + nw - ws;
+      uint64_t v = __ldg(&a[src]) << bs;
+      if (bs) v |= __ldg(&a[src ? src - 1 : nw - 1]) >> (64 - bs);
+      acc ^= v;
+    }
+  }
+  if (w < nw && acc) atomicXor(reinterpret_cast<unsigned long long *>(out + w), (unsigned long long)acc);
+}
+
 static int launch_sparse(const uint64_t *a_d, const uint64_t *pos_d, int weight, uint64_t n, uint64_t *out_d,
                          int r2, cudaStream_t st) {
   if (cudaMemsetAsync(out_d, 0, n / 8, st) != cudaSuccess) return launch_status(0);
   if (weight == 0) return launch_status(0);
   const uint64_t nw = n / 64;
-  const dim3 grid(unsigned((nw + 255) / 256), unsigned((weight + kSparseChunk - 1) / kSparseChunk));
-  qc_sparse<<<grid, 256, 0, st>>>(a_d, pos_d, weight, n, out_d, r2);
-  return launch_status();
+  const unsigned gx = unsigned((nw + 255) / 256);
+  const bool win = !r2 && nw < (1ull << 31);
+  // Window chunk: in tree order (one position in each run of n / weight
+  // bits) `chunk` consecutive positions span less than chunk * n / weight
+  // bits, i.e. chunk * nw / weight words; the chunk is chosen so that this
+  // fits kSparseWin - 257 (a multiple of 32 in [32, kSparseChunk]).
+  int chunk = kSparseChunk;
+  if (win) {
+    const uint64_t sp = nw / uint64_t(weight) > 1 ? nw / uint64_t(weight) : 1;
+    const uint64_t c = uint64_t(kSparseWin - 257) / sp;
+    chunk = c >= uint64_t(kSparseChunk) ? kSparseChunk : c < 32 ? 32 : int(c / 32 * 32);
+  }
+  // at most 65,535 chunks per launch (grid y)
+  const int per_launch = 65535 * chunk;
+  int launches = 0;
+  for (int off = 0; off < weight; off += per_launch) {
+    const int wpart = weight - off < per_launch ? weight - off : per_launch;
+    const dim3 grid(gx, unsigned((wpart + chunk - 1) / chunk));
+    if (win)
+      qc_sparse_win<<<grid, 256, 0, st>>>(a_d, pos_d + off, wpart, chunk, n, out_d);
+    else
+      qc_sparse<<<grid, 256, 0, st>>>(a_d, pos_d + off, wpart, n, out_d, r2);
+    launches++;
+  }
+  return launch_status(launches);
 }
 
 // ---------------------------------------------------------------------------

@@ -3,6 +3,7 @@ bit-exact against the CPU oracle on seeded inputs and against the golden
 fixtures; full-size configurations are checked through size-independent
 properties (COT correlation, sender/receiver agreement, linearity)."""
 import hashlib
+import zlib
 
 import numpy as np
 import pytest
@@ -357,6 +358,44 @@ def test_sot_dual_lpn_r2_vs_oracle(ctx, e):
     plan.dual_lpn_r2(d, d[:n])
     assert np.array_equal(to_host(d)[:n], exp)
     assert np.array_equal(to_host(d)[n:], x[n:])
+
+
+def _tree_positions(rng, n, h):
+    t = n >> h
+    return np.arange(t, dtype=np.int64) * (1 << h) + rng.integers(0, 1 << h, t)
+
+
+@pytest.mark.parametrize("case", ["tree_h10_n22", "tree_h11_n21", "tree_h14_n20", "tree_h4_n10", "unsorted_wide",
+                                  "unsorted_close", "beyond_n", "n_not_pow2", "duplicates"])
+def test_qc_encode_sparse_position_orders(ctx, case):
+    """The sparse encode (receiver choice bits a * e) against the oracle for
+    the position layouts it meets: tree order (one position per GGM tree,
+    where a chunk's windows of `a` are staged in shared memory), positions
+    spread too wide for the window (the global-memory loop), positions >= n
+    (ignored), n not a power of two, repeated positions (they cancel)."""
+    rng = np.random.default_rng(zlib.crc32(case.encode()))
+    n = {"tree_h10_n22": 1 << 22, "tree_h11_n21": 1 << 21, "tree_h14_n20": 1 << 20, "tree_h4_n10": 1 << 10,
+         "n_not_pow2": 64 * 1000}.get(case, 1 << 18)
+    if case.startswith("tree"):
+        pos = _tree_positions(rng, n, int(case.split("_h")[1].split("_")[0]))
+    elif case == "unsorted_wide":
+        pos = rng.integers(0, n, 3000)
+    elif case == "unsorted_close":
+        pos = rng.permutation(np.arange(5000, 5000 + 64 * 300, 64) + rng.integers(0, 64, 300))
+    elif case == "beyond_n":
+        pos = np.concatenate([rng.integers(0, n, 500), rng.integers(n, 3 * n, 100), [n, n - 1, 0]])
+        rng.shuffle(pos)
+    elif case == "n_not_pow2":
+        pos = np.sort(rng.integers(0, n, 700))
+    else:
+        base = rng.integers(0, n, 200)
+        pos = np.concatenate([base, base[:50], rng.integers(0, n, 30)])
+    a_np = rng.integers(0, 2**63, n // 64, dtype=np.uint64) | (rng.integers(0, 2, n // 64, dtype=np.uint64) << np.uint64(63))
+    a = to_dev(a_np.view(np.int64))
+    out = torch.full((n // 64,), -1, dtype=torch.int64, device="cuda")  # overwritten, not XORed into
+    ctx.qc_encode_sparse(a, to_dev(pos.astype(np.int64)), n, out)
+    exp = oracle.qc_encode_sparse(a_np, pos.astype(np.uint64), n)
+    assert np.array_equal(to_host(out).view(np.uint64), exp)
 
 
 def test_qc_encode_sparse_r2(ctx):
